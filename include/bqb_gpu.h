@@ -1,0 +1,208 @@
+/*
+ * bqb_gpu.h -- C ABI of libbqb_gpu.so, the B200 implementation of BiqBin's
+ * per-node SDP bounding path.
+ *
+ * Part 1 (drop-in): the exact entry points the reference's host code
+ * (bounding.c, bundle.c's callers, bab_functions.c, evaluate.c, the pybind
+ * bridge) calls today.  Signatures, argument meaning, global-state contract
+ * and fatal-error behaviour follow the reference declarations cited beside
+ * each.  Linking the reference's host objects against this library instead
+ * of ipm_mc_pk.c, bundle.c, operators.c, cutting_planes.c,
+ * qap_simulated_annealing.c and heuristic.c makes its branch-and-bound loop
+ * run its bounding on the GPU.
+ *
+ * Global state: like the reference, these functions read and write the
+ * process globals X, Z, X_bundle, X_test, dual_gamma, dgamma, gamma_test,
+ * lambda, eta, F, G, g, f, Cuts, List, Pent_Cuts, Pent_List, Hepta_Cuts,
+ * Hepta_List, params, SP, PP, BabPbSize (src/global_var.h:1-48,
+ * src/heap.c:7-8).  The library defines them too; when the host program
+ * defines them (the reference's allocate_free.c / heap.c), the program's
+ * definitions are the ones used.
+ *
+ * Part 2 (additions): initialisation and status, the batched and
+ * device-pointer entry points used by the batched B&B driver and the
+ * benchmarks, and a standalone solver.
+ *
+ * Errors: numeric failures on the path are fatal in the reference
+ * (MPI_Abort(MPI_COMM_WORLD, 10), e.g. src/ipm_mc_pk.c:132-136).  Here they
+ * call the abort hook (default: print and exit(10)); bqb_last_error() keeps
+ * the message.  There is no CPU fallback: without a usable CUDA device every
+ * entry point fails through the same hook.
+ */
+#ifndef BQB_GPU_H
+#define BQB_GPU_H
+
+#include <stddef.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- types (layouts identical to the reference) --------------------- */
+#define BQB_NMAX 1024                 /* src/biqbin_cpp_api.h:38 NMAX */
+#define BQB_MAX_TRI_INEQ 50000        /* src/biqbin.h:37 MaxTriIneqAdded */
+#define BQB_MAX_PENT_INEQ 50000       /* src/biqbin.h:38 */
+#define BQB_MAX_HEPTA_INEQ 50000      /* src/biqbin.h:39 */
+#define BQB_MAX_BUNDLE 400            /* src/biqbin.h:42 MaxBundle */
+
+#ifndef BIQBIN_CPP_API_H
+/* src/biqbin_cpp_api.h:27-35 */
+typedef struct Problem {
+    double *L;
+    int n;
+    int NIneq;
+    int NPentIneq;
+    int NHeptaIneq;
+    int bundle;
+} Problem;
+
+/* src/biqbin_cpp_api.h:41-63 */
+typedef struct BabSolution {
+    int X[BQB_NMAX];
+} BabSolution;
+
+typedef struct BabNode {
+    int xfixed[BQB_NMAX];
+    BabSolution sol;
+    double fracsol[BQB_NMAX];
+    int level;
+    double upper_bound;
+} BabNode;
+#endif
+
+#ifndef BIQBIN_H
+/* src/biqbin.h:81-107 */
+typedef struct Triangle_Inequality {
+    int i, j, k, type;
+    double value;
+    double y;
+} Triangle_Inequality;
+
+typedef struct Pentagonal_Inequality {
+    int type;
+    int permutation[5];
+    double value;
+    double y;
+} Pentagonal_Inequality;
+
+typedef struct Heptagonal_Inequality {
+    int type;
+    int permutation[7];
+    double value;
+    double y;
+} Heptagonal_Inequality;
+
+/* src/biqbin.h:49-84 (PARAM_FIELDS, same order and types) */
+typedef struct BiqBinParameters {
+    int init_bundle_iter;
+    int max_bundle_iter;
+    int triag_iter;
+    int pent_iter;
+    int hept_iter;
+    int max_outer_iter;
+    int extra_iter;
+    double violated_TriIneq;
+    int TriIneq;
+    int adjust_TriIneq;
+    int PentIneq;
+    int HeptaIneq;
+    int Pent_Trials;
+    int Hepta_Trials;
+    int include_Pent;
+    int include_Hepta;
+    int root;
+    int use_diff;
+    int time_limit;
+    int branchingStrategy;
+} BiqBinParameters;
+#endif
+
+/* ==== Part 1: drop-in entry points ==================================== */
+
+/* Basic SDP bound, src/ipm_mc_pk.c:28 (decl. src/biqbin.h:181).
+ * L: n x n column-major; X: n x n output; phi: output. print is ignored. */
+void ipm_mc_pk(double *L, int n, double *X, double *phi, int print);
+
+/* y -= B(X) over the global cut lists, src/operators.c:51 (biqbin.h:186). */
+void op_B(const Problem *P, double *y, const double *X);
+/* X -= B^T(tt), src/operators.c:140 (biqbin.h:187). */
+void op_Bt(const Problem *P, double *X, const double *tt);
+/* diag / Diag, src/operators.c:14,26 (biqbin.h:184-185). */
+void diag(const double *X, double *y, int n);
+void Diag(double *X, const double *y, int n);
+
+/* Dual function value and subgradient, src/bundle.c:242 (biqbin.h:145). */
+double fct_eval(const Problem *PP, double *dual_gamma, double *X, double *g);
+/* Bundle QP pieces, src/bundle.c:390 and :292 (biqbin.h:146-147). */
+void solve_lambda(int k, double *Q, double *c, double *lambda);
+void lambda_eta(const Problem *PP, double *zeta, double *G, double *dual_gamma, double *dgamma,
+                double *lambda, double *eta, double *t);
+/* Proximal bundle iterations on the globals, src/bundle.c:9 (biqbin.h:148). */
+void bundle_method(Problem *PP, double *t, int bdl_iter);
+
+/* Separation, src/cutting_planes.c:20,48,132,224,316,416,509 (biqbin.h:151-157). */
+double evaluateTriangleInequality(double *XX, int N, int type, int ii, int jj, int kk);
+double getViolated_TriangleInequalities(double *X, int N, Triangle_Inequality *List, int *ListSize);
+double updateTriangleInequalities(Problem *PP, double *y, int *NumAdded, int *NumSubtracted);
+double getViolated_PentagonalInequalities(double *X, int N, Pentagonal_Inequality *Pent_List,
+                                          int *ListSize);
+double updatePentagonalInequalities(Problem *PP, double *y, int *NumAdded, int *NumSubtracted,
+                                    int triag);
+double getViolated_HeptagonalInequalities(double *X, int N, Heptagonal_Inequality *Hepta_List,
+                                          int *ListSize);
+double updateHeptagonalInequalities(Problem *PP, double *y, int *NumAdded, int *NumSubtracted,
+                                    int hept_index);
+/* src/qap_simulated_annealing.c:12 (biqbin.h:192). */
+double qap_simulated_annealing(int *H, int k, double *X, int n, int *pent);
+
+/* Heuristic, src/heuristic.c:11,19,119,195,304 (biqbin.h:170-174,
+ * biqbin_cpp_api.h:65,68). */
+double runHeuristic(Problem *P0, Problem *P, BabNode *node, int *x);
+double runHeuristic_unpacked(double *P0_L, int P0_N, double *P_L, int P_N, int *node_xfixed,
+                             int *node_sol_X, int *x);
+double GW_heuristic(double *P0_L, int P0_N, double *P_L, int P_N, int *node_xfixed,
+                    int *node_sol_X, int *x, int num);
+double mc_1opt(int *x, double *P_L, int P_N);
+int update_best(int *xbest, int *xnew, double *best, int P0_N);
+
+/* ==== Part 2: additions =============================================== */
+
+/* Bind the library to a CUDA device (default 0) and create its stream.
+ * Called implicitly by every entry point; returns 0 on success. */
+int bqb_init(int device);
+/* Last error message ("" if none). */
+const char *bqb_last_error(void);
+/* Replace the fatal-error action (default: print, exit(10)).  The hook
+ * receives the reference's abort code 10; if it returns, the failing entry
+ * point returns with its outputs unspecified. */
+void bqb_set_abort_hook(void (*hook)(int code));
+/* Number of CUDA kernels this library has launched so far. */
+unsigned long long bqb_kernel_launches(void);
+/* Wait for all work the library queued. */
+void bqb_synchronize(void);
+
+/* Batched basic SDP bound over device-resident problems: one CTA per
+ * problem, one launch.  Ls[i], Xs[i]: device pointers, n x n column-major,
+ * n = ns[i] (sizes may differ); out: device array of 4*nprob doubles:
+ * phi, iterations, status (0 ok), <L,X>.
+ * A plan holds the device descriptors and scratch; launching it is
+ * asynchronous on `stream` (a cudaStream_t; NULL = the library stream). */
+typedef struct bqb_ipm_plan bqb_ipm_plan;
+bqb_ipm_plan *bqb_ipm_plan_create(const double *const *Ls, double *const *Xs, const int *ns,
+                                  int nprob, double *out);
+int bqb_ipm_plan_launch(bqb_ipm_plan *plan, void *stream);
+void bqb_ipm_plan_destroy(bqb_ipm_plan *plan);
+/* create + launch + synchronize + destroy. */
+int bqb_ipm_batch_device(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
+                         double *out, void *stream);
+
+/* Same, host memory in and out (copies included), synchronous. */
+int bqb_ipm_batch(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
+                  double *phi, int *iters, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BQB_GPU_H */

@@ -1,0 +1,491 @@
+// Basic Max-Cut SDP interior-point method (FP64), one CTA per problem.
+//
+// Restates the primal-dual predictor-corrector loop of the reference
+// ipm_mc_pk (src/ipm_mc_pk.c:28-359):
+//   max <L,X> s.t. diag(X) = e, X psd;   min e'y s.t. Z = Diag(y) - L psd.
+// Start y = 1.1 + column sums of |L|, X = I, Z = Diag(y) - L (:65-99); loop
+// while |phi - psi| > 1e-2 (:124-126).  Per iteration: Zi = inv(Z)
+// (:129-150), predictor dy1 = (Zi.*X) \ (-e) (:157-173),
+// dX1 = -Zi Diag(dy1) X - X symmetrised (:181-199), corrector
+// dy2 = (Zi.*X) \ (mu diag(Zi) - (Zi.*dX1) dy1) (:207-230),
+// dX2 = mu Zi - Zi (Diag(dy2) X + Diag(dy1) dX1) (:238-260), dX = dX1 + dX2
+// symmetrised, dZ = Diag(dy) (:265-275), line searches alpha *= 0.8 until
+// the Cholesky of X + a dX / Z + a dZ succeeds, then *0.95 (:281-309),
+// updates and mu heuristics (:313-324).
+//
+// Z is never stored: off the diagonal Z = -L exactly (Diag(y) - L, and dZ is
+// diagonal), so only its diagonal zd is kept and updated as the reference
+// updates Z_ii.  The Schur matrix M = Zi.*X is factored once per iteration
+// and reused for the corrector solve (the reference refactors the same
+// matrix).  Zi is formed by a symmetric Gauss-Jordan sweep on the lower
+// triangle; its pivots are the Schur complements of Z, so a non-positive
+// pivot is exactly "Z not positive definite".
+#include "ipm.cuh"
+
+#include <math.h>
+
+namespace bqb {
+namespace {
+
+// Cholesky of the lower triangle of A (in place).  Returns false, uniformly
+// over the block, at the first non-positive pivot (the line-search test).
+__device__ bool cta_potrf_lower(double* A, int n, int ld, double* col)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int k = 0; k < n; ++k) {
+        const double d = A[k + (size_t)k * ld];
+        if (!(d > 0.0)) return false;
+        const double s = sqrt(d);
+        const double inv = 1.0 / s;
+        for (int i = k + 1 + tid; i < n; i += nt) {
+            const double v = A[i + (size_t)k * ld] * inv;
+            col[i] = v;
+            A[i + (size_t)k * ld] = v;
+        }
+        __syncthreads();
+        if (tid == 0) A[k + (size_t)k * ld] = s;
+        for (int j = k + 1 + warp; j < n; j += nw) {
+            const double cj = col[j];
+            double* Aj = A + (size_t)j * ld;
+            for (int i = j + lane; i < n; i += 32) Aj[i] = fma(-col[i], cj, Aj[i]);
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// In-place inverse of a symmetric positive definite matrix held in the lower
+// triangle (symmetric sweep / Gauss-Jordan without pivoting).  On success A
+// holds the full symmetric inverse (both triangles).
+__device__ bool cta_spd_inverse(double* A, int n, int ld, double* col)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int k = 0; k < n; ++k) {
+        const double d = A[k + (size_t)k * ld];
+        if (!(d > 0.0)) return false;
+        for (int i = tid; i < n; i += nt)
+            col[i] = (i >= k) ? A[i + (size_t)k * ld] : A[k + (size_t)i * ld];
+        __syncthreads();
+        const double inv = 1.0 / d;
+        for (int j = warp; j < n; j += nw) {
+            double* Aj = A + (size_t)j * ld;
+            if (j == k) {
+                for (int i = j + lane; i < n; i += 32) Aj[i] = (i == k) ? -inv : col[i] * inv;
+            } else {
+                const double tj = col[j] * inv;
+                for (int i = j + lane; i < n; i += 32)
+                    Aj[i] = (i == k) ? tj : fma(-col[i], tj, Aj[i]);
+            }
+        }
+        __syncthreads();
+    }
+    // the sweep leaves -inv(A); negate and mirror to the upper triangle
+    for (int j = warp; j < n; j += nw) {
+        for (int i = j + lane; i < n; i += 32) {
+            const double v = -A[i + (size_t)j * ld];
+            A[i + (size_t)j * ld] = v;
+            A[j + (size_t)i * ld] = v;
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// Solve (F F^T) x = b with F the lower Cholesky factor; one warp; b in smem.
+__device__ void warp_chol_solve(const double* F, int n, int ld, double* b)
+{
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < n; ++k) {
+        const double bk = b[k] / F[k + (size_t)k * ld];
+        __syncwarp();
+        if (lane == 0) b[k] = bk;
+        const double* Fk = F + (size_t)k * ld;
+        for (int i = k + 1 + lane; i < n; i += 32) b[i] = fma(-Fk[i], bk, b[i]);
+        __syncwarp();
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        const double xk = b[k] / F[k + (size_t)k * ld];
+        __syncwarp();
+        if (lane == 0) b[k] = xk;
+        for (int i = lane; i < k; i += 32) b[i] = fma(-F[k + (size_t)i * ld], xk, b[i]);
+        __syncwarp();
+    }
+}
+
+// Exact symmetrisation A = (A + A^T)/2 as the reference writes it
+// (src/ipm_mc_pk.c:196-199): both entries get 0.5*(a_ij + a_ji).
+__device__ void cta_symmetrize(double* A, int n)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = warp; j < n; j += nw) {
+        for (int i = j + 1 + lane; i < n; i += 32) {
+            const double v = 0.5 * (A[j + (size_t)i * n] + A[i + (size_t)j * n]);
+            A[i + (size_t)j * n] = v;
+            A[j + (size_t)i * n] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// C = A * B' with A (n x n, column-major, read in place) and B'(k, c) formed
+// on the fly by `bfun` and staged through shared memory in k-chunks.  Each
+// thread owns a 4 x 8 register tile of a 128 x 128 supertile.  The k sum is
+// sequential, so results are deterministic.  `epi(r, c, acc)` stores.
+constexpr int STG_LD = IPM_TILE + 1;
+
+template <class BF, class EF>
+__device__ void cta_gemm(const double* A, int n, int lda, BF bfun, EF epi, double* stage)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tr = tid & 31;
+    const int tc = tid >> 5;   // 0..15
+    for (int r0 = 0; r0 < n; r0 += IPM_TILE) {
+        for (int c0 = 0; c0 < n; c0 += IPM_TILE) {
+            double acc[4][8];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+            for (int k0 = 0; k0 < n; k0 += IPM_KC) {
+                for (int e = tid; e < IPM_KC * IPM_TILE; e += nt) {
+                    const int kk = e % IPM_KC, cc = e / IPM_KC;
+                    const int k = k0 + kk, c = c0 + cc;
+                    stage[kk * STG_LD + cc] = (k < n && c < n) ? bfun(k, c) : 0.0;
+                }
+                __syncthreads();
+                const int kmax = min(IPM_KC, n - k0);
+                for (int kk = 0; kk < kmax; ++kk) {
+                    const double* Ak = A + (size_t)(k0 + kk) * lda;
+                    double av[4], bv[8];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const int r = r0 + tr + 32 * a;
+                        av[a] = (r < n) ? Ak[r] : 0.0;
+                    }
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) bv[b] = stage[kk * STG_LD + tc + 16 * b];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int r = r0 + tr + 32 * a;
+                if (r >= n) continue;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    const int c = c0 + tc + 16 * b;
+                    if (c < n) epi(r, c, acc[a][b]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+struct Layout {
+    double* red;   // 64
+    double* y;     // n
+    double* zd;    // n   diagonal of Z
+    double* dy;    // n
+    double* dy1;   // n
+    double* rhs;   // n
+    double* col;   // n
+    double* stage; // IPM_KC * STG_LD
+    double* F;     // n*n  Cholesky workspace
+    double* Zi;    // n*n
+    double* dX;    // n*n
+    double* dX1;   // n*n
+};
+
+__host__ __device__ inline size_t ipm_fixed_smem_doubles(int n)
+{
+    return 64 + 6 * (size_t)((n + 1) & ~1) + (size_t)IPM_KC * STG_LD;
+}
+
+__device__ Layout make_layout(const IpmDesc& d, double* smem, int place)
+{
+    const int n = d.n;
+    const size_t nn = (size_t)n * n;
+    const size_t nv = (size_t)((n + 1) & ~1);
+    Layout l;
+    l.red = smem;
+    l.y = l.red + 64;
+    l.zd = l.y + nv;
+    l.dy = l.zd + nv;
+    l.dy1 = l.dy + nv;
+    l.rhs = l.dy1 + nv;
+    l.col = l.rhs + nv;
+    l.stage = l.col + nv;
+    double* after = l.stage + (size_t)IPM_KC * STG_LD;
+    double* ws = d.ws;
+    if (place & 1) { l.F = after; after += nn; } else { l.F = ws; ws += nn; }
+    if (place & 2) { l.Zi = after; after += nn; } else { l.Zi = ws; ws += nn; }
+    l.dX = ws; ws += nn;
+    l.dX1 = ws;
+    return l;
+}
+
+__device__ void ipm_body(const IpmDesc& d, double* smem, int place)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    const int n = d.n;
+    const size_t nn = (size_t)n * n;
+    const double* __restrict__ L = d.L;
+    double* __restrict__ X = d.X;
+    Layout s = make_layout(d, smem, place);
+
+    // ---- initial point (src/ipm_mc_pk.c:65-99) ----
+    for (int c = tid; c < n; c += nt) {
+        double acc = 0.0;
+        const double* Lc = L + (size_t)c * n;
+        for (int r = 0; r < n; ++r) acc += fabs(Lc[r]);
+        s.y[c] = acc + 1.1;
+    }
+    for (size_t e = tid; e < nn; e += nt) X[e] = 0.0;
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) {
+        X[i + (size_t)i * n] = 1.0;
+        s.zd[i] = s.y[i] - L[i + (size_t)i * n];
+    }
+    __syncthreads();
+    {
+        double a = 0.0, b = 0.0;
+        for (int i = tid; i < n; i += nt) { a += L[i + (size_t)i * n]; b += s.zd[i]; }
+        a = block_sum(a, s.red);
+        b = block_sum(b, s.red);
+        double phi = 0.0;
+        for (int i = tid; i < n; i += nt) phi += s.y[i];
+        phi = block_sum(phi, s.red);
+        double psi = a;
+        double mu = b / (2.0 * n);
+        double gap = fabs(phi - psi);
+        int iter = 0;
+        int status = IPM_OK;
+
+        while (gap > 1e-2) {
+            if (++iter > IPM_MAX_ITERS) { status = IPM_MAXITER; break; }
+
+            // ---- Zi = inv(Z), Z = Diag(zd) - L off the diagonal ----
+            for (int j = warp; j < n; j += nw)
+                for (int i = j + lane; i < n; i += 32)
+                    s.Zi[i + (size_t)j * n] = (i == j) ? s.zd[i] : -L[i + (size_t)j * n];
+            __syncthreads();
+            if (!cta_spd_inverse(s.Zi, n, n, s.col)) { status = IPM_Z_NOT_PD; break; }
+
+            // ---- predictor: M = Zi .* X, dy1 = M \ (-e) ----
+            for (int j = warp; j < n; j += nw)
+                for (int i = j + lane; i < n; i += 32)
+                    s.F[i + (size_t)j * n] = s.Zi[i + (size_t)j * n] * X[i + (size_t)j * n];
+            for (int i = tid; i < n; i += nt) s.rhs[i] = -1.0;
+            __syncthreads();
+            if (!cta_potrf_lower(s.F, n, n, s.col)) { status = IPM_M_NOT_PD; break; }
+            if (warp == 0) warp_chol_solve(s.F, n, n, s.rhs);
+            __syncthreads();
+            for (int i = tid; i < n; i += nt) s.dy1[i] = s.rhs[i];
+            __syncthreads();
+
+            // ---- dX1 = Zi * (-Diag(dy1) X) - X, symmetrised ----
+            {
+                const double* dy1 = s.dy1;
+                double* dX1 = s.dX1;
+                cta_gemm(
+                    s.Zi, n, n,
+                    [=] __device__(int k, int c) { return -dy1[k] * X[k + (size_t)c * n]; },
+                    [=] __device__(int r, int c, double acc) {
+                        dX1[r + (size_t)c * n] = acc - X[r + (size_t)c * n];
+                    },
+                    s.stage);
+                cta_symmetrize(dX1, n);
+            }
+
+            // ---- corrector rhs = mu diag(Zi) - (Zi .* dX1) dy1 ----
+            for (int r = warp; r < n; r += nw) {
+                double acc = 0.0;
+                for (int c = lane; c < n; c += 32)
+                    acc = fma(s.Zi[r + (size_t)c * n] * s.dX1[r + (size_t)c * n], s.dy1[c], acc);
+                acc = warp_sum(acc);
+                if (lane == 0) s.rhs[r] = mu * s.Zi[r + (size_t)r * n] - acc;
+            }
+            __syncthreads();
+            if (warp == 0) warp_chol_solve(s.F, n, n, s.rhs);
+            __syncthreads();
+
+            // ---- dX = Zi * (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1 ----
+            {
+                const double* dy1 = s.dy1;
+                const double* dy2 = s.rhs;
+                const double* dX1 = s.dX1;
+                const double* Zi = s.Zi;
+                double* dX = s.dX;
+                const double muc = mu;
+                cta_gemm(
+                    s.Zi, n, n,
+                    [=] __device__(int k, int c) {
+                        const size_t e = k + (size_t)c * n;
+                        return -dy2[k] * X[e] + -dy1[k] * dX1[e];
+                    },
+                    [=] __device__(int r, int c, double acc) {
+                        const size_t e = r + (size_t)c * n;
+                        dX[e] = dX1[e] + (acc + muc * Zi[e]);
+                    },
+                    s.stage);
+                cta_symmetrize(dX, n);
+            }
+            for (int i = tid; i < n; i += nt) s.dy[i] = s.dy1[i] + s.rhs[i];
+            __syncthreads();
+
+            // ---- primal line search: chol(X + ap dX) ----
+            double ap = 1.0;
+            int trials = 0;
+            bool ok = false;
+            while (true) {
+                for (int j = warp; j < n; j += nw)
+                    for (int i = j + lane; i < n; i += 32) {
+                        const size_t e = i + (size_t)j * n;
+                        s.F[e] = fma(ap, s.dX[e], X[e]);
+                    }
+                __syncthreads();
+                if (cta_potrf_lower(s.F, n, n, s.col)) { ok = true; break; }
+                __syncthreads();
+                if (++trials >= IPM_MAX_TRIALS) break;
+                ap *= 0.8;
+            }
+            if (!ok) { status = IPM_LINESEARCH; break; }
+            if (ap < 1.0) ap *= 0.95;
+
+            // ---- dual line search: chol(Z + ad Diag(dy)) ----
+            double ad = 1.0;
+            trials = 0;
+            ok = false;
+            while (true) {
+                for (int j = warp; j < n; j += nw)
+                    for (int i = j + lane; i < n; i += 32)
+                        s.F[i + (size_t)j * n] =
+                            (i == j) ? fma(ad, s.dy[i], s.zd[i]) : -L[i + (size_t)j * n];
+                __syncthreads();
+                if (cta_potrf_lower(s.F, n, n, s.col)) { ok = true; break; }
+                __syncthreads();
+                if (++trials >= IPM_MAX_TRIALS) break;
+                ad *= 0.8;
+            }
+            if (!ok) { status = IPM_LINESEARCH; break; }
+            if (ad < 1.0) ad *= 0.95;
+
+            // ---- update (src/ipm_mc_pk.c:313-334) ----
+            double zx = 0.0, lx = 0.0;
+            for (int j = warp; j < n; j += nw) {
+                for (int i = lane; i < n; i += 32) {
+                    const size_t e = i + (size_t)j * n;
+                    const double xv = fma(ap, s.dX[e], X[e]);
+                    X[e] = xv;
+                    const double lv = L[e];
+                    lx = fma(lv, xv, lx);
+                    if (i != j) zx = fma(-lv, xv, zx);
+                }
+            }
+            __syncthreads();
+            double ysum = 0.0;
+            for (int i = tid; i < n; i += nt) {
+                const double yi = fma(ad, s.dy[i], s.y[i]);
+                const double zi = fma(ad, s.dy[i], s.zd[i]);
+                s.y[i] = yi;
+                s.zd[i] = zi;
+                ysum += yi;
+                zx = fma(zi, X[i + (size_t)i * n], zx);
+            }
+            zx = block_sum(zx, s.red);
+            lx = block_sum(lx, s.red);
+            ysum = block_sum(ysum, s.red);
+            mu = zx / (2.0 * n);
+            if (ap + ad > 1.6) mu *= 0.5;
+            if (ap + ad > 1.9) mu *= 0.2;
+            phi = ysum;
+            psi = lx;
+            gap = fabs(phi - psi);
+        }
+
+        if (tid == 0) {
+            d.out[0] = phi;
+            d.out[1] = (double)iter;
+            d.out[2] = (double)status;
+            d.out[3] = psi;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(IPM_THREADS, 1)
+ipm_batched_kernel(const IpmDesc* __restrict__ descs, int place)
+{
+    extern __shared__ __align__(16) double smem[];
+    const IpmDesc d = descs[blockIdx.x];
+    if (d.n <= 0) return;
+    ipm_body(d, smem, place);
+}
+
+__global__ void __launch_bounds__(IPM_THREADS, 1)
+ipm_one_kernel(IpmDesc d, int place)
+{
+    extern __shared__ __align__(16) double smem[];
+    if (d.n <= 0) return;
+    ipm_body(d, smem, place);
+}
+
+}  // namespace
+
+int ipm_place(int n_max, size_t smem_limit, size_t* smem_bytes)
+{
+    const size_t fixed = ipm_fixed_smem_doubles(n_max) * sizeof(double);
+    const size_t mat = (size_t)n_max * n_max * sizeof(double);
+    int place = 0;
+    size_t bytes = fixed;
+    if (fixed + 2 * mat <= smem_limit) {
+        place = 3;
+        bytes = fixed + 2 * mat;
+    } else if (fixed + mat <= smem_limit) {
+        place = 1;
+        bytes = fixed + mat;
+    }
+    if (smem_bytes) *smem_bytes = bytes;
+    return place;
+}
+
+size_t ipm_ws_doubles(int n, int place)
+{
+    const size_t nn = (size_t)n * n;
+    return nn * (2 + ((place & 1) ? 0 : 1) + ((place & 2) ? 0 : 1));
+}
+
+static void set_smem_attr(const void* fn, size_t bytes)
+{
+    BQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+void ipm_launch(const IpmDesc* d_descs, int nprob, int n_max, cudaStream_t s)
+{
+    if (nprob <= 0) return;
+    size_t bytes = 0;
+    const int place = ipm_place(n_max, rt().smem_optin, &bytes);
+    set_smem_attr((const void*)ipm_batched_kernel, bytes);
+    ipm_batched_kernel<<<nprob, IPM_THREADS, bytes, s>>>(d_descs, place);
+    BQB_COUNT_LAUNCH();
+    check_launch("ipm_batched_kernel");
+}
+
+void ipm_launch_one(const IpmDesc& d, cudaStream_t s)
+{
+    size_t bytes = 0;
+    const int place = ipm_place(d.n, rt().smem_optin, &bytes);
+    set_smem_attr((const void*)ipm_one_kernel, bytes);
+    ipm_one_kernel<<<1, IPM_THREADS, bytes, s>>>(d, place);
+    BQB_COUNT_LAUNCH();
+    check_launch("ipm_one_kernel");
+}
+
+}  // namespace bqb

@@ -1,0 +1,138 @@
+// Process runtime: device binding, stream, error/abort plumbing, and the
+// definitions of the reference's process globals (used when the host
+// program does not define them itself).
+#include <stdarg.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "../../include/bqb_gpu.h"
+#include "bqb_common.cuh"
+
+// ---- the reference's globals (src/global_var.h:1-48, src/heap.c:7-8) ----
+// A host program that defines them (the reference's allocate_free.c and
+// heap.c) takes precedence at dynamic link time; these copies serve
+// standalone use of the library.
+extern "C" {
+__attribute__((visibility("default"))) BiqBinParameters params;
+__attribute__((visibility("default"))) Problem* SP = nullptr;
+__attribute__((visibility("default"))) Problem* PP = nullptr;
+__attribute__((visibility("default"))) double* X = nullptr;
+__attribute__((visibility("default"))) double* Z = nullptr;
+__attribute__((visibility("default"))) double* X_bundle = nullptr;
+__attribute__((visibility("default"))) double* X_test = nullptr;
+__attribute__((visibility("default"))) double* dual_gamma = nullptr;
+__attribute__((visibility("default"))) double* dgamma = nullptr;
+__attribute__((visibility("default"))) double* gamma_test = nullptr;
+__attribute__((visibility("default"))) double* lambda = nullptr;
+__attribute__((visibility("default"))) double* eta = nullptr;
+__attribute__((visibility("default"))) double* F = nullptr;
+__attribute__((visibility("default"))) double* G = nullptr;
+__attribute__((visibility("default"))) double* g = nullptr;
+__attribute__((visibility("default"))) double f = 0.0;
+__attribute__((visibility("default"))) Triangle_Inequality* Cuts = nullptr;
+__attribute__((visibility("default"))) Triangle_Inequality* List = nullptr;
+__attribute__((visibility("default"))) Pentagonal_Inequality* Pent_Cuts = nullptr;
+__attribute__((visibility("default"))) Pentagonal_Inequality* Pent_List = nullptr;
+__attribute__((visibility("default"))) Heptagonal_Inequality* Hepta_Cuts = nullptr;
+__attribute__((visibility("default"))) Heptagonal_Inequality* Hepta_List = nullptr;
+__attribute__((visibility("default"))) int BabPbSize = 0;
+}
+
+namespace bqb {
+
+unsigned long long g_launches = 0;
+
+static char g_last_error[512] = "";
+static void (*g_abort_hook)(int) = nullptr;
+
+void set_error(const char* where, const char* msg)
+{
+    snprintf(g_last_error, sizeof g_last_error, "%s: %s", where, msg);
+}
+
+void fatal(const char* where, const char* msg)
+{
+    set_error(where, msg);
+    fprintf(stderr, "bqb_gpu fatal: %s\n", g_last_error);
+    fflush(stderr);
+    if (g_abort_hook) {
+        g_abort_hook(10);
+        return;
+    }
+    exit(10);
+}
+
+static Runtime g_rt;
+static std::once_flag g_once;
+
+static void init_device(int dev)
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        fatal("bqb_init", e != cudaSuccess ? cudaGetErrorString(e) : "no CUDA device");
+        return;
+    }
+    if (dev < 0 || dev >= count) dev = 0;
+    BQB_CUDA(cudaSetDevice(dev));
+    cudaDeviceProp prop;
+    BQB_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) {
+        char buf[128];
+        snprintf(buf, sizeof buf, "device %s is sm_%d%d; this build targets sm_100a", prop.name,
+                 prop.major, prop.minor);
+        fatal("bqb_init", buf);
+        return;
+    }
+    g_rt.device = dev;
+    g_rt.num_sms = prop.multiProcessorCount;
+    g_rt.smem_optin = prop.sharedMemPerBlockOptin;
+    BQB_CUDA(cudaStreamCreateWithFlags(&g_rt.stream, cudaStreamNonBlocking));
+}
+
+Runtime& rt()
+{
+    std::call_once(g_once, [] {
+        const char* env = getenv("BQB_DEVICE");
+        init_device(env ? atoi(env) : 0);
+    });
+    return g_rt;
+}
+
+}  // namespace bqb
+
+extern "C" {
+
+__attribute__((visibility("default"))) int bqb_init(int device)
+{
+    if (device >= 0) {
+        char buf[16];
+        snprintf(buf, sizeof buf, "%d", device);
+        setenv("BQB_DEVICE", buf, 0);
+    }
+    bqb::rt();
+    return bqb::rt().device >= 0 ? 0 : 1;
+}
+
+__attribute__((visibility("default"))) const char* bqb_last_error(void)
+{
+    return bqb::g_last_error;
+}
+
+__attribute__((visibility("default"))) void bqb_set_abort_hook(void (*hook)(int))
+{
+    bqb::g_abort_hook = hook;
+}
+
+__attribute__((visibility("default"))) unsigned long long bqb_kernel_launches(void)
+{
+    return bqb::g_launches;
+}
+
+__attribute__((visibility("default"))) void bqb_synchronize(void)
+{
+    BQB_CUDA(cudaStreamSynchronize(bqb::rt().stream));
+}
+
+}  // extern "C"
