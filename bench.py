@@ -1,0 +1,473 @@
+#!/usr/bin/env python
+"""Benchmark: B&B node-bounding throughput (nodes/s) on B200.
+
+Workload (the batched node-bounding configuration): a G(100, 0.5) Max-Cut
+instance with edge weights uniform in {-1, +1} (seeded, synthetic), and 512
+of its B&B subproblems, each with k uniform in [0, 40] vertices fixed to
+uniform 0/1 values (subproblem sizes n = 60..100), triangle budget
+TriIneq = 3n (adjust_TriIneq = 0), otherwise the reference's shipped
+parameters.  First the root is bounded with rank 0 (this sets the incumbent
+and `diff` as the reference's master does); then every subproblem is bounded
+as a worker bounds a node (rank 1): IPM, heuristic, prune / give-up tests,
+cutting planes and bundle iterations to the reference's stopping rules.
+A step bounds one batch of subproblems; the metric is nodes/s.
+
+  value : SDPbound on device-resident subproblem matrices (inputs in HBM)
+  e2e   : Evaluate(node, SP, PP, 1) through the C ABI with host buffers, as
+          the reference's B&B calls it (subproblem construction and every
+          host<->device copy inside the timed region)
+
+`--impl reference` times the reference's own C implementation (built
+unmodified into oracle/_ref/libbqb_ref.so) on the host cores, one process per
+core, each bounding its share of a sample of the same subproblems.
+
+Multi-GPU (torchrun): B&B nodes are independent, so each rank bounds its own
+share of the subproblems (weak scaling, no data-path collective); time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import faulthandler
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from parallel_biqbin_maxcut_b200 import _lib, instances  # noqa: E402
+
+NV = 100
+N_SUB = 512
+KMAX = 40
+TRI_PER_N = 3
+METRIC = "B&B nodes/s & time-to-optimality: batched+learned vs plain GPU, bounds ±1e-6 rel"
+WORKLOAD = "G(100,0.5) ±1 weights; 512 subproblems, k~U[0,40] fixed (n=60..100); TriIneq=3n"
+# Algorithmic flops of one IPM iteration at size n (the dense work of
+# src/ipm_mc_pk.c per iteration: two SYMMs 4n^3, POTRF+POTRI of Z n^3,
+# Cholesky of Zi.*X n^3/3 (reused for both solves), two line-search
+# Cholesky factorizations 2n^3/3): 6.0 n^3; the reference's count with its
+# second POSV is 6.33 n^3.  The smaller count is used.
+FLOP_PER_ITER_N3 = 6.0
+
+
+def workload():
+    A = instances.gnp_pm1(NV, 0.5, seed=1)
+    subs = instances.random_fixings(NV, N_SUB, KMAX, seed=2)
+    return np.ascontiguousarray(A), subs
+
+
+def workload_params() -> dict:
+    p = dict(_lib.PARAMS_FILE)
+    p.update(adjust_TriIneq=0, TriIneq=TRI_PER_N * NV)
+    return p
+
+
+def peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained", d["bf16_tflops"]),
+                "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "source": "fallback"}
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_node(xf, sol) -> _lib.BabNode:
+    nd = _lib.BabNode()
+    nd.xfixed[: len(xf)] = [int(v) for v in xf]
+    nd.sol[: len(sol)] = [int(v) for v in sol]
+    nd.level = int(np.sum(xf))
+    return nd
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+class GpuArm:
+    def __init__(self, device: int):
+        import torch
+        self.torch = torch
+        self.lib = lib = _lib.load()
+        assert lib.bqb_init(device) == 0, lib.bqb_last_error()
+        self.device = device
+        self.A, self.subs = workload()
+        self.N0 = self.A.shape[0]
+        _lib.set_params(lib, _lib.make_params(**workload_params()))
+        lib.process_adj_matrix(_lib.dptr(self.A.copy()), self.N0)
+        self.glob = _lib.GlobalArrays(lib, self.N0)
+        self.babsol = (C.c_int * _lib.NMAX)()
+        C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(self.babsol)
+        self.SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+        self.PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
+        # keep the host address as an integer: a pointer read from a ctypes
+        # structure field aliases the field itself
+        self.PP_L_host = C.cast(self.PP.contents.L, C.c_void_p).value
+        C.CDLL("libc.so.6").srand(2020)
+        root = _lib.BabNode()
+        self.root_bound = lib.Evaluate(C.byref(root), self.SP, self.PP, 0)
+        self.lb = lib.Bab_LBGet()
+        self.nodes = [make_node(xf, sol) for xf, sol in self.subs]
+        # device-resident subproblem matrices (PP->L of every node)
+        self.n = []
+        self.dL = []
+        tmp = np.zeros(self.N0 * self.N0)
+        for nd in self.nodes:
+            self.PP.contents.L = tmp.ctypes.data_as(C.POINTER(C.c_double))
+            lib.createSubproblem(C.byref(nd), self.SP, self.PP)
+            n = self.PP.contents.n
+            t = torch.from_numpy(tmp[: n * n].copy()).to(f"cuda:{device}")
+            self.n.append(n)
+            self.dL.append(t)
+        self.restore_host_L()
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+        torch.cuda.synchronize()
+
+    def bound_device(self, idx):
+        """value leg: SDPbound with PP->L resident in HBM."""
+        lib, PP = self.lib, self.PP.contents
+        for i in idx:
+            PP.n = self.n[i]
+            PP.L = C.cast(C.c_void_p(self.dL[i].data_ptr()), C.POINTER(C.c_double))
+            lib.SDPbound(C.byref(self.nodes[i]), self.SP, self.PP, 1)
+        self.restore_host_L()
+
+    def restore_host_L(self):
+        self.PP.contents.L = C.cast(C.c_void_p(self.PP_L_host), C.POINTER(C.c_double))
+        assert C.cast(self.PP.contents.L, C.c_void_p).value == self.PP_L_host
+
+    def bound_e2e(self, idx):
+        """e2e leg: the reference-facing Evaluate with host buffers."""
+        lib = self.lib
+        return [lib.Evaluate(C.byref(self.nodes[i]), self.SP, self.PP, 1) for i in idx]
+
+    def l2_flush(self):
+        self.flush.zero_()
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_gpu(args):
+    import torch
+    ws, rank, local = _dist()
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    arm = GpuArm(local)
+    B = args.nodes_per_step
+    # rank r bounds its own slice: weak scaling (per-GPU work fixed)
+    order = [(rank * B + q) % N_SUB for q in range(B * (args.warmup + args.steps))]
+    order = [(i * 7919 + rank * 131) % N_SUB for i in range(len(order))]
+
+    def batches(start):
+        for s in range(start, start + args.steps):
+            yield order[s * B:(s + 1) * B]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    for s in range(args.warmup):
+        arm.bound_device(order[s * B:(s + 1) * B])
+    stream = torch.cuda.ExternalStream(arm.lib.bqb_stream())
+
+    # ---- value: device-resident inputs ----
+    arm.lib.bqb_stats_reset()
+    arm.lib.bqb_stats_enable(1)
+    clocks = ClockSampler(local)
+    launches0 = arm.lib.bqb_kernel_launches()
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for b in batches(args.warmup):
+        arm.l2_flush()
+        arm.bound_device(b)
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    launches = arm.lib.bqb_kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    stats = (C.c_double * 6)()
+    arm.lib.bqb_ipm_stats(stats)
+    arm.lib.bqb_stats_enable(0)
+    ms_max = max_over_ranks(ms)
+    total_nodes = B * args.steps * ws
+    value = total_nodes / (ms_max / 1e3)
+
+    # ---- e2e: host buffers through Evaluate ----
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    bounds = []
+    for b in batches(args.warmup):
+        arm.l2_flush()
+        bounds += arm.bound_e2e(b)
+    t1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(t0.elapsed_time(t1))
+    e2e = total_nodes / (ms_e2e / 1e3)
+    h2d = sum(arm.n[i] ** 2 * 8 + 2 * 4 * (NV - 1) for i in order[args.warmup * B:(args.warmup + 1) * B])
+    d2h = B * 8
+
+    pk = peaks()
+    kernel_ms = stats[4]
+    flops = FLOP_PER_ITER_N3 * stats[0]
+    achieved = flops / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else 0.0
+    peak = pk["bf16_tflops_sustained"]
+    roof = {"kernel": "ipm_one_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
+                           f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
+            "launches": int(stats[5]), "avg_launch_us": 1e3 * kernel_ms / max(stats[5], 1),
+            "ipm_iterations": int(stats[2]), "ipm_problems": int(stats[1]),
+            "linesearch_factorizations": int(stats[3]),
+            "flop_per_iteration": f"{FLOP_PER_ITER_N3} n^3",
+            "kernel_time_share": kernel_ms / ms if ms > 0 else None}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nodes_per_step": B, "nodes_per_step_total": B * ws,
+                       "l2": "flushed (256 MB write) before every step", "precision": "FP64 throughout",
+                       "mode": "plain GPU drop-in (one node at a time)", "root_bound": arm.root_bound,
+                       "incumbent": arm.lb, "parallelism": f"replicas over nodes x{ws}"},
+            "e2e": {"value": e2e, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
+# reference (CPU) arm -- the reference's own code, oracle/_ref
+# --------------------------------------------------------------------------
+def _ref_worker(conn, wid, nworkers):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    from oracle import refbind
+    A, subs = workload()
+    ref = refbind.RefLib()
+    ref.setup(A, workload_params())
+    L = ref.lib
+    SP = C.pointer(ref.problem("SP"))
+    PP = C.pointer(ref.problem("PP"))
+    C.CDLL("libc.so.6").srand(2020)
+    root = refbind.BabNode()
+    L.Evaluate(C.byref(root), SP, PP, 0)
+    conn.send(("ready", L.Bab_LBGet()))
+    while True:
+        msg = conn.recv()
+        if msg is None:
+            break
+        idx = msg
+        t0 = time.perf_counter()
+        for i in idx:
+            xf, sol = subs[i]
+            nd = refbind.BabNode()
+            nd.xfixed[: len(xf)] = [int(v) for v in xf]
+            nd.sol[: len(sol)] = [int(v) for v in sol]
+            L.Evaluate(C.byref(nd), SP, PP, 1)
+        conn.send(("done", time.perf_counter() - t0))
+
+
+class RefPool:
+    def __init__(self, nworkers: int):
+        ctx = mp.get_context("spawn")
+        self.conns, self.procs = [], []
+        for w in range(nworkers):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_ref_worker, args=(b, w, nworkers), daemon=True)
+            p.start()
+            self.conns.append(a)
+            self.procs.append(p)
+        self.lbs = [c.recv()[1] for c in self.conns]
+
+    def run(self, assignments):
+        for c, idx in zip(self.conns, assignments):
+            c.send(idx)
+        return [c.recv()[1] for c in self.conns]
+
+    def close(self):
+        for c in self.conns:
+            c.send(None)
+        for p in self.procs:
+            p.join(timeout=10)
+
+
+def cpu_baseline(seconds: float) -> dict:
+    """One core, the reference's Evaluate on a bounded sample of the workload."""
+    from oracle import refbind
+    if not refbind.available():
+        return {"value": None, "unit": "nodes/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    pool = RefPool(1)
+    done, t = 0, 0.0
+    i = 0
+    while t < seconds and done < N_SUB:
+        idx = [(i * 7919) % N_SUB, ((i + 1) * 7919) % N_SUB]
+        t += pool.run([idx])[0]
+        done += 2
+        i += 2
+    pool.close()
+    return {"value": done / t, "unit": "nodes/s", "cores": 1, "kind": "reference",
+            "sample": f"{done} of the 512 subproblems, same root state, serial reference build "
+                      f"(-O3 -ffast-math, OpenBLAS 1 thread), {t:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from oracle import refbind
+    if not refbind.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources)"}))
+        return
+    P = max(1, min(os.cpu_count() or 1, args.ref_procs))
+    per = max(1, args.ref_nodes_per_proc)
+    pool = RefPool(P)
+    step = 0
+
+    def assign(s):
+        base = s * P * per
+        return [[((base + w * per + q) * 7919) % N_SUB for q in range(per)] for w in range(P)]
+
+    for _ in range(args.warmup):
+        pool.run(assign(step))
+        step += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pool.run(assign(step))
+        step += 1
+    wall = time.perf_counter() - t0
+    pool.close()
+    nodes = P * per * args.steps
+    v = nodes / wall
+    line = {"metric": METRIC, "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "nodes_per_step": P * per, "processes": P},
+            "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": P, "kind": "reference",
+                             "sample": f"{P * per} subproblems per step ({per} per process), {P} processes"},
+            "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--nodes-per-step", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--ref-nodes-per-proc", type=int, default=1)
+    args = ap.parse_args()
+    faulthandler.enable(all_threads=True)
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

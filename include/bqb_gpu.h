@@ -166,7 +166,49 @@ double GW_heuristic(double *P0_L, int P0_N, double *P_L, int P_N, int *node_xfix
 double mc_1opt(int *x, double *P_L, int P_N);
 int update_best(int *xbest, int *xnew, double *best, int P0_N);
 
+/* Node bound orchestrator, src/bounding.c:24 (biqbin.h:142), with all
+ * matrices resident on the device; reads/writes the same globals. */
+double SDPbound(BabNode *node, Problem *SP, Problem *PP, int rank);
+
+/* Host B&B pieces the bound calls (restated for standalone use; a host
+ * program's own definitions take precedence): src/evaluate.c:11,38,123,
+ * src/bab_functions.c:96,114,387,425, src/heap.c:15,185,
+ * src/process_input.c:201,259. */
+double Evaluate(BabNode *node, Problem *SP, Problem *PP, int rank);
+void createSubproblem(BabNode *node, Problem *SP, Problem *PP);
+double getFixedValue(BabNode *node, Problem *SP);
+double evaluateSolution(int *sol);
+int updateSolution(int *x);
+int getBranchingVariable(BabNode *node);
+int countFixedVariables(BabNode *node);
+double Bab_LBGet(void);
+int Bab_LBUpd(double new_lb, BabSolution *bs);
+int Bab_numEvalNodes(void);
+double *readData(const char *instance, int *adj_N);
+int process_adj_matrix(double *Adj, int Adj_N);
+
 /* ==== Part 2: additions =============================================== */
+
+/* Parameters: header defaults (src/biqbin.h:49-78) and a params-file
+ * reader ("name = value" lines, src/process_input.c:158-197). */
+void bqb_default_params(BiqBinParameters *p);
+int bqb_read_params(const char *path, BiqBinParameters *p);
+
+/* Standalone solver: serial best-first B&B to optimality with every node
+ * bounded on the GPU.  adj: num_vertices x num_vertices symmetric integer
+ * weights; the last vertex is fixed to 0 as in the reference.  prm NULL
+ * means the reference's shipped `params` file values.  rand() is seeded
+ * with 2020 as the reference's Bab_Init does. */
+typedef struct bqb_solve_result {
+    double best_value;      /* "Maximum value" */
+    double root_bound;      /* "Root node bound" */
+    int nodes;              /* evaluated B&B nodes */
+    int stopped;            /* time limit reached */
+    double seconds;         /* wall time of the B&B */
+    int num_vertices;
+    int solution[BQB_NMAX]; /* 0/1 per vertex (vertex i+1 in the cut set if 1) */
+} bqb_solve_result;
+int bqb_solve(const double *adj, int num_vertices, const BiqBinParameters *prm, bqb_solve_result *out);
 
 /* Bind the library to a CUDA device (default 0) and create its stream.
  * Called implicitly by every entry point; returns 0 on success. */
@@ -179,6 +221,14 @@ const char *bqb_last_error(void);
 void bqb_set_abort_hook(void (*hook)(int code));
 /* Number of CUDA kernels this library has launched so far. */
 unsigned long long bqb_kernel_launches(void);
+/* The library's CUDA stream (a cudaStream_t). */
+void *bqb_stream(void);
+/* IPM work and time counters: enable per-launch CUDA-event timing, reset,
+ * read out[6] = {sum(iterations * n^3), problems, iterations, line-search
+ * factorizations, kernel milliseconds, timed launches}. */
+void bqb_stats_enable(int on);
+void bqb_stats_reset(void);
+void bqb_ipm_stats(double *out);
 /* Wait for all work the library queued. */
 void bqb_synchronize(void);
 

@@ -92,9 +92,29 @@ SIGNATURES = {
     "GW_heuristic": (C.c_double, [D, C.c_int, D, C.c_int, I, I, I, C.c_int]),
     "mc_1opt": (C.c_double, [I, D, C.c_int]),
     "update_best": (C.c_int, [I, I, D, C.c_int]),
+    "SDPbound": (C.c_double, [C.POINTER(BabNode), C.POINTER(Problem), C.POINTER(Problem), C.c_int]),
+    "Evaluate": (C.c_double, [C.POINTER(BabNode), C.POINTER(Problem), C.POINTER(Problem), C.c_int]),
+    "createSubproblem": (None, [C.POINTER(BabNode), C.POINTER(Problem), C.POINTER(Problem)]),
+    "getFixedValue": (C.c_double, [C.POINTER(BabNode), C.POINTER(Problem)]),
+    "evaluateSolution": (C.c_double, [I]),
+    "updateSolution": (C.c_int, [I]),
+    "getBranchingVariable": (C.c_int, [C.POINTER(BabNode)]),
+    "countFixedVariables": (C.c_int, [C.POINTER(BabNode)]),
+    "Bab_LBGet": (C.c_double, []),
+    "Bab_LBUpd": (C.c_int, [C.c_double, C.c_void_p]),
+    "Bab_numEvalNodes": (C.c_int, []),
+    "readData": (C.POINTER(C.c_double), [C.c_char_p, I]),
+    "process_adj_matrix": (C.c_int, [D, C.c_int]),
+    "bqb_default_params": (None, [C.POINTER(Params)]),
+    "bqb_read_params": (C.c_int, [C.c_char_p, C.POINTER(Params)]),
+    "bqb_solve": (C.c_int, [D, C.c_int, C.c_void_p, C.c_void_p]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),
     "bqb_kernel_launches": (C.c_ulonglong, []),
+    "bqb_stream": (C.c_void_p, []),
+    "bqb_stats_enable": (None, [C.c_int]),
+    "bqb_stats_reset": (None, []),
+    "bqb_ipm_stats": (None, [D]),
     "bqb_synchronize": (None, []),
     "bqb_ipm_plan_create": (C.c_void_p, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), I, C.c_int,
                                          C.c_void_p]),
@@ -151,3 +171,72 @@ def from_colmajor(flat: np.ndarray, n: int) -> np.ndarray:
 def global_ptr(name: str, ctype):
     """The library's own copy of a reference global (standalone use)."""
     return ctype.in_dll(load(), name)
+
+
+class SolveResult(C.Structure):
+    """bqb_solve_result (include/bqb_gpu.h)."""
+    _fields_ = [("best_value", C.c_double), ("root_bound", C.c_double), ("nodes", C.c_int),
+                ("stopped", C.c_int), ("seconds", C.c_double), ("num_vertices", C.c_int),
+                ("solution", C.c_int * NMAX)]
+
+
+def make_params(**overrides) -> Params:
+    """Parameters as the reference tests run them (its shipped `params` file),
+    with overrides."""
+    p = Params()
+    vals = dict(PARAMS_FILE)
+    vals.update(overrides)
+    for k, v in vals.items():
+        setattr(p, k, v)
+    return p
+
+
+def solve(adj: np.ndarray, **param_overrides) -> dict:
+    """Solve Max-Cut on ``adj`` to optimality (serial B&B, GPU bounding)."""
+    lib = load()
+    A = np.ascontiguousarray(adj, dtype=np.float64)
+    p = make_params(**param_overrides)
+    res = SolveResult()
+    rc = lib.bqb_solve(dptr(A), A.shape[0], C.cast(C.pointer(p), C.c_void_p),
+                       C.cast(C.pointer(res), C.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"bqb_solve failed: {lib.bqb_last_error().decode()}")
+    nv = A.shape[0]
+    sol = np.array(res.solution[: nv - 1], dtype=np.int32)
+    return dict(best_value=res.best_value, root_bound=res.root_bound, nodes=res.nodes,
+                seconds=res.seconds, stopped=bool(res.stopped), x=sol,
+                solution=[i + 1 for i in range(nv - 1) if sol[i] == 1])
+
+
+class GlobalArrays:
+    """Allocates the reference-layout globals in a library (X, Z, X_test,
+    dual_gamma, ..., cut arrays) and points the library's pointer globals at
+    them, as src/allocate_free.c:8-42 does.  Keeps the buffers alive."""
+
+    def __init__(self, cdll, N: int, bundle_cap: int = 64, mmax: int = 20000, list_cap: int = 20000):
+        self.cdll = cdll
+        self.N = N
+        dbl = {"X": N * N, "Z": N * N, "X_test": N * N, "X_bundle": N * N * bundle_cap,
+               "dual_gamma": mmax, "dgamma": mmax, "gamma_test": mmax, "eta": mmax, "g": mmax,
+               "lambda": bundle_cap, "F": bundle_cap, "G": mmax * bundle_cap}
+        self.arr = {}
+        for name, size in dbl.items():
+            a = np.zeros(size)
+            self.arr[name] = a
+            C.c_void_p.in_dll(cdll, name).value = a.ctypes.data
+        self.cuts = (TriIneq * mmax)()
+        self.lst = (TriIneq * list_cap)()
+        self.pcuts = (PentIneq * mmax)()
+        self.plst = (PentIneq * list_cap)()
+        self.hcuts = (HeptIneq * mmax)()
+        self.hlst = (HeptIneq * list_cap)()
+        for name, obj in (("Cuts", self.cuts), ("List", self.lst), ("Pent_Cuts", self.pcuts),
+                          ("Pent_List", self.plst), ("Hepta_Cuts", self.hcuts), ("Hepta_List", self.hlst)):
+            C.c_void_p.in_dll(cdll, name).value = C.addressof(obj)
+
+    def __getitem__(self, name):
+        return self.arr[name]
+
+
+def set_params(cdll, p: Params) -> None:
+    Params.in_dll(cdll, "params").__init__(*[getattr(p, f) for f, _ in Params._fields_])

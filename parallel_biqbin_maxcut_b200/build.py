@@ -27,6 +27,16 @@ NVCC_FLAGS = ARCH + [
 ]
 
 
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+# Host-only C++ sources are compiled with g++.  host_sep.cpp restates the
+# reference's simulated annealing and takes the reference's floating-point
+# flags (-O3 -ffast-math, reference Makefile:17) so its accept/reject
+# decisions match the reference build.
+CXX_FLAGS = ["-O3", "-fPIC", "-fvisibility=hidden", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+             "-I" + os.path.join(CUDA_HOME, "include")]
+PER_FILE_FLAGS = {"host_sep.cpp": ["-ffast-math"]}
+
+
 def nvcc() -> str:
     for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
         if cand and os.path.exists(cand):
@@ -44,7 +54,10 @@ def _compile(src: str, hdr_mtime: float, extra: list[str]) -> str:
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_mtime):
         return obj
-    cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
+    if src.endswith(".cpp"):
+        cmd = ["g++"] + CXX_FLAGS + PER_FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
+    else:
+        cmd = [nvcc()] + NVCC_FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,475 @@
+// Host branch-and-bound runtime around the GPU bounding path, and a
+// standalone serial solver.
+//
+// Restated from the reference's host files so that the library can be used
+// on its own (the reference's own host objects, when linked against this
+// library, take precedence over every symbol defined here):
+//   heap.c         priority queue on upper_bound, incumbent (LB, BabSol)
+//   bab_functions.c evaluateSolution, updateSolution, getBranchingVariable,
+//                  countFixedVariables, the worker step
+//   evaluate.c     Evaluate, createSubproblem, getFixedValue
+//   process_input.c process_adj_matrix (SP->L from an adjacency matrix),
+//                  the Rudy reader and the parameter-file reader
+// The driver is serial and best-first: the root is bounded with rank 0
+// (recording diff), its two children are queued, then nodes are popped and
+// bounded with rank 1 (so the use_diff give-up test applies), as one worker
+// of the reference's MPI code does when it never finds a free peer.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <vector>
+
+#include "globals.h"
+
+extern "C" {
+double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank);
+__attribute__((visibility("default"))) double diff = 0.0;
+__attribute__((visibility("default"))) double root_bound = 0.0;
+__attribute__((visibility("default"))) double TIME = 0.0;
+__attribute__((visibility("default"))) int stopped = 0;
+__attribute__((visibility("default"))) BabSolution* BabSol = nullptr;
+}
+
+namespace {
+
+constexpr double BIG_NUMBER = 1e9;
+double g_LB = 0.0;
+int g_num_nodes = 0;
+
+double wtime()
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+// Binary max-heap on upper_bound with the reference's comparison and
+// sift rules (src/heap.c:27-133).
+struct NodeHeap {
+    std::vector<BabNode*> data;
+    int used = 0;
+    static int cmp(const BabNode* a, const BabNode* b) { return a->upper_bound > b->upper_bound ? 1 : -1; }
+    void swap_e(int i, int j)
+    {
+        BabNode* t = data[i];
+        data[i] = data[j];
+        data[j] = t;
+    }
+    void down(int cur)
+    {
+        int child = 2 * cur + 1;
+        if (child + 1 < used && cmp(data[child + 1], data[child]) > 0) child++;
+        while (child < used && cmp(data[cur], data[child]) < 0) {
+            swap_e(cur, child);
+            cur = child;
+            child = 2 * cur + 1;
+            if (child + 1 < used && cmp(data[child + 1], data[child]) > 0) child++;
+        }
+    }
+    void up(int cur)
+    {
+        int parent = (cur - 1) / 2;
+        while (cur > 0 && cmp(data[parent], data[cur]) < 0) {
+            swap_e(cur, parent);
+            cur = parent;
+            parent = (cur - 1) / 2;
+        }
+    }
+    void push(BabNode* n)
+    {
+        if ((int)data.size() <= used) data.resize(used + 64, nullptr);
+        data[used++] = n;
+        up(used - 1);
+    }
+    BabNode* pop()
+    {
+        BabNode* n = data[0];
+        data[0] = nullptr;
+        used--;
+        swap_e(0, used);
+        down(0);
+        return n;
+    }
+    bool empty() const { return used == 0; }
+};
+
+BabNode* new_node(const BabNode* parent)
+{
+    BabNode* node = (BabNode*)malloc(sizeof(BabNode));
+    if (!node) {
+        fprintf(stderr, "Error: Not enough memory for creating new node.\n");
+        exit(10);
+    }
+    for (int i = 0; i < BabPbSize; ++i) {
+        node->xfixed[i] = parent ? parent->xfixed[i] : 0;
+        node->sol.X[i] = (parent && node->xfixed[i]) ? parent->sol.X[i] : 0;
+    }
+    node->level = parent ? parent->level + 1 : 0;
+    node->upper_bound = 0.0;
+    return node;
+}
+
+}  // namespace
+
+// ---- incumbent (src/heap.c:15, 172-193) -----------------------------------
+BQB_API double Bab_LBGet(void) { return g_LB; }
+
+BQB_API int Bab_LBUpd(double new_lb, BabSolution* bs)
+{
+    if (new_lb > g_LB) {
+        g_LB = new_lb;
+        if (BabSol) *BabSol = *bs;
+        return 1;
+    }
+    return 0;
+}
+
+BQB_API int Bab_numEvalNodes(void) { return g_num_nodes; }
+
+// ---- src/bab_functions.c:96-134 --------------------------------------------
+BQB_API double evaluateSolution(int* sol)
+{
+    double val = 0.0;
+    for (int i = 0; i < BabPbSize; ++i)
+        for (int j = 0; j < BabPbSize; ++j) val += SP->L[j + (size_t)i * SP->n] * sol[i] * sol[j];
+    return val;
+}
+
+BQB_API int updateSolution(int* x)
+{
+    BabSolution solx;
+    for (int i = 0; i < BabPbSize; ++i) solx.X[i] = x[i];
+    const double v = evaluateSolution(x);
+    return Bab_LBUpd(v, &solx);
+}
+
+// ---- src/bab_functions.c:387-436 -------------------------------------------
+BQB_API int countFixedVariables(BabNode* node)
+{
+    int c = 0;
+    for (int i = 0; i < BabPbSize; ++i) c += node->xfixed[i] ? 1 : 0;
+    return c;
+}
+
+BQB_API int getBranchingVariable(BabNode* node)
+{
+    int ic = -1;
+    if (params.branchingStrategy == 0) {   // LEAST_FRACTIONAL
+        double maxv = -BIG_NUMBER;
+        for (int i = 0; i < BabPbSize; ++i)
+            if (!node->xfixed[i] && fabs(0.5 - node->fracsol[i]) > maxv) {
+                ic = i;
+                maxv = fabs(0.5 - node->fracsol[ic]);
+            }
+    } else if (params.branchingStrategy == 1) {   // MOST_FRACTIONAL
+        double minv = BIG_NUMBER;
+        for (int i = 0; i < BabPbSize; ++i)
+            if (!node->xfixed[i] && fabs(0.5 - node->fracsol[i]) < minv) {
+                ic = i;
+                minv = fabs(0.5 - node->fracsol[ic]);
+            }
+    } else {
+        fprintf(stderr, "Error: Wrong value for params.branchingStrategy\n");
+        exit(10);
+    }
+    return ic;
+}
+
+// ---- src/evaluate.c:38-138 --------------------------------------------------
+BQB_API void createSubproblem(BabNode* node, Problem* SP_, Problem* PP_)
+{
+    PP_->n = BabPbSize + 1 - countFixedVariables(node);
+    const int N = SP_->n;
+    const int n = PP_->n;
+    std::vector<double> fixedRow(n > 1 ? n - 1 : 1, 0.0);
+    int index = 0;
+    for (int i = 0; i < BabPbSize; ++i) {
+        double row_sum = 0.0;
+        int fixed = 0;
+        for (int j = 0; j < BabPbSize; ++j) {
+            if (!node->xfixed[i] && !node->xfixed[j]) {
+                PP_->L[index] = SP_->L[j + (size_t)i * N];
+                row_sum += PP_->L[index];
+                ++index;
+            } else if ((node->xfixed[i] && node->sol.X[i] == 1) && !node->xfixed[j]) {
+                fixedRow[fixed] += SP_->L[j + (size_t)i * N];
+                ++fixed;
+            }
+        }
+        if (!node->xfixed[i]) PP_->L[index++] = row_sum;
+    }
+    for (int i = 0; i < n - 1; ++i) PP_->L[i + (size_t)(n - 1) * n] = PP_->L[n - 1 + (size_t)i * n];
+    double sum = 0.0;
+    for (int i = 0; i < n - 1; ++i) {
+        PP_->L[i + (size_t)i * n] += 2 * fixedRow[i];
+        PP_->L[n - 1 + (size_t)i * n] += 2 * fixedRow[i];
+        PP_->L[i + (size_t)(n - 1) * n] += 2 * fixedRow[i];
+        sum += PP_->L[i + (size_t)(n - 1) * n];
+    }
+    PP_->L[n - 1 + (size_t)(n - 1) * n] = sum;
+    const size_t nn = (size_t)n * n;
+    for (size_t e = 0; e < nn; ++e) PP_->L[e] *= 0.25;
+}
+
+BQB_API double getFixedValue(BabNode* node, Problem* SP_)
+{
+    const int N = SP_->n;
+    double v = 0.0;
+    for (int i = 0; i < BabPbSize; ++i)
+        for (int j = 0; j < BabPbSize; ++j)
+            if (node->xfixed[i] && node->xfixed[j]) v += SP_->L[j + (size_t)i * N] * node->sol.X[i] * node->sol.X[j];
+    return v;
+}
+
+BQB_API double Evaluate(BabNode* node, Problem* SP_, Problem* PP_, int rank)
+{
+    createSubproblem(node, SP_, PP_);
+    return SDPbound(node, SP_, PP_, rank);
+}
+
+// ---- src/process_input.c:259-344 --------------------------------------------
+BQB_API int process_adj_matrix(double* Adj, int num_vertices)
+{
+    BabPbSize = num_vertices - 1;
+    if (!SP) SP = (Problem*)calloc(1, sizeof(Problem));
+    if (!PP) PP = (Problem*)calloc(1, sizeof(Problem));
+    SP->n = num_vertices;
+    free(SP->L);
+    free(PP->L);
+    SP->L = (double*)calloc((size_t)num_vertices * num_vertices, sizeof(double));
+    PP->L = (double*)calloc((size_t)num_vertices * num_vertices, sizeof(double));
+    PP->n = SP->n;
+    const int nv = num_vertices;
+    std::vector<double> Adje(nv, 0.0);
+    for (int ii = 0; ii < nv; ++ii)
+        for (int jj = 0; jj < nv; ++jj) Adje[ii] += Adj[jj + (size_t)ii * nv];
+    double sum = 0.0;
+    for (int ii = 0; ii < nv; ++ii) {
+        double sum_row = 0.0;
+        for (int jj = 0; jj < nv; ++jj) {
+            const size_t e = jj + (size_t)ii * nv;
+            if (ii < nv - 1 && jj < nv - 1) {
+                SP->L[e] = (ii == jj ? Adje[ii] : 0.0) - Adj[e];
+                sum_row += SP->L[e];
+            } else if (jj == nv - 1 && ii != nv - 1) {
+                SP->L[e] = sum_row;
+                sum += sum_row;
+            } else if (ii == nv - 1 && jj != nv - 1) {
+                SP->L[e] = SP->L[ii + (size_t)jj * nv];
+            } else {
+                SP->L[e] = sum;
+            }
+        }
+    }
+    memcpy(PP->L, SP->L, (size_t)nv * nv * sizeof(double));
+    return 0;
+}
+
+// Rudy edge list: "n m" then m lines "i j w" (1-based, integer weights),
+// src/process_input.c:201-253.  Returns a calloc'd n x n matrix or NULL.
+BQB_API double* readData(const char* instance, int* adj_N)
+{
+    FILE* fh = fopen(instance, "r");
+    if (!fh) {
+        fprintf(stderr, "Error: problem opening input file %s\n", instance);
+        return nullptr;
+    }
+    int nv = 0, ne = 0;
+    if (fscanf(fh, "%d %d \n", &nv, &ne) != 2 || nv <= 0) {
+        fprintf(stderr, "\nError: Problem reading number of vertices and edges\n");
+        fclose(fh);
+        return nullptr;
+    }
+    double* A = (double*)calloc((size_t)nv * nv, sizeof(double));
+    for (int e = 0; e < ne; ++e) {
+        int i, j;
+        double w;
+        if (fscanf(fh, "%d %d %lf \n", &i, &j, &w) != 3 || i < 1 || i > nv || j < 1 || j > nv ||
+            (double)(int)w != w) {
+            fprintf(stderr, "\nError: Problem reading edges of the graph\n");
+            fclose(fh);
+            free(A);
+            return nullptr;
+        }
+        A[(size_t)nv * (j - 1) + (i - 1)] = w;
+        A[(size_t)nv * (i - 1) + (j - 1)] = w;
+    }
+    fclose(fh);
+    *adj_N = nv;
+    return A;
+}
+
+// Parameter defaults of src/biqbin.h:49-78.
+BQB_API void bqb_default_params(BiqBinParameters* p)
+{
+    p->init_bundle_iter = 3;
+    p->max_bundle_iter = 15;
+    p->triag_iter = 5;
+    p->pent_iter = 5;
+    p->hept_iter = 5;
+    p->max_outer_iter = 20;
+    p->extra_iter = 10;
+    p->violated_TriIneq = 1e-3;
+    p->TriIneq = 5000;
+    p->adjust_TriIneq = 1;
+    p->PentIneq = 5000;
+    p->HeptaIneq = 5000;
+    p->Pent_Trials = 60;
+    p->Hepta_Trials = 50;
+    p->include_Pent = 1;
+    p->include_Hepta = 1;
+    p->root = 0;
+    p->use_diff = 1;
+    p->time_limit = 0;
+    p->branchingStrategy = 1;
+}
+
+// "name = value" lines (src/process_input.c:158-197); unknown names ignored.
+BQB_API int bqb_read_params(const char* path, BiqBinParameters* p)
+{
+    bqb_default_params(p);
+    FILE* fh = fopen(path, "r");
+    if (!fh) return 1;
+    char line[256], name[64];
+    while (fgets(line, sizeof line, fh)) {
+        if (sscanf(line, "%63[^=^ ]", name) != 1) continue;
+        const char* eq = strchr(line, '=');
+        if (!eq) continue;
+        const double v = atof(eq + 1);
+#define BQB_PI(field) \
+    if (strcmp(name, #field) == 0) p->field = (int)v;
+#define BQB_PD(field) \
+    if (strcmp(name, #field) == 0) p->field = v;
+        BQB_PI(init_bundle_iter) BQB_PI(max_bundle_iter) BQB_PI(triag_iter) BQB_PI(pent_iter)
+        BQB_PI(hept_iter) BQB_PI(max_outer_iter) BQB_PI(extra_iter) BQB_PD(violated_TriIneq)
+        BQB_PI(TriIneq) BQB_PI(adjust_TriIneq) BQB_PI(PentIneq) BQB_PI(HeptaIneq)
+        BQB_PI(Pent_Trials) BQB_PI(Hepta_Trials) BQB_PI(include_Pent) BQB_PI(include_Hepta)
+        BQB_PI(root) BQB_PI(use_diff) BQB_PI(time_limit) BQB_PI(branchingStrategy)
+#undef BQB_PI
+#undef BQB_PD
+    }
+    fclose(fh);
+    return 0;
+}
+
+// Allocate the reference globals the bounding path reads on the host
+// (src/allocate_free.c:8-42).  X_bundle and G stay on the device in this
+// driver, so their host copies are not allocated.
+static void alloc_globals(int N)
+{
+    auto dalloc = [](size_t n) { return (double*)calloc(n, sizeof(double)); };
+    const size_t mmax = (size_t)BQB_MAX_TRI_INEQ + BQB_MAX_PENT_INEQ + BQB_MAX_HEPTA_INEQ;
+    free(Cuts);
+    free(List);
+    free(Pent_Cuts);
+    free(Pent_List);
+    free(Hepta_Cuts);
+    free(Hepta_List);
+    Cuts = (Triangle_Inequality*)calloc(BQB_MAX_TRI_INEQ, sizeof(Triangle_Inequality));
+    List = (Triangle_Inequality*)calloc(params.TriIneq > 0 ? params.TriIneq : 1, sizeof(Triangle_Inequality));
+    Pent_Cuts = (Pentagonal_Inequality*)calloc(BQB_MAX_PENT_INEQ, sizeof(Pentagonal_Inequality));
+    Pent_List = (Pentagonal_Inequality*)calloc(params.PentIneq > 0 ? params.PentIneq : 1,
+                                               sizeof(Pentagonal_Inequality));
+    Hepta_Cuts = (Heptagonal_Inequality*)calloc(BQB_MAX_HEPTA_INEQ, sizeof(Heptagonal_Inequality));
+    Hepta_List = (Heptagonal_Inequality*)calloc(params.HeptaIneq > 0 ? params.HeptaIneq : 1,
+                                                sizeof(Heptagonal_Inequality));
+    free(X);
+    free(Z);
+    free(X_test);
+    X = dalloc((size_t)N * N);
+    Z = dalloc((size_t)N * N);
+    X_test = dalloc((size_t)N * N);
+    free(dual_gamma);
+    free(dgamma);
+    free(gamma_test);
+    free(eta);
+    free(g);
+    free(lambda);
+    free(F);
+    dual_gamma = dalloc(mmax);
+    dgamma = dalloc(mmax);
+    gamma_test = dalloc(mmax);
+    eta = dalloc(mmax);
+    g = dalloc(mmax);
+    lambda = dalloc(BQB_MAX_BUNDLE);
+    F = dalloc(BQB_MAX_BUNDLE);
+}
+
+// Serial best-first B&B to optimality on the GPU bounding path.  adj:
+// num_vertices^2 symmetric integer weights (column-major = row-major);
+// prm: parameters (NULL: the reference's shipped `params` file values).
+// Seeds rand() with 2020 as Bab_Init does (src/bab_functions.c:82).
+BQB_API int bqb_solve(const double* adj, int num_vertices, const BiqBinParameters* prm, bqb_solve_result* out)
+{
+    if (num_vertices < 3 || num_vertices > BQB_NMAX) return 1;
+    if (prm) {
+        params = *prm;
+    } else {
+        bqb_default_params(&params);
+        params.init_bundle_iter = 5;
+        params.violated_TriIneq = 0.05;
+    }
+    std::vector<double> A(adj, adj + (size_t)num_vertices * num_vertices);
+    process_adj_matrix(A.data(), num_vertices);
+    if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
+    srand(2020);
+    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
+    memset(BabSol, 0, sizeof(BabSolution));
+    g_LB = 0.0;
+    g_num_nodes = 0;
+    stopped = 0;
+    diff = 0.0;
+    alloc_globals(SP->n);
+
+    TIME = wtime();
+    NodeHeap heap;
+    BabNode* root = new_node(nullptr);
+    ++g_num_nodes;
+    root_bound = Evaluate(root, SP, PP, 0);
+    root->upper_bound = root_bound;
+    if (Bab_LBGet() + 1.0 < root->upper_bound)
+        heap.push(root);
+    else
+        free(root);
+
+    auto branch = [&](BabNode* node) {
+        const int ic = getBranchingVariable(node);
+        for (int xic = 0; xic <= 1; ++xic) {
+            BabNode* child = new_node(node);
+            child->xfixed[ic] = 1;
+            child->sol.X[ic] = xic;
+            ++g_num_nodes;
+            heap.push(child);
+        }
+    };
+    if (!heap.empty() && !params.root) {
+        BabNode* node = heap.pop();
+        branch(node);
+        free(node);
+        while (!heap.empty()) {
+            if (params.time_limit > 0 && (wtime() - TIME) > params.time_limit) {
+                stopped = 1;
+                break;
+            }
+            BabNode* nd = heap.pop();
+            nd->upper_bound = Evaluate(nd, SP, PP, 1);
+            if (Bab_LBGet() + 1.0 < nd->upper_bound) branch(nd);
+            free(nd);
+        }
+    }
+    while (!heap.empty()) free(heap.pop());
+
+    if (out) {
+        out->best_value = Bab_LBGet();
+        out->root_bound = root_bound;
+        out->nodes = g_num_nodes;
+        out->stopped = stopped;
+        out->seconds = wtime() - TIME;
+        out->num_vertices = num_vertices;
+        for (int i = 0; i < BQB_NMAX; ++i) out->solution[i] = (i < BabPbSize) ? BabSol->X[i] : 0;
+    }
+    return 0;
+}

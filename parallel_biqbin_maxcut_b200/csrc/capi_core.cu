@@ -7,6 +7,7 @@
 
 #include "cuts.cuh"
 #include "globals.h"
+#include "internal.h"
 #include "ipm.cuh"
 
 namespace bqb {
@@ -41,7 +42,9 @@ CoreState& core()
     return s;
 }
 
-void check_ipm_status(const double* out)
+}  // namespace
+
+void check_ipm_status_host(const double* out)
 {
     const int status = (int)out[2];
     if (status == IPM_OK) return;
@@ -51,16 +54,16 @@ void check_ipm_status(const double* out)
                                                  : "iteration limit reached";
     fatal("ipm_mc_pk", msg);
 }
-}  // namespace
 
 // Device-level basic SDP bound for one problem (used by every caller).
-void ipm_device(const double* dL, double* dX, int n, double* dout, cudaStream_t s)
+// xslot (optional, device): write X into dX + (*xslot) * n * n.
+void ipm_device(const double* dL, double* dX, int n, double* dout, cudaStream_t s, const int* xslot)
 {
     CoreState& c = core();
     size_t bytes = 0;
     const int place = ipm_place(n, rt().smem_optin, &bytes);
     double* ws = c.ws.ensure(ipm_ws_doubles(n, place));
-    IpmDesc d{dL, dX, ws, dout, n, 0};
+    IpmDesc d{dL, dX, ws, dout, xslot, n, 0};
     ipm_launch_one(d, s);
 }
 
@@ -83,7 +86,7 @@ BQB_API void ipm_mc_pk(double* L, int n, double* Xout, double* phi, int print)
     BQB_CUDA(cudaMemcpyAsync(Xout, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaMemcpyAsync(hout, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaStreamSynchronize(R.stream));
-    check_ipm_status(hout);
+    check_ipm_status_host(hout);
     *phi = hout[0];
 }
 
@@ -167,7 +170,7 @@ BQB_API double fct_eval(const Problem* PP_, double* gam, double* Xout, double* g
     if (m > 0) BQB_CUDA(cudaMemcpyAsync(gout, dy, m * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaMemcpyAsync(hout, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaStreamSynchronize(R.stream));
-    check_ipm_status(hout);
+    check_ipm_status_host(hout);
     double fv = hout[0];
     // sum in index order, as src/bundle.c:264-265
     for (int i = 0; i < m; ++i) fv += gam[i];
@@ -198,7 +201,7 @@ BQB_API bqb_ipm_plan* bqb_ipm_plan_create(const double* const* Ls, double* const
     std::vector<IpmDesc> h(nprob > 0 ? nprob : 1);
     size_t off = 0;
     for (int i = 0; i < nprob; ++i) {
-        h[i] = IpmDesc{Ls[i], Xs[i], ws + off, out + 4 * (size_t)i, ns[i], 0};
+        h[i] = IpmDesc{Ls[i], Xs[i], ws + off, out + 4 * (size_t)i, nullptr, ns[i], 0};
         off += ipm_ws_doubles(ns[i], place);
     }
     IpmDesc* dd = p->descs.ensure(nprob > 0 ? nprob : 1);

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) opB_kernel(const CutRec* __restrict__ cut
             }
         }
     }
-    double* y = Y + c + (size_t)j * ldy;
+    double* y = Y + c + (size_t)(slot ? slot[j] : j) * ldy;
     const double y0 = init_one ? 1.0 : *y;
     if (k == 3)
         *y = y0 - acc;

@@ -44,9 +44,10 @@ struct DevCuts {
     void upload(const std::vector<CutRec>& cuts, int mt, int mp, int mh, cudaStream_t s);
 };
 
-// Y[c + j*ldy] = (init_one ? 1 : Y[c + j*ldy]) - B_c(X_j) for every cut c
-// and every matrix j < ncols; X_j = Xbase + slot[j] * ldx_mat (slot may be
-// null: slot[j] = j).  ld of every X_j is n.
+// Y[c + s_j*ldy] = (init_one ? 1 : Y[c + s_j*ldy]) - B_c(X_j) for every cut
+// c and every matrix j < ncols; X_j = Xbase + s_j * ldx_mat with
+// s_j = slot[j] (slot may be null: s_j = j).  ld of every X_j is n.  The
+// slot array lets the bundle address its physical matrix/column slots.
 void opB_launch(const DevCuts& dc, const double* Xbase, size_t ldx_mat, const int* slot, int ncols,
                 int n, double* Y, size_t ldy, bool init_one, cudaStream_t s);
 

@@ -21,172 +21,19 @@
 // triangle; its pivots are the Schur complements of Z, so a non-positive
 // pivot is exactly "Z not positive definite".
 #include "ipm.cuh"
+#include "cta_linalg.cuh"
 
 #include <math.h>
 
+#include <vector>
+
 namespace bqb {
+
+// Work counters for the roofline: [0] sum over finished problems of
+// iterations * n^3, [1] problems, [2] iterations, [3] line-search trials.
+__device__ double g_ipm_stats[4];
+
 namespace {
-
-// Cholesky of the lower triangle of A (in place).  Returns false, uniformly
-// over the block, at the first non-positive pivot (the line-search test).
-__device__ bool cta_potrf_lower(double* A, int n, int ld, double* col)
-{
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int k = 0; k < n; ++k) {
-        const double d = A[k + (size_t)k * ld];
-        if (!(d > 0.0)) return false;
-        const double s = sqrt(d);
-        const double inv = 1.0 / s;
-        for (int i = k + 1 + tid; i < n; i += nt) {
-            const double v = A[i + (size_t)k * ld] * inv;
-            col[i] = v;
-            A[i + (size_t)k * ld] = v;
-        }
-        __syncthreads();
-        if (tid == 0) A[k + (size_t)k * ld] = s;
-        for (int j = k + 1 + warp; j < n; j += nw) {
-            const double cj = col[j];
-            double* Aj = A + (size_t)j * ld;
-            for (int i = j + lane; i < n; i += 32) Aj[i] = fma(-col[i], cj, Aj[i]);
-        }
-        __syncthreads();
-    }
-    return true;
-}
-
-// In-place inverse of a symmetric positive definite matrix held in the lower
-// triangle (symmetric sweep / Gauss-Jordan without pivoting).  On success A
-// holds the full symmetric inverse (both triangles).
-__device__ bool cta_spd_inverse(double* A, int n, int ld, double* col)
-{
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    for (int k = 0; k < n; ++k) {
-        const double d = A[k + (size_t)k * ld];
-        if (!(d > 0.0)) return false;
-        for (int i = tid; i < n; i += nt)
-            col[i] = (i >= k) ? A[i + (size_t)k * ld] : A[k + (size_t)i * ld];
-        __syncthreads();
-        const double inv = 1.0 / d;
-        for (int j = warp; j < n; j += nw) {
-            double* Aj = A + (size_t)j * ld;
-            if (j == k) {
-                for (int i = j + lane; i < n; i += 32) Aj[i] = (i == k) ? -inv : col[i] * inv;
-            } else {
-                const double tj = col[j] * inv;
-                for (int i = j + lane; i < n; i += 32)
-                    Aj[i] = (i == k) ? tj : fma(-col[i], tj, Aj[i]);
-            }
-        }
-        __syncthreads();
-    }
-    // the sweep leaves -inv(A); negate and mirror to the upper triangle
-    for (int j = warp; j < n; j += nw) {
-        for (int i = j + lane; i < n; i += 32) {
-            const double v = -A[i + (size_t)j * ld];
-            A[i + (size_t)j * ld] = v;
-            A[j + (size_t)i * ld] = v;
-        }
-    }
-    __syncthreads();
-    return true;
-}
-
-// Solve (F F^T) x = b with F the lower Cholesky factor; one warp; b in smem.
-__device__ void warp_chol_solve(const double* F, int n, int ld, double* b)
-{
-    const int lane = threadIdx.x & 31;
-    for (int k = 0; k < n; ++k) {
-        const double bk = b[k] / F[k + (size_t)k * ld];
-        __syncwarp();
-        if (lane == 0) b[k] = bk;
-        const double* Fk = F + (size_t)k * ld;
-        for (int i = k + 1 + lane; i < n; i += 32) b[i] = fma(-Fk[i], bk, b[i]);
-        __syncwarp();
-    }
-    for (int k = n - 1; k >= 0; --k) {
-        const double xk = b[k] / F[k + (size_t)k * ld];
-        __syncwarp();
-        if (lane == 0) b[k] = xk;
-        for (int i = lane; i < k; i += 32) b[i] = fma(-F[k + (size_t)i * ld], xk, b[i]);
-        __syncwarp();
-    }
-}
-
-// Exact symmetrisation A = (A + A^T)/2 as the reference writes it
-// (src/ipm_mc_pk.c:196-199): both entries get 0.5*(a_ij + a_ji).
-__device__ void cta_symmetrize(double* A, int n)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int j = warp; j < n; j += nw) {
-        for (int i = j + 1 + lane; i < n; i += 32) {
-            const double v = 0.5 * (A[j + (size_t)i * n] + A[i + (size_t)j * n]);
-            A[i + (size_t)j * n] = v;
-            A[j + (size_t)i * n] = v;
-        }
-    }
-    __syncthreads();
-}
-
-// C = A * B' with A (n x n, column-major, read in place) and B'(k, c) formed
-// on the fly by `bfun` and staged through shared memory in k-chunks.  Each
-// thread owns a 4 x 8 register tile of a 128 x 128 supertile.  The k sum is
-// sequential, so results are deterministic.  `epi(r, c, acc)` stores.
-constexpr int STG_LD = IPM_TILE + 1;
-
-template <class BF, class EF>
-__device__ void cta_gemm(const double* A, int n, int lda, BF bfun, EF epi, double* stage)
-{
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int tr = tid & 31;
-    const int tc = tid >> 5;   // 0..15
-    for (int r0 = 0; r0 < n; r0 += IPM_TILE) {
-        for (int c0 = 0; c0 < n; c0 += IPM_TILE) {
-            double acc[4][8];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
-            for (int k0 = 0; k0 < n; k0 += IPM_KC) {
-                for (int e = tid; e < IPM_KC * IPM_TILE; e += nt) {
-                    const int kk = e % IPM_KC, cc = e / IPM_KC;
-                    const int k = k0 + kk, c = c0 + cc;
-                    stage[kk * STG_LD + cc] = (k < n && c < n) ? bfun(k, c) : 0.0;
-                }
-                __syncthreads();
-                const int kmax = min(IPM_KC, n - k0);
-                for (int kk = 0; kk < kmax; ++kk) {
-                    const double* Ak = A + (size_t)(k0 + kk) * lda;
-                    double av[4], bv[8];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int r = r0 + tr + 32 * a;
-                        av[a] = (r < n) ? Ak[r] : 0.0;
-                    }
-#pragma unroll
-                    for (int b = 0; b < 8; ++b) bv[b] = stage[kk * STG_LD + tc + 16 * b];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a)
-#pragma unroll
-                        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-                }
-                __syncthreads();
-            }
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const int r = r0 + tr + 32 * a;
-                if (r >= n) continue;
-#pragma unroll
-                for (int b = 0; b < 8; ++b) {
-                    const int c = c0 + tc + 16 * b;
-                    if (c < n) epi(r, c, acc[a][b]);
-                }
-            }
-        }
-    }
-    __syncthreads();
-}
 
 struct Layout {
     double* red;   // 64
@@ -196,7 +43,7 @@ struct Layout {
     double* dy1;   // n
     double* rhs;   // n
     double* col;   // n
-    double* stage; // IPM_KC * STG_LD
+    double* stage; // CTA_KC * STG_LD
     double* F;     // n*n  Cholesky workspace
     double* Zi;    // n*n
     double* dX;    // n*n
@@ -205,7 +52,7 @@ struct Layout {
 
 __host__ __device__ inline size_t ipm_fixed_smem_doubles(int n)
 {
-    return 64 + 6 * (size_t)((n + 1) & ~1) + (size_t)IPM_KC * STG_LD;
+    return 64 + 6 * (size_t)((n + 1) & ~1) + (size_t)CTA_KC * STG_LD;
 }
 
 __device__ Layout make_layout(const IpmDesc& d, double* smem, int place)
@@ -222,7 +69,7 @@ __device__ Layout make_layout(const IpmDesc& d, double* smem, int place)
     l.rhs = l.dy1 + nv;
     l.col = l.rhs + nv;
     l.stage = l.col + nv;
-    double* after = l.stage + (size_t)IPM_KC * STG_LD;
+    double* after = l.stage + (size_t)CTA_KC * STG_LD;
     double* ws = d.ws;
     if (place & 1) { l.F = after; after += nn; } else { l.F = ws; ws += nn; }
     if (place & 2) { l.Zi = after; after += nn; } else { l.Zi = ws; ws += nn; }
@@ -238,7 +85,7 @@ __device__ void ipm_body(const IpmDesc& d, double* smem, int place)
     const int n = d.n;
     const size_t nn = (size_t)n * n;
     const double* __restrict__ L = d.L;
-    double* __restrict__ X = d.X;
+    double* __restrict__ X = d.X + (d.xslot ? (size_t)(*d.xslot) * nn : 0);
     Layout s = make_layout(d, smem, place);
 
     // ---- initial point (src/ipm_mc_pk.c:65-99) ----
@@ -267,6 +114,7 @@ __device__ void ipm_body(const IpmDesc& d, double* smem, int place)
         double mu = b / (2.0 * n);
         double gap = fabs(phi - psi);
         int iter = 0;
+        int ls_total = 0;
         int status = IPM_OK;
 
         while (gap > 1e-2) {
@@ -357,6 +205,7 @@ __device__ void ipm_body(const IpmDesc& d, double* smem, int place)
                 if (++trials >= IPM_MAX_TRIALS) break;
                 ap *= 0.8;
             }
+            ls_total += trials + 1;
             if (!ok) { status = IPM_LINESEARCH; break; }
             if (ap < 1.0) ap *= 0.95;
 
@@ -375,6 +224,7 @@ __device__ void ipm_body(const IpmDesc& d, double* smem, int place)
                 if (++trials >= IPM_MAX_TRIALS) break;
                 ad *= 0.8;
             }
+            ls_total += trials + 1;
             if (!ok) { status = IPM_LINESEARCH; break; }
             if (ad < 1.0) ad *= 0.95;
 
@@ -416,6 +266,11 @@ __device__ void ipm_body(const IpmDesc& d, double* smem, int place)
             d.out[1] = (double)iter;
             d.out[2] = (double)status;
             d.out[3] = psi;
+            const double n3 = (double)n * n * n;
+            atomicAdd(&g_ipm_stats[0], iter * n3);
+            atomicAdd(&g_ipm_stats[1], 1.0);
+            atomicAdd(&g_ipm_stats[2], (double)iter);
+            atomicAdd(&g_ipm_stats[3], (double)ls_total);
         }
     }
 }
@@ -462,30 +317,110 @@ size_t ipm_ws_doubles(int n, int place)
     return nn * (2 + ((place & 1) ? 0 : 1) + ((place & 2) ? 0 : 1));
 }
 
-static void set_smem_attr(const void* fn, size_t bytes)
+// Raise the dynamic shared-memory limit only when a launch needs more than
+// was set before (the attribute call costs host time).
+static void set_smem_attr(const void* fn, size_t bytes, size_t* current)
 {
+    if (bytes <= *current) return;
     BQB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    *current = bytes;
 }
+
+// Optional CUDA-event timing of every IPM launch on its stream (for the
+// benchmark's per-kernel roofline figure).
+struct IpmTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    size_t used = 0;
+    double ms = 0.0;
+    long launches = 0;
+    void mark(cudaStream_t s)
+    {
+        if (!on) return;
+        if (used == ev.size()) {
+            cudaEvent_t e;
+            BQB_CUDA(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        BQB_CUDA(cudaEventRecord(ev[used++], s));
+    }
+    void collect()
+    {
+        if (used >= 2) BQB_CUDA(cudaEventSynchronize(ev[used - 1]));
+        for (size_t i = 0; i + 1 < used; i += 2) {
+            float t = 0.f;
+            BQB_CUDA(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+            ms += t;
+            ++launches;
+        }
+        used = 0;
+    }
+};
+static IpmTimer g_timer;
 
 void ipm_launch(const IpmDesc* d_descs, int nprob, int n_max, cudaStream_t s)
 {
+    static size_t cur = 0;
     if (nprob <= 0) return;
     size_t bytes = 0;
     const int place = ipm_place(n_max, rt().smem_optin, &bytes);
-    set_smem_attr((const void*)ipm_batched_kernel, bytes);
+    set_smem_attr((const void*)ipm_batched_kernel, bytes, &cur);
+    g_timer.mark(s);
     ipm_batched_kernel<<<nprob, IPM_THREADS, bytes, s>>>(d_descs, place);
+    g_timer.mark(s);
     BQB_COUNT_LAUNCH();
     check_launch("ipm_batched_kernel");
+    if (g_timer.used > 4096) g_timer.collect();
 }
 
 void ipm_launch_one(const IpmDesc& d, cudaStream_t s)
 {
+    static size_t cur = 0;
     size_t bytes = 0;
     const int place = ipm_place(d.n, rt().smem_optin, &bytes);
-    set_smem_attr((const void*)ipm_one_kernel, bytes);
+    set_smem_attr((const void*)ipm_one_kernel, bytes, &cur);
+    g_timer.mark(s);
     ipm_one_kernel<<<1, IPM_THREADS, bytes, s>>>(d, place);
+    g_timer.mark(s);
     BQB_COUNT_LAUNCH();
     check_launch("ipm_one_kernel");
+    if (g_timer.used > 4096) g_timer.collect();
 }
 
 }  // namespace bqb
+
+// ---- work/timing counters of the IPM kernels ------------------------------
+
+extern "C" __attribute__((visibility("default"))) void bqb_stats_enable(int on)
+{
+    bqb::rt();
+    bqb::g_timer.on = on != 0;
+}
+
+extern "C" __attribute__((visibility("default"))) void bqb_stats_reset(void)
+{
+    bqb::rt();
+    bqb::g_timer.collect();
+    bqb::g_timer.ms = 0.0;
+    bqb::g_timer.launches = 0;
+    const double z[4] = {0, 0, 0, 0};
+    BQB_CUDA(cudaMemcpyToSymbol(bqb::g_ipm_stats, z, sizeof z));
+}
+
+// out[0] sum(iterations * n^3), out[1] problems, out[2] iterations,
+// out[3] line-search factorizations, out[4] summed kernel time (ms, CUDA
+// events), out[5] timed launches.
+extern "C" __attribute__((visibility("default"))) void bqb_ipm_stats(double* out)
+{
+    bqb::rt();
+    BQB_CUDA(cudaDeviceSynchronize());
+    bqb::g_timer.collect();
+    BQB_CUDA(cudaMemcpyFromSymbol(out, bqb::g_ipm_stats, 4 * sizeof(double)));
+    out[4] = bqb::g_timer.ms;
+    out[5] = (double)bqb::g_timer.launches;
+}
+
+extern "C" __attribute__((visibility("default"))) void* bqb_stream(void)
+{
+    return (void*)bqb::rt().stream;
+}

@@ -6,8 +6,6 @@
 namespace bqb {
 
 constexpr int IPM_THREADS = 512;
-constexpr int IPM_KC = 16;            // k-chunk of the staged GEMM B operand
-constexpr int IPM_TILE = 128;         // GEMM supertile (rows and cols)
 constexpr int IPM_MAX_ITERS = 500;    // reference loops until gap <= 1e-2 with no cap
 constexpr int IPM_MAX_TRIALS = 200;   // line-search halvings (0.8^200 ~ 4e-20)
 
@@ -23,12 +21,15 @@ enum IpmStatus : int {
 // One problem.  L: n x n column-major (ld = n), read only.  X: n x n output.
 // ws: per-problem scratch of ipm_ws_doubles(n, place) doubles.
 // out[0] = phi (dual value e'y), out[1] = iterations, out[2] = status,
-// out[3] = final primal value <L,X>.
+// out[3] = final primal value <L,X>.  xslot (optional, device): the output
+// matrix is X + (*xslot) * n * n, so a bundle can direct the result into a
+// free slot chosen on the device.
 struct IpmDesc {
     const double* L;
     double* X;
     double* ws;
     double* out;
+    const int* xslot;
     int n;
     int pad_;
 };

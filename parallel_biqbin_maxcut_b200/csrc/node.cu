@@ -1,0 +1,280 @@
+// Bounding of one B&B node with all matrices resident in HBM.
+//
+// SDPbound restates src/bounding.c:24-342 line for line in its control
+// flow (the same tests, constants and parameter use); every matrix
+// operation runs on the device: the basic IPM, the heuristic, the triangle
+// separation, the bundle iterations (lambda_eta, fct_eval, step
+// bookkeeping) and the subgradient rebuild after the cuts change.  The host
+// keeps the cut lists (the reference's global arrays) and reads back only
+// scalars, the separated triangle list, X's last column (fracsol) and, when
+// pentagonal / heptagonal separation runs, X itself.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "internal.h"
+#include "ipm.cuh"
+#include "node.h"
+#include "separation.h"
+
+extern "C" {
+double Bab_LBGet(void);
+int updateSolution(int* x);
+double getFixedValue(BabNode* node, Problem* SP_);
+extern double diff;
+}
+
+namespace bqb {
+
+NodeDev& node_dev()
+{
+    static NodeDev nd;
+    return nd;
+}
+
+void upload_cuts(NodeDev& nd, const Problem* P, cudaStream_t s)
+{
+    std::vector<CutRec> rec = pack_global_cuts(P);
+    nd.cuts.upload(rec, P->NIneq, P->NPentIneq, P->NHeptaIneq, s);
+    nd.b.ensure_m(nd.cuts.m, s);
+}
+
+double tri_update_dev(NodeDev& nd, Problem* P, const double* y, int* added, int* subtracted, cudaStream_t s)
+{
+    const int kept = tri_purge(Cuts, P->NIneq, y);
+    *subtracted = P->NIneq - kept;
+    P->NIneq = kept;
+    TriSepState& st = trisep_state();
+    int size = 0;
+    const double mx = trisep_device(st, nd.X.p, P->n, params.TriIneq, params.violated_TriIneq, &size, s);
+    *added = tri_append(Cuts, kept, st.hlist.p, size);
+    P->NIneq += *added;
+    return mx;
+}
+
+static void fetch_state(NodeDev& nd, cudaStream_t s)
+{
+    BQB_CUDA(cudaMemcpyAsync(nd.hs.p, nd.b.dstate.p, BD_WORDS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(nd.hi.p, nd.b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaStreamSynchronize(s));
+    const int err = nd.hi.p[BI_ERR];
+    if (err & 1) fatal("bundle_method", "Bundle size too large! Adjust MaxBundle");
+    if (err & 2) fatal("solve_lambda", "Problem in solving linear system");
+    if (err & 4) fatal("ipm_mc_pk", "Problem with Cholesky factorization or linear system");
+    if (err & 8) fatal("bundle_method", "no free bundle slot");
+}
+
+double bundle_iterations(NodeDev& nd, int bdl_iter, double* t, cudaStream_t s)
+{
+    BundleDev& b = nd.b;
+    const int n = nd.n;
+    const size_t nn = (size_t)n * n;
+    nd.hs.ensure(8);
+    nd.hi.ensure(8);
+    // k grows by at most one per iteration
+    BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaStreamSynchronize(s));
+    const int k = nd.hi.p[BI_K];
+    b.ensure_cap(k + bdl_iter + 2, n, s);
+    nd.hi.p[BI_CAP] = b.cap;
+    BQB_CUDA(cudaMemcpyAsync(b.istate.p + BI_CAP, nd.hi.p + BI_CAP, sizeof(int), cudaMemcpyHostToDevice, s));
+    nd.hs.p[0] = *t;
+    BQB_CUDA(cudaMemcpyAsync(b.dstate.p + BD_T, nd.hs.p, sizeof(double), cudaMemcpyHostToDevice, s));
+    for (int it = 0; it < bdl_iter; ++it) {
+        lambda_eta_launch(b, nullptr, s);
+        BQB_CUDA(cudaMemcpyAsync(nd.L0.p, nd.L.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (nd.cuts.m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gtest.p, s);
+        ipm_device(nd.L0.p, b.Xb.p, n, nd.out.p, s, b.istate.p + BI_NEXT);
+        if (nd.cuts.m > 0)
+            opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
+        bundle_step_launch(b, nd.out.p, nd.L.p, s);
+        bundle_xcomb_launch(b, nd.X.p, s);
+    }
+    fetch_state(nd, s);
+    *t = nd.hs.p[BD_T];
+    return nd.hs.p[BD_F];
+}
+
+}  // namespace bqb
+
+using namespace bqb;
+
+// SDPbound (src/bounding.c:24-342).
+BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
+{
+    Runtime& R = rt();
+    cudaStream_t s = R.stream;
+    NodeDev& nd = node_dev();
+    const int n = PP_->n;
+    const int N0 = SP_->n;
+    const int NB = N0 - 1;   // BabPbSize
+    const size_t nn = (size_t)n * n;
+    nd.n = n;
+    nd.hs.ensure(8);
+    nd.hi.ensure(8);
+
+    double* dL = nd.L.ensure(nn);
+    nd.L0.ensure(nn);
+    double* dX = nd.X.ensure(nn);
+    double* dout = nd.out.ensure(4);
+    // PP->L may be host or device memory (unified addressing decides)
+    BQB_CUDA(cudaMemcpyAsync(dL, PP_->L, nn * sizeof(double), cudaMemcpyDefault, s));
+    if (nd.P0L_src != SP_->L || nd.P0N != N0) {
+        nd.P0L.ensure((size_t)N0 * N0);
+        BQB_CUDA(cudaMemcpyAsync(nd.P0L.p, SP_->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice, s));
+        nd.P0L_src = SP_->L;
+        nd.P0N = N0;
+    }
+    std::vector<int> x(NB > 0 ? NB : 1);
+    std::vector<double> col(n);
+    auto store_fracsol = [&]() {
+        BQB_CUDA(cudaMemcpyAsync(col.data(), dX + (size_t)(n - 1) * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+        int index = 0;
+        for (int i = 0; i < NB; ++i) {
+            if (node->xfixed[i])
+                node->fracsol[i] = (double)node->sol.X[i];
+            else
+                node->fracsol[i] = 0.5 * (col[index++] + 1.0);
+        }
+    };
+    auto heuristic = [&]() {
+        for (int i = 0; i < NB; ++i) x[i] = node->xfixed[i] ? node->sol.X[i] : 0;
+        heuristic_device(dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
+        updateSolution(x.data());
+    };
+
+    int bdl_iter = params.init_bundle_iter;
+    const double fixedvalue = getFixedValue(node, SP_);
+    PP_->NIneq = 0;
+    PP_->NPentIneq = 0;
+    PP_->NHeptaIneq = 0;
+    int tri_add = 0, tri_sub = 0, pent_add = 0, pent_sub = 0, hept_add = 0, hept_sub = 0;
+    double viol3 = 0.0, viol5 = 0.0, viol7 = 0.0;
+    (void)viol7;
+
+    // basic SDP relaxation
+    ipm_device(dL, dX, n, dout, s);
+    BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaStreamSynchronize(s));
+    check_ipm_status_host(nd.hs.p);
+    f = nd.hs.p[0];
+    const double basic_bound = f + fixedvalue;
+    store_fracsol();
+    heuristic();
+
+    double bound = f + fixedvalue;
+    if (bound < Bab_LBGet() + 1.0) return bound;
+    if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) return bound;
+
+    viol3 = tri_update_dev(nd, PP_, dual_gamma, &tri_add, &tri_sub, s);
+    for (int i = 0; i < PP_->NIneq; ++i) dual_gamma[i] = Cuts[i].y;
+    double t = 0.5 * (bound - Bab_LBGet()) / (PP_->NIneq * viol3 * viol3);
+
+    // bundle init: X_bundle(0) = X, G(:,0) = 1 - B(X), F(0) = <L,X>, bundle = 1
+    upload_cuts(nd, PP_, s);
+    BundleDev& b = nd.b;
+    b.ensure_cap(1 + bdl_iter + 2, n, s);
+    const int m0 = nd.cuts.m;
+    BQB_CUDA(cudaMemcpyAsync(b.gam.p, dual_gamma, (size_t)m0 * sizeof(double), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(b.Xb.p, dX, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    opB_launch(nd.cuts, b.Xb.p, nn, nullptr, 1, n, b.G.p, b.ldg, true, s);
+    {
+        int* hi = nd.hi.p;
+        for (int q = 0; q < 8; ++q) hi[q] = 0;
+        hi[BI_K] = 0;        // F(0) is written at position 0 below, then K = 1
+        hi[BI_NEXT] = 0;
+        hi[BI_CAP] = b.cap;
+        BQB_CUDA(cudaMemcpyAsync(b.istate.p, hi, BI_WORDS * sizeof(int), cudaMemcpyHostToDevice, s));
+        bundle_fval_launch(b, dL, b.istate.p + BI_NEXT, b.istate.p + BI_K, s);
+        bundle_append_launch(b, s);
+        nd.hs.p[BD_F] = f;
+        nd.hs.p[BD_T] = t;
+        nd.hs.p[BD_FTEST] = 0.0;
+        nd.hs.p[BD_DEL] = 0.0;
+        BQB_CUDA(cudaMemcpyAsync(b.dstate.p, nd.hs.p, BD_WORDS * sizeof(double), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+    }
+
+    int count = 0;
+    bool done = false, prune = false, giveup = false;
+    std::vector<double> hX;
+    while (!done) {
+        ++count;
+        const double oldf = f;
+        f = bundle_iterations(nd, bdl_iter, &t, s);
+        bound = f + fixedvalue;
+        prune = bound < Bab_LBGet() + 1.0;
+        if (!prune) {
+            heuristic();
+            prune = bound < Bab_LBGet() + 1.0;
+        }
+        const double gap = bound - Bab_LBGet();
+        if (count == params.triag_iter + params.pent_iter + params.hept_iter)
+            if (gap - 1.0 > (oldf - f) * (params.max_outer_iter - count)) giveup = true;
+        if (count == params.max_outer_iter)
+            if (gap - 1.0 > (oldf - f) * params.extra_iter) giveup = true;
+        if (count == params.max_outer_iter + params.extra_iter) giveup = true;
+
+        if (!prune && !giveup) {
+            const int triag = PP_->NIneq;
+            const int penta = PP_->NPentIneq;
+            const int m = PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq;
+            BQB_CUDA(cudaMemcpyAsync(dual_gamma, b.gam.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+            viol3 = tri_update_dev(nd, PP_, dual_gamma, &tri_add, &tri_sub, s);
+            const bool do_pent = params.include_Pent && (count > params.triag_iter || viol3 < 0.2);
+            const bool do_hept_pre = params.include_Hepta;
+            if (do_pent || do_hept_pre) {
+                BQB_CUDA(cudaMemcpyAsync(X, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+                BQB_CUDA(cudaStreamSynchronize(s));
+            }
+            if (do_pent) viol5 = updatePentagonalInequalities(PP_, dual_gamma, &pent_add, &pent_sub, triag);
+            if (params.include_Hepta &&
+                ((count > params.triag_iter + params.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4))))
+                viol7 = updateHeptagonalInequalities(PP_, dual_gamma, &hept_add, &hept_sub, triag + penta);
+        } else {
+            tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
+        }
+        done = prune || giveup;
+        store_fracsol();
+
+        if (!done) {
+            for (int i = 0; i < PP_->NIneq; ++i) dual_gamma[i] = Cuts[i].y;
+            for (int i = 0; i < PP_->NPentIneq; ++i) dual_gamma[i + PP_->NIneq] = Pent_Cuts[i].y;
+            for (int i = 0; i < PP_->NHeptaIneq; ++i)
+                dual_gamma[i + PP_->NIneq + PP_->NPentIneq] = Hepta_Cuts[i].y;
+            upload_cuts(nd, PP_, s);
+            const int m = nd.cuts.m;
+            BQB_CUDA(cudaMemcpyAsync(b.gam.p, dual_gamma, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
+            // current bundle size (host copy) for capacity and the G rebuild
+            BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+            const int k = nd.hi.p[BI_K];
+            b.ensure_cap(k + 2 + bdl_iter + 2, n, s);
+            nd.hi.p[BI_CAP] = b.cap;
+            BQB_CUDA(cudaMemcpyAsync(b.istate.p + BI_CAP, nd.hi.p + BI_CAP, sizeof(int), cudaMemcpyHostToDevice, s));
+            // fct_eval(PP, dual_gamma, X_test, g) into the free slot
+            BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            if (m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gam.p, s);
+            ipm_device(nd.L0.p, b.Xb.p, n, dout, s, b.istate.p + BI_NEXT);
+            // G(:, i) = 1 - B(X_bundle(i)) for the bundle, then g for the new element
+            opB_launch(nd.cuts, b.Xb.p, nn, b.slot.p, k, n, b.G.p, b.ldg, true, s);
+            opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
+            bundle_fval_launch(b, dL, b.istate.p + BI_NEXT, b.istate.p + BI_K, s);
+            bundle_append_launch(b, s);
+            BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+            check_ipm_status_host(nd.hs.p);
+            if (nd.hi.p[BI_ERR] & 1) fatal("SDPbound", "Bundle size too large! Adjust MaxBundle");
+            t *= 1.05;
+        }
+        bdl_iter += count % 2;
+        bdl_iter = (bdl_iter < params.max_bundle_iter) ? bdl_iter : params.max_bundle_iter;
+    }
+    bound = f + fixedvalue;
+    if (rank == 0) diff = basic_bound - bound;
+    return bound;
+}

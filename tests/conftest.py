@@ -28,3 +28,23 @@ def lib():
     L = _lib.load()
     assert L.bqb_init(0) == 0, L.bqb_last_error()
     return L
+
+
+@pytest.fixture(scope="session")
+def lib_globals(lib):
+    """The product library's reference-layout globals, sized for n <= 344."""
+    from parallel_biqbin_maxcut_b200 import _lib
+    return _lib.GlobalArrays(lib, 344)
+
+
+@pytest.fixture(scope="session")
+def ref():
+    """The reference's own C code (oracle/_ref), globals sized for n <= 101.
+    Skips when the reference build is absent."""
+    from oracle import refbind
+    from parallel_biqbin_maxcut_b200 import instances
+    if not refbind.available():
+        pytest.skip("reference build absent (oracle/Makefile)")
+    r = refbind.RefLib()
+    r.setup(instances.gnp_unit(101, 0.5, 99), {"init_bundle_iter": 5, "violated_TriIneq": 0.05})
+    return r

@@ -1,0 +1,201 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own C
+code (oracle/_ref, built from the reference sources by oracle/Makefile).
+
+Run in a container that has the reference sources:
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Every input is seeded synthetic data (parallel_biqbin_maxcut_b200.instances);
+every output is what the reference build returns for it.  The fixtures pin
+the CPU oracle (oracle/bqb_oracle.py) and the host-side separation code
+without needing the reference at test time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import bqb_oracle as O  # noqa: E402
+from oracle import refbind  # noqa: E402
+from parallel_biqbin_maxcut_b200 import _lib, instances  # noqa: E402
+
+libc = C.CDLL("libc.so.6")
+libc.rand.restype = C.c_int
+
+
+def colmajor(A):
+    return np.ascontiguousarray(np.asarray(A, dtype=np.float64).T).reshape(-1)
+
+
+def from_col(v, n):
+    return np.asarray(v[: n * n]).reshape(n, n).T.copy()
+
+
+def main():
+    ref = refbind.RefLib()
+    A0 = instances.gnp_unit(31, 0.5, 101)
+    ref.setup(A0, {"init_bundle_iter": 5, "violated_TriIneq": 0.05})
+    SPL = ref.SP_L()
+    N0 = SPL.shape[0]
+    out = {}
+
+    # 1. IPM on two subproblems
+    rng = np.random.default_rng(5)
+    for tag, (xf, sol) in (("root", (np.zeros(N0 - 1, np.int32), np.zeros(N0 - 1, np.int32))),
+                           ("sub", instances.random_fixings(N0, 1, 8, seed=6)[0])):
+        L = O.create_subproblem(SPL, xf, sol)
+        X, phi = ref.ipm(L)
+        out[f"ipm_{tag}_L"] = L
+        out[f"ipm_{tag}_X"] = X
+        out[f"ipm_{tag}_phi"] = np.array([phi])
+
+    # 2. op_B / op_Bt with triangle, pentagonal and heptagonal cuts
+    n = 20
+    cuts = O.Cuts(
+        tri=np.array([np.sort(rng.choice(n, 3, replace=False))[::-1] for _ in range(40)], np.int32),
+        tri_type=rng.integers(1, 5, 40).astype(np.int32),
+        pent=np.array([rng.choice(n, 5, replace=False) for _ in range(12)], np.int32),
+        pent_type=rng.integers(1, 4, 12).astype(np.int32),
+        hept=np.array([rng.choice(n, 7, replace=False) for _ in range(9)], np.int32),
+        hept_type=rng.integers(1, 5, 9).astype(np.int32))
+    Cp = ref.gptr("Cuts", refbind.TriIneq)
+    Pp = ref.gptr("Pent_Cuts", refbind.PentIneq)
+    Hp = ref.gptr("Hepta_Cuts", refbind.HeptIneq)
+    for c in range(40):
+        Cp[c].i, Cp[c].j, Cp[c].k = (int(v) for v in cuts.tri[c])
+        Cp[c].type = int(cuts.tri_type[c])
+    for c in range(12):
+        Pp[c].type = int(cuts.pent_type[c])
+        for a in range(5):
+            Pp[c].permutation[a] = int(cuts.pent[c, a])
+    for c in range(9):
+        Hp[c].type = int(cuts.hept_type[c])
+        for a in range(7):
+            Hp[c].permutation[a] = int(cuts.hept[c, a])
+    Xs = rng.standard_normal((n, n))
+    Xs = Xs + Xs.T
+    Xc = colmajor(Xs)
+    prob = refbind.Problem()
+    prob.L = Xc.ctypes.data_as(C.POINTER(C.c_double))
+    prob.n, prob.NIneq, prob.NPentIneq, prob.NHeptaIneq = n, 40, 12, 9
+    y = rng.standard_normal(cuts.m)
+    yo = y.copy()
+    ref.lib.op_B(C.byref(prob), refbind.dptr(yo), refbind.dptr(Xc))
+    t = np.abs(rng.standard_normal(cuts.m))
+    Xo = Xc.copy()
+    ref.lib.op_Bt(C.byref(prob), refbind.dptr(Xo), refbind.dptr(t))
+    for k, v in (("tri", cuts.tri), ("tri_type", cuts.tri_type), ("pent", cuts.pent),
+                 ("pent_type", cuts.pent_type), ("hept", cuts.hept), ("hept_type", cuts.hept_type)):
+        out[f"cuts_{k}"] = v
+    out.update(cuts_X=Xs, cuts_y=y, cuts_yout=yo, cuts_t=t, cuts_Xout=from_col(Xo, n))
+
+    # 3. triangle separation: the full value table (thr -10, list = all
+    #    triples in scan order) and a streaming top-K case
+    for tag, (nv, seed, T, thr) in (("all", (12, 7, 10 ** 6, -10.0)), ("topk", (30, 8, 60, 0.05))):
+        Xm = O.ipm_mc_pk(O.create_subproblem(O.build_SP_L(instances.gnp_unit(nv, 0.5, seed)),
+                                             np.zeros(nv - 1, int), np.zeros(nv - 1, int))).X
+        ref.set_param("TriIneq", min(T, 4 * nv ** 3))
+        ref.set_param("violated_TriIneq", thr)
+        cap = min(T, 4 * nv ** 3)
+        lst = (refbind.TriIneq * cap)()
+        size = C.c_int()
+        mx = ref.lib.getViolated_TriangleInequalities(refbind.dptr(colmajor(Xm)), nv, lst, C.byref(size))
+        out[f"tri_{tag}_X"] = Xm
+        out[f"tri_{tag}_param"] = np.array([cap, thr])
+        out[f"tri_{tag}_list"] = np.array([(lst[q].type, lst[q].i, lst[q].j, lst[q].k) for q in range(size.value)],
+                                          np.int32).reshape(-1, 4)
+        out[f"tri_{tag}_values"] = np.array([lst[q].value for q in range(size.value)])
+        out[f"tri_{tag}_max"] = np.array([mx])
+
+    # 4. heuristic on a subproblem of SP, from a fixed rand() state
+    xf, sol = instances.random_fixings(N0, 1, 6, seed=9)[0]
+    L = O.create_subproblem(SPL, xf, sol)
+    nsub = L.shape[0]
+    Xm = O.ipm_mc_pk(L).X
+    refX = ref.gptr("X", C.c_double)
+    Xc = colmajor(Xm)
+    for q in range(nsub * nsub):
+        refX[q] = Xc[q]
+    libc.srand(4242)
+    x = np.zeros(N0 - 1, np.int32)
+    v = ref.lib.runHeuristic_unpacked(refbind.dptr(colmajor(SPL)), N0, refbind.dptr(colmajor(L)), nsub,
+                                      refbind.iptr(xf), refbind.iptr(sol), refbind.iptr(x))
+    out.update(heur_SPL=SPL, heur_L=L, heur_X=Xm, heur_xfixed=xf, heur_sol=sol, heur_seed=np.array([4242]),
+               heur_value=np.array([v]), heur_x=x, heur_rand_after=np.array([libc.rand()]))
+
+    # 5. mc_1opt
+    x0 = rng.choice(np.array([-1, 1], np.int32), nsub)
+    xo = x0.copy()
+    cost = ref.lib.mc_1opt(refbind.iptr(xo), refbind.dptr(colmajor(L)), nsub)
+    out.update(opt_L=L, opt_x0=x0, opt_x=xo, opt_cost=np.array([cost]))
+
+    # 6. solve_lambda and lambda_eta
+    G = rng.standard_normal((60, 7)) * 0.3
+    tq = 0.3
+    Q = tq * (G.T @ G)
+    c = rng.standard_normal(7) * 3
+    lam = np.zeros(7)
+    ref.lib.solve_lambda(7, refbind.dptr(colmajor(Q)), refbind.dptr(c.copy()), refbind.dptr(lam))
+    out.update(qp_Q=Q, qp_c=c, qp_lambda=lam)
+    zeta = -rng.random(7) * 10
+    gam = np.where(rng.random(60) < 0.5, 0.0, rng.random(60))
+    prob = refbind.Problem()
+    prob.NIneq, prob.bundle = 60, 7
+    dg, lm, et = np.zeros(60), np.zeros(7), np.zeros(60)
+    tt = C.c_double(tq)
+    Gc = colmajor(G)   # m x k, column-major
+    ref.lib.lambda_eta(C.byref(prob), refbind.dptr(zeta.copy()), refbind.dptr(Gc), refbind.dptr(gam.copy()),
+                       refbind.dptr(dg), refbind.dptr(lm), refbind.dptr(et), C.byref(tt))
+    out.update(le_G=G, le_zeta=zeta, le_gamma=gam, le_t=np.array([tq]), le_dgamma=dg, le_lambda=lm, le_eta=et,
+               le_tout=np.array([tt.value]))
+
+    # 7. simulated annealing (pentagonal H2) from a fixed rand() state
+    ref.lib.qap_simulated_annealing.restype = C.c_double
+    ref.lib.qap_simulated_annealing.argtypes = [C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double), C.c_int,
+                                               C.POINTER(C.c_int)]
+    e = np.array([-1, 1, 1, 1, 1])
+    Hm = np.ascontiguousarray(np.outer(e, e).reshape(-1), dtype=np.int32)
+    libc.srand(77)
+    p = np.zeros(5, np.int32)
+    sa_v = ref.lib.qap_simulated_annealing(refbind.iptr(Hm), 5, refbind.dptr(colmajor(Xm)), nsub, refbind.iptr(p))
+    out.update(sa_X=Xm, sa_H=Hm, sa_seed=np.array([77]), sa_value=np.array([sa_v]), sa_perm=p,
+               sa_rand_after=np.array([libc.rand()]))
+
+    np.savez_compressed(os.path.join(HERE, "components.npz"), **out)
+
+    # 8. end-to-end optimal values of the reference's serial B&B
+    e2e = []
+    with tempfile.TemporaryDirectory() as td:
+        for kind, nv, seed in (("unit", 40, 1), ("unit", 60, 2), ("pm1", 40, 3), ("qubo", 30, 4)):
+            if kind == "unit":
+                A = instances.gnp_unit(nv, 0.5, seed)
+            elif kind == "pm1":
+                A = instances.gnp_pm1(nv, 0.5, seed)
+            else:
+                A = instances.qubo_to_maxcut(instances.qubo_dense(nv, 0.1, seed))
+            inst, prm = os.path.join(td, "g.rudy"), os.path.join(td, "params")
+            instances.write_rudy(inst, A)
+            instances.write_params(prm, _lib.PARAMS_FILE)
+            txt = subprocess.run([refbind.REF_BAB, inst, prm], capture_output=True, text=True,
+                                 env=dict(os.environ, OPENBLAS_NUM_THREADS="1")).stdout
+            e2e.append({"kind": kind, "nv": nv, "seed": seed,
+                        "max_value": float(re.search(r"Maximum value = (\S+)", txt).group(1)),
+                        "nodes": int(re.search(r"Nodes = (\d+)", txt).group(1)),
+                        "root_bound": float(re.search(r"Root node bound = (\S+)", txt).group(1))})
+    with open(os.path.join(HERE, "bab_optima.json"), "w") as fh:
+        json.dump(e2e, fh, indent=1)
+    print("wrote", os.path.join(HERE, "components.npz"), "and bab_optima.json")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,120 @@
+"""CPU: pin the oracle (oracle/bqb_oracle.py) against golden vectors the
+reference's own C code produced (tests/golden/make_golden.py), and against
+the reference build itself when it is present in this container."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import bqb_oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+G = np.load(os.path.join(HERE, "golden", "components.npz"))
+
+
+def test_ipm_matches_golden():
+    for tag in ("root", "sub"):
+        r = O.ipm_mc_pk(G[f"ipm_{tag}_L"])
+        assert abs(r.phi - G[f"ipm_{tag}_phi"][0]) <= 1e-9 * abs(G[f"ipm_{tag}_phi"][0])
+        assert np.max(np.abs(r.X - G[f"ipm_{tag}_X"])) <= 1e-9
+
+
+def _cuts():
+    return O.Cuts(tri=G["cuts_tri"], tri_type=G["cuts_tri_type"], pent=G["cuts_pent"],
+                  pent_type=G["cuts_pent_type"], hept=G["cuts_hept"], hept_type=G["cuts_hept_type"])
+
+
+def test_opB_opBt_match_golden():
+    cuts = _cuts()
+    y = O.op_B(cuts, G["cuts_y"], G["cuts_X"])
+    np.testing.assert_allclose(y, G["cuts_yout"], rtol=0, atol=1e-13)
+    Xo = O.op_Bt(cuts, G["cuts_X"], G["cuts_t"])
+    np.testing.assert_allclose(Xo, G["cuts_Xout"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("tag", ["all", "topk"])
+def test_triangle_separation_matches_golden_bit_exact(tag):
+    cap, thr = G[f"tri_{tag}_param"]
+    lst, mx = O.getViolated_TriangleInequalities(G[f"tri_{tag}_X"], int(cap), float(thr))
+    got = np.array([r[:4] for r in lst], np.int32).reshape(-1, 4)
+    assert np.array_equal(got, G[f"tri_{tag}_list"])
+    assert np.array_equal(np.array([r[4] for r in lst]), G[f"tri_{tag}_values"])   # bit-exact
+    assert mx == G[f"tri_{tag}_max"][0]
+
+
+def test_heuristic_matches_golden():
+    O.srand(int(G["heur_seed"][0]))
+    x = np.zeros(len(G["heur_x"]), np.int64)
+    v = O.runHeuristic_unpacked(G["heur_SPL"], G["heur_L"], G["heur_xfixed"], G["heur_sol"], x, G["heur_X"])
+    assert v == G["heur_value"][0]
+    assert np.array_equal(x, G["heur_x"])
+    assert O.rand() == G["heur_rand_after"][0]
+
+
+def test_mc_1opt_matches_golden():
+    x = G["opt_x0"].astype(np.int64).copy()
+    cost = O.mc_1opt(x, G["opt_L"])
+    assert cost == G["opt_cost"][0]
+    assert np.array_equal(x, G["opt_x"])
+
+
+def test_bundle_qp_matches_golden():
+    lam = O.solve_lambda(G["qp_Q"], G["qp_c"])
+    np.testing.assert_allclose(lam, G["qp_lambda"], rtol=0, atol=1e-9)
+    dg, lm, et, t = O.lambda_eta(G["le_zeta"], G["le_G"], G["le_gamma"], float(G["le_t"][0]))
+    np.testing.assert_allclose(lm, G["le_lambda"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(dg, G["le_dgamma"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(et, G["le_eta"], rtol=0, atol=1e-8)
+    assert t == G["le_tout"][0]
+
+
+def test_subproblem_construction_consistent():
+    """createSubproblem / getFixedValue restated: the subproblem objective
+    plus the fixed value equals the full objective for every completion."""
+    SPL = G["heur_SPL"]
+    xf, sol = G["heur_xfixed"], G["heur_sol"]
+    L = O.create_subproblem(SPL, xf, sol)
+    fv = O.fixed_value(SPL, xf, sol)
+    rng = np.random.default_rng(0)
+    free = np.nonzero(xf == 0)[0]
+    for _ in range(20):
+        s = sol.astype(np.int64).copy()
+        s[free] = rng.integers(0, 2, len(free))
+        xpm = np.concatenate([2 * s[free] - 1, [1]]).astype(np.float64)
+        assert abs(xpm @ L @ xpm + fv - O.evaluateSolution(SPL, s)) < 1e-9
+
+
+def test_bab_optima_fixture_present():
+    with open(os.path.join(HERE, "golden", "bab_optima.json")) as fh:
+        rows = json.load(fh)
+    assert len(rows) >= 4 and all(r["max_value"] > 0 for r in rows)
+
+
+def test_reference_build_reproduces_reference_fixtures():
+    """The reference build itself against the reference's tests/rudy
+    expected outputs (read where they lie; only in a container that has the
+    reference sources)."""
+    import re
+    import subprocess
+    import tempfile
+    from oracle import refbind
+    src = "/root/reference/tests/rudy"
+    if not (refbind.available() and os.path.isdir(src)):
+        pytest.skip("reference sources or build absent")
+    with tempfile.TemporaryDirectory() as td:
+        params = os.path.join(td, "params")
+        with open("/root/reference/params") as fi, open(params, "w") as fo:
+            fo.write(fi.read())
+        for name in ("g05_60.0",):
+            inst = os.path.join(td, name)
+            with open(os.path.join(src, name)) as fi, open(inst, "w") as fo:
+                fo.write(fi.read())
+            out = subprocess.run([refbind.REF_BAB, inst, params], capture_output=True, text=True,
+                                 env=dict(os.environ, OPENBLAS_NUM_THREADS="1")).stdout
+            with open(os.path.join(src, name + "-expected_output")) as fh:
+                exp = fh.read()
+            for key in ("Maximum value =", "Solution ="):
+                got = re.search(re.escape(key) + r".*", out).group(0)
+                want = re.search(re.escape(key) + r".*", exp).group(0)
+                assert got.strip() == want.strip()
