@@ -1,0 +1,69 @@
+"""Summaries of Nsight Compute output for the profiles/ notes.
+
+    python -m parallel_biqbin_maxcut_b200.profiling launches <launches.csv>
+        per-kernel launch count, total time and share from a
+        `ncu --metrics gpu__time_duration.sum --csv --log-file ...` list
+    python -m parallel_biqbin_maxcut_b200.profiling raw <report.csv>
+        selected counters from `ncu -i report.ncu-rep --page raw --csv`
+"""
+from __future__ import annotations
+
+import collections
+import csv
+import re
+import sys
+
+UNIT = {"ns": 1e-3, "nsecond": 1e-3, "us": 1.0, "usecond": 1.0, "ms": 1e3, "msecond": 1e3, "s": 1e6, "second": 1e6}
+
+
+def kernel_short_name(full: str) -> str:
+    name = full.split("(")[0]
+    name = re.sub(r"<.*>$", "", name) if not name.endswith(">::") else name
+    return name.replace("bqb::", "").replace("<unnamed>::", "").strip()
+
+
+def summarize_launches(path: str) -> str:
+    rows = list(csv.reader(open(path)))
+    hdr = next(i for i, r in enumerate(rows) if "Kernel Name" in r)
+    h = rows[hdr]
+    ki, vi, ui = h.index("Kernel Name"), h.index("Metric Value"), h.index("Metric Unit")
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for r in rows[hdr + 1:]:
+        if len(r) <= vi or not r[vi]:
+            continue
+        us = float(r[vi].replace(",", "")) * UNIT.get(r[ui], 1.0)
+        a = agg[kernel_short_name(r[ki])]
+        a[0] += 1
+        a[1] += us
+    tot = sum(a[1] for a in agg.values())
+    out = [f"{'kernel':44s} {'launches':>8s} {'total ms':>10s} {'share':>7s} {'avg us':>10s}"]
+    for k, (c, t) in sorted(agg.items(), key=lambda x: -x[1][1]):
+        out.append(f"{k[:44]:44s} {c:8d} {t / 1e3:10.3f} {100 * t / tot:6.2f}% {t / c:10.1f}")
+    out.append(f"{'total':44s} {sum(a[0] for a in agg.values()):8d} {tot / 1e3:10.3f}")
+    return "\n".join(out)
+
+
+RAW_KEYS = ("gpu__time_duration.sum", "dram__bytes_read.sum", "dram__bytes_write.sum", "dram__cycles_active",
+            "gpu__dram_throughput", "sm__pipe_tensor_cycles_active", "sm__warps_active",
+            "smsp__average_warps_issue_stalled", "launch__registers_per_thread", "sm__throughput",
+            "sm__inst_executed_pipe_fp64", "smsp__inst_executed.sum", "l1tex__data_bank_conflicts",
+            "launch__shared_mem_per_block", "sm__pipe_fp64_cycles_active")
+
+
+def summarize_raw(path: str) -> str:
+    rows = list(csv.reader(open(path)))
+    hdr = rows[0]
+    units = rows[1] if len(rows) > 1 else [""] * len(hdr)
+    out = []
+    for r in rows[2:]:
+        name = r[hdr.index("Kernel Name")] if "Kernel Name" in hdr else "?"
+        out.append(f"== {kernel_short_name(name)}")
+        for i, col in enumerate(hdr):
+            if any(col.startswith(k) for k in RAW_KEYS):
+                out.append(f"  {col} = {r[i]} {units[i]}")
+    return "\n".join(out)
+
+
+if __name__ == "__main__":
+    mode, path = sys.argv[1], sys.argv[2]
+    print(summarize_launches(path) if mode == "launches" else summarize_raw(path))
