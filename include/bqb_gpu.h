@@ -247,6 +247,21 @@ void bqb_ipm_plan_destroy(bqb_ipm_plan *plan);
 int bqb_ipm_batch_device(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
                          double *out, void *stream);
 
+/* Basic SDP bound of one problem without any device allocation.  No
+ * counterpart in the reference: it exists for callers that may not call
+ * cudaMalloc while they run (e.g. inside a host application whose memory
+ * manager owns the GPU, or in a loop that must not synchronise on an
+ * allocation).  L, X: device pointers, n x n column-major; out: device, 4
+ * doubles (phi, iterations, status, <L,X>).  Scratch is a fixed array in the
+ * library's static device memory (3 * 128^2 doubles per GPU, held until
+ * exit), so n <= BQB_IPM_NOALLOC_NMAX; larger n returns 1 with a message in
+ * bqb_last_error().  The first call on a device resolves the array's address
+ * and should precede any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race.  Asynchronous on `stream` (a cudaStream_t; NULL =
+ * the legacy default stream).  Returns 0 on success, 2 on a CUDA error. */
+#define BQB_IPM_NOALLOC_NMAX 128
+int bqb_ipm_noalloc(const double *L, double *X, int n, double *out, void *stream);
+
 /* Same, host memory in and out (copies included), synchronous. */
 int bqb_ipm_batch(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
                   double *phi, int *iters, int *status);

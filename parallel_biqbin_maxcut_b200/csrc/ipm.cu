@@ -387,6 +387,18 @@ void ipm_launch_one(const IpmDesc& d, cudaStream_t s)
     if (g_timer.used > 4096) g_timer.collect();
 }
 
+// Single-problem launch for callers that manage the scratch (d.ws) and the
+// placement themselves; records no timing events and caches nothing.
+cudaError_t ipm_launch_prepared(const IpmDesc& d, int place, size_t smem_bytes, cudaStream_t s)
+{
+    cudaError_t e = cudaFuncSetAttribute((const void*)ipm_one_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    ipm_one_kernel<<<1, IPM_THREADS, smem_bytes, s>>>(d, place);
+    BQB_COUNT_LAUNCH();
+    return cudaGetLastError();
+}
+
 }  // namespace bqb
 
 // ---- work/timing counters of the IPM kernels ------------------------------

@@ -43,5 +43,8 @@ size_t ipm_ws_doubles(int n, int place);
 void ipm_launch(const IpmDesc* d_descs, int nprob, int n_max, cudaStream_t s);
 // Single problem: descriptor passed by value.
 void ipm_launch_one(const IpmDesc& d, cudaStream_t s);
+// Single problem with placement chosen by the caller; returns the launch
+// status instead of raising it.
+cudaError_t ipm_launch_prepared(const IpmDesc& d, int place, size_t smem_bytes, cudaStream_t s);
 
 }  // namespace bqb
