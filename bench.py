@@ -10,12 +10,17 @@ parameters.  First the root is bounded with rank 0 (this sets the incumbent
 and `diff` as the reference's master does); then every subproblem is bounded
 as a worker bounds a node (rank 1): IPM, heuristic, prune / give-up tests,
 cutting planes and bundle iterations to the reference's stopping rules.
-A step bounds one batch of subproblems; the metric is nodes/s.
+A step bounds one batch of subproblems with --threads concurrent bounding
+engines (bqb_bound_nodes: one host thread, CUDA stream and set of buffers
+per engine, nodes handed out dynamically); the metric is nodes/s.
 
-  value : SDPbound on device-resident subproblem matrices (inputs in HBM)
-  e2e   : Evaluate(node, SP, PP, 1) through the C ABI with host buffers, as
-          the reference's B&B calls it (subproblem construction and every
-          host<->device copy inside the timed region)
+  value : bqb_bound_nodes on device-resident subproblem matrices (inputs in
+          HBM)
+  e2e   : bqb_bound_nodes with host nodes: subproblem construction on the
+          host (createSubproblem) and every host<->device copy inside the
+          timed region
+  dropin_serial : the reference-facing Evaluate(node, SP, PP, 1), one node
+          at a time on the library stream, as the reference's worker calls it
 
 `--impl reference` times the reference's own C implementation (built
 unmodified into oracle/_ref/libbqb_ref.so) on the host cores, one process per
@@ -187,21 +192,39 @@ class GpuArm:
         self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
         torch.cuda.synchronize()
 
-    def bound_device(self, idx):
-        """value leg: SDPbound with PP->L resident in HBM."""
-        lib, PP = self.lib, self.PP.contents
-        for i in idx:
-            PP.n = self.n[i]
-            PP.L = C.cast(C.c_void_p(self.dL[i].data_ptr()), C.POINTER(C.c_double))
-            lib.SDPbound(C.byref(self.nodes[i]), self.SP, self.PP, 1)
-        self.restore_host_L()
+    def node_array(self, idx):
+        arr = (_lib.BabNode * len(idx))()
+        for q, i in enumerate(idx):
+            C.memmove(C.byref(arr[q]), C.byref(self.nodes[i]), C.sizeof(_lib.BabNode))
+        return arr
+
+    def device_ptrs(self, idx):
+        return (C.c_void_p * len(idx))(*[self.dL[i].data_ptr() for i in idx])
+
+    def bound_device(self, arr, ptrs, threads):
+        """value leg: concurrent engines on device-resident PP->L."""
+        out = np.zeros(len(arr))
+        rc = self.lib.bqb_bound_nodes(arr, len(arr), 1, threads, ptrs, _lib.dptr(out))
+        assert rc == 0, self.lib.bqb_last_error()
+        return out
+
+    def bound_e2e(self, idx, threads):
+        """e2e leg: the same C-ABI call with host nodes; every subproblem is
+        built on the host (createSubproblem) and copied in, and the bounds
+        and fractional solutions come back to the host."""
+        arr = self.node_array(idx)
+        out = np.zeros(len(idx))
+        rc = self.lib.bqb_bound_nodes(arr, len(idx), 1, threads, None, _lib.dptr(out))
+        assert rc == 0, self.lib.bqb_last_error()
+        return out
 
     def restore_host_L(self):
         self.PP.contents.L = C.cast(C.c_void_p(self.PP_L_host), C.POINTER(C.c_double))
         assert C.cast(self.PP.contents.L, C.c_void_p).value == self.PP_L_host
 
-    def bound_e2e(self, idx):
-        """e2e leg: the reference-facing Evaluate with host buffers."""
+    def dropin_serial(self, idx):
+        """The reference-facing drop-in: Evaluate one node at a time on the
+        library stream, as the reference's worker calls it."""
         lib = self.lib
         return [lib.Evaluate(C.byref(self.nodes[i]), self.SP, self.PP, 1) for i in idx]
 
@@ -228,13 +251,13 @@ def run_gpu(args):
         pg = dist
     arm = GpuArm(local)
     B = args.nodes_per_step
-    # rank r bounds its own slice: weak scaling (per-GPU work fixed)
-    order = [(rank * B + q) % N_SUB for q in range(B * (args.warmup + args.steps))]
-    order = [(i * 7919 + rank * 131) % N_SUB for i in range(len(order))]
-
-    def batches(start):
-        for s in range(start, start + args.steps):
-            yield order[s * B:(s + 1) * B]
+    T = args.threads
+    # rank r bounds its own share of the subproblems (weak scaling: per-GPU
+    # work fixed); each step is a batch of B subproblems
+    order = [(i * 7919 + rank * 131) % N_SUB for i in range(B * (args.warmup + args.steps))]
+    batches = [order[s * B:(s + 1) * B] for s in range(args.warmup + args.steps)]
+    arrays = [arm.node_array(b) for b in batches]
+    ptrs = [arm.device_ptrs(b) for b in batches]
 
     def barrier():
         torch.cuda.synchronize()
@@ -249,29 +272,35 @@ def run_gpu(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up
+    # warm-up (also sizes every engine's device buffers)
     for s in range(args.warmup):
-        arm.bound_device(order[s * B:(s + 1) * B])
-    stream = torch.cuda.ExternalStream(arm.lib.bqb_stream())
+        arm.bound_device(arm.node_array(batches[s]), ptrs[s], T)
+    stream = torch.cuda.current_stream()
 
     # ---- value: device-resident inputs ----
+    # bqb_bound_nodes returns when every engine stream is idle; the events on
+    # the (idle) current stream bracket the whole call on the device clock
     arm.lib.bqb_stats_reset()
     arm.lib.bqb_stats_enable(1)
     clocks = ClockSampler(local)
     launches0 = arm.lib.bqb_kernel_launches()
     barrier()
     clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for b in batches(args.warmup):
+    ms = 0.0
+    bounds_dev = []
+    for s in range(args.warmup, args.warmup + args.steps):
         arm.l2_flush()
-        arm.bound_device(b)
-    ev1.record(stream)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        bounds_dev.append(arm.bound_device(arrays[s], ptrs[s], T))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms += ev0.elapsed_time(ev1)
     barrier()
     clk = clocks.stop()
     launches = arm.lib.bqb_kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
     stats = (C.c_double * 6)()
     arm.lib.bqb_ipm_stats(stats)
     arm.lib.bqb_stats_enable(0)
@@ -279,36 +308,58 @@ def run_gpu(args):
     total_nodes = B * args.steps * ws
     value = total_nodes / (ms_max / 1e3)
 
-    # ---- e2e: host buffers through Evaluate ----
+    # ---- e2e: host nodes through the same C-ABI call ----
     barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    bounds = []
-    for b in batches(args.warmup):
+    ms_e2e = 0.0
+    for s in range(args.warmup, args.warmup + args.steps):
         arm.l2_flush()
-        bounds += arm.bound_e2e(b)
-    t1.record(stream)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        arm.bound_e2e(batches[s], T)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e += t0.elapsed_time(t1)
     barrier()
-    ms_e2e = max_over_ranks(t0.elapsed_time(t1))
+    ms_e2e = max_over_ranks(ms_e2e)
     e2e = total_nodes / (ms_e2e / 1e3)
-    h2d = sum(arm.n[i] ** 2 * 8 + 2 * 4 * (NV - 1) for i in order[args.warmup * B:(args.warmup + 1) * B])
-    d2h = B * 8
+    b0 = batches[args.warmup]
+    h2d = sum(arm.n[i] ** 2 * 8 + 3 * 4 * (NV - 1) for i in b0)
+    d2h = B * 8 + B * (NV - 1) * 8
+
+    # ---- the plain drop-in (one node at a time, library stream) ----
+    drop = None
+    if args.dropin_nodes > 0:
+        idx = b0[: args.dropin_nodes]
+        barrier()
+        d0 = torch.cuda.Event(enable_timing=True)
+        d1 = torch.cuda.Event(enable_timing=True)
+        d0.record(stream)
+        arm.dropin_serial(idx)
+        d1.record(stream)
+        torch.cuda.synchronize()
+        drop = {"value": len(idx) / (d0.elapsed_time(d1) / 1e3), "unit": "nodes/s",
+                "nodes": len(idx), "call": "Evaluate(node, SP, PP, 1), host buffers, serial"}
 
     pk = peaks()
     kernel_ms = stats[4]
     flops = FLOP_PER_ITER_N3 * stats[0]
+    nl = max(stats[5], 1)
     achieved = flops / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else 0.0
+    aggregate = flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
     peak = pk["bf16_tflops_sustained"]
-    roof = {"kernel": "ipm_one_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
+    roof = {"kernel": "ipm_reg_one_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
             "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
                            f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
-            "launches": int(stats[5]), "avg_launch_us": 1e3 * kernel_ms / max(stats[5], 1),
+            "launches": int(stats[5]), "avg_launch_us": 1e3 * kernel_ms / nl,
             "ipm_iterations": int(stats[2]), "ipm_problems": int(stats[1]),
             "linesearch_factorizations": int(stats[3]),
             "flop_per_iteration": f"{FLOP_PER_ITER_N3} n^3",
-            "kernel_time_share": kernel_ms / ms if ms > 0 else None}
+            "aggregate_ipm_tflops": aggregate,
+            "aggregate_note": "all IPM flops of the value leg / its device time (engines run concurrently)",
+            "kernel_busy_share": kernel_ms / ms if ms > 0 else None}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -320,11 +371,17 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "nodes_per_step": B, "nodes_per_step_total": B * ws,
-                       "l2": "flushed (256 MB write) before every step", "precision": "FP64 throughout",
-                       "mode": "plain GPU drop-in (one node at a time)", "root_bound": arm.root_bound,
-                       "incumbent": arm.lb, "parallelism": f"replicas over nodes x{ws}"},
+                       "engines": T, "l2": "flushed (256 MB write) before every step",
+                       "precision": "FP64 throughout",
+                       "mode": f"{T} concurrent bounding engines (bqb_bound_nodes)",
+                       "root_bound": arm.root_bound, "incumbent": arm.lb,
+                       "mean_bound": float(np.mean(np.concatenate(bounds_dev))),
+                       "parallelism": f"replicas over nodes x{ws}",
+                       "sync": os.environ.get("BQB_SYNC", "auto")},
             "e2e": {"value": e2e, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps,
+                    "call": "bqb_bound_nodes with host nodes (subproblems built on the host)"},
+            "dropin_serial": drop,
             "gpu_launches": int(launches),
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -455,7 +512,10 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--nodes-per-step", type=int, default=64)
+    ap.add_argument("--nodes-per-step", type=int, default=512)
+    ap.add_argument("--threads", type=int, default=64, help="concurrent bounding engines per GPU")
+    ap.add_argument("--dropin-nodes", type=int, default=16,
+                    help="nodes timed through the serial drop-in Evaluate (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=64)

@@ -210,6 +210,29 @@ typedef struct bqb_solve_result {
 } bqb_solve_result;
 int bqb_solve(const double *adj, int num_vertices, const BiqBinParameters *prm, bqb_solve_result *out);
 
+/* The same B&B with `threads` nodes bounded at the same time, each by its
+ * own bounding engine (CUDA stream, device buffers, cut lists, random
+ * stream) on its own host thread: the reference's MPI workers
+ * (src/bab_functions.c:224-336, src/main.c:195-240) as engines of one
+ * process.  The root is bounded first on the library globals with rank 0;
+ * later nodes with rank 1.  Engine i draws its random numbers from the
+ * stream srandom(2021 + i) starts, so node order and heuristic cuts (not the
+ * optimum) can differ from the serial solver's.  threads <= 1: bqb_solve. */
+int bqb_solve_parallel(const double *adj, int num_vertices, const BiqBinParameters *prm, int threads,
+                       bqb_solve_result *out);
+
+/* Bound `count` independent nodes of the problem set up by
+ * process_adj_matrix (SP) with `threads` concurrent engines: bounds[i] is
+ * SDPbound(nodes[i], SP, <engine subproblem>, rank) (src/bounding.c:24-342)
+ * and nodes[i].fracsol is filled as SDPbound fills it.  L_dev: NULL (each
+ * subproblem is built on the host by createSubproblem), or count device
+ * pointers to the subproblem matrices createSubproblem would build (n x n,
+ * column-major, n = BabPbSize + 1 - fixed variables).  Returns 0, or 1 when
+ * SP is not set up.  No reference counterpart (the reference bounds one
+ * node per MPI process). */
+int bqb_bound_nodes(BabNode *nodes, int count, int rank, int threads, const double *const *L_dev,
+                    double *bounds);
+
 /* Bind the library to a CUDA device (default 0) and create its stream.
  * Called implicitly by every entry point; returns 0 on success. */
 int bqb_init(int device);

@@ -108,6 +108,9 @@ SIGNATURES = {
     "bqb_default_params": (None, [C.POINTER(Params)]),
     "bqb_read_params": (C.c_int, [C.c_char_p, C.POINTER(Params)]),
     "bqb_solve": (C.c_int, [D, C.c_int, C.c_void_p, C.c_void_p]),
+    "bqb_solve_parallel": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "bqb_bound_nodes": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(C.c_void_p), D]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),
     "bqb_kernel_launches": (C.c_ulonglong, []),
@@ -191,14 +194,19 @@ def make_params(**overrides) -> Params:
     return p
 
 
-def solve(adj: np.ndarray, **param_overrides) -> dict:
-    """Solve Max-Cut on ``adj`` to optimality (serial B&B, GPU bounding)."""
+def solve(adj: np.ndarray, threads: int = 1, **param_overrides) -> dict:
+    """Solve Max-Cut on ``adj`` to optimality (best-first B&B, GPU bounding;
+    ``threads`` > 1 bounds that many nodes concurrently)."""
     lib = load()
     A = np.ascontiguousarray(adj, dtype=np.float64)
     p = make_params(**param_overrides)
     res = SolveResult()
-    rc = lib.bqb_solve(dptr(A), A.shape[0], C.cast(C.pointer(p), C.c_void_p),
-                       C.cast(C.pointer(res), C.c_void_p))
+    pp = C.cast(C.pointer(p), C.c_void_p)
+    rp = C.cast(C.pointer(res), C.c_void_p)
+    if threads > 1:
+        rc = lib.bqb_solve_parallel(dptr(A), A.shape[0], pp, int(threads), rp)
+    else:
+        rc = lib.bqb_solve(dptr(A), A.shape[0], pp, rp)
     if rc != 0:
         raise RuntimeError(f"bqb_solve failed: {lib.bqb_last_error().decode()}")
     nv = A.shape[0]

@@ -20,8 +20,13 @@
 #include <string.h>
 #include <time.h>
 
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <vector>
 
+#include "engine.h"
 #include "globals.h"
 
 extern "C" {
@@ -36,7 +41,10 @@ __attribute__((visibility("default"))) BabSolution* BabSol = nullptr;
 namespace {
 
 constexpr double BIG_NUMBER = 1e9;
-double g_LB = 0.0;
+// The incumbent value is read by every concurrent bound; updates are
+// serialised so the value and BabSol change together.
+std::atomic<double> g_LB{0.0};
+std::mutex g_lb_mu;
 int g_num_nodes = 0;
 
 double wtime()
@@ -115,12 +123,13 @@ BabNode* new_node(const BabNode* parent)
 }  // namespace
 
 // ---- incumbent (src/heap.c:15, 172-193) -----------------------------------
-BQB_API double Bab_LBGet(void) { return g_LB; }
+BQB_API double Bab_LBGet(void) { return g_LB.load(); }
 
 BQB_API int Bab_LBUpd(double new_lb, BabSolution* bs)
 {
-    if (new_lb > g_LB) {
-        g_LB = new_lb;
+    std::lock_guard<std::mutex> lock(g_lb_mu);
+    if (new_lb > g_LB.load()) {
+        g_LB.store(new_lb);
         if (BabSol) *BabSol = *bs;
         return 1;
     }
@@ -234,6 +243,7 @@ BQB_API double Evaluate(BabNode* node, Problem* SP_, Problem* PP_, int rank)
 BQB_API int process_adj_matrix(double* Adj, int num_vertices)
 {
     BabPbSize = num_vertices - 1;
+    ++bqb::g_sp_generation;
     if (!SP) SP = (Problem*)calloc(1, sizeof(Problem));
     if (!PP) PP = (Problem*)calloc(1, sizeof(Problem));
     SP->n = num_vertices;
@@ -360,42 +370,37 @@ BQB_API int bqb_read_params(const char* path, BiqBinParameters* p)
 // driver, so their host copies are not allocated.
 static void alloc_globals(int N)
 {
-    auto dalloc = [](size_t n) { return (double*)calloc(n, sizeof(double)); };
+    // Only arrays this function allocated earlier are freed: a host program
+    // (or a binding) may have pointed the globals at memory of its own.
+    static std::vector<void*> owned;
+    auto give = [](void** slot, size_t count, size_t size) {
+        for (size_t q = 0; q < owned.size(); ++q)
+            if (owned[q] == *slot) {
+                free(*slot);
+                owned.erase(owned.begin() + q);
+                break;
+            }
+        *slot = calloc(count > 0 ? count : 1, size);
+        owned.push_back(*slot);
+    };
     const size_t mmax = (size_t)BQB_MAX_TRI_INEQ + BQB_MAX_PENT_INEQ + BQB_MAX_HEPTA_INEQ;
-    free(Cuts);
-    free(List);
-    free(Pent_Cuts);
-    free(Pent_List);
-    free(Hepta_Cuts);
-    free(Hepta_List);
-    Cuts = (Triangle_Inequality*)calloc(BQB_MAX_TRI_INEQ, sizeof(Triangle_Inequality));
-    List = (Triangle_Inequality*)calloc(params.TriIneq > 0 ? params.TriIneq : 1, sizeof(Triangle_Inequality));
-    Pent_Cuts = (Pentagonal_Inequality*)calloc(BQB_MAX_PENT_INEQ, sizeof(Pentagonal_Inequality));
-    Pent_List = (Pentagonal_Inequality*)calloc(params.PentIneq > 0 ? params.PentIneq : 1,
-                                               sizeof(Pentagonal_Inequality));
-    Hepta_Cuts = (Heptagonal_Inequality*)calloc(BQB_MAX_HEPTA_INEQ, sizeof(Heptagonal_Inequality));
-    Hepta_List = (Heptagonal_Inequality*)calloc(params.HeptaIneq > 0 ? params.HeptaIneq : 1,
-                                                sizeof(Heptagonal_Inequality));
-    free(X);
-    free(Z);
-    free(X_test);
-    X = dalloc((size_t)N * N);
-    Z = dalloc((size_t)N * N);
-    X_test = dalloc((size_t)N * N);
-    free(dual_gamma);
-    free(dgamma);
-    free(gamma_test);
-    free(eta);
-    free(g);
-    free(lambda);
-    free(F);
-    dual_gamma = dalloc(mmax);
-    dgamma = dalloc(mmax);
-    gamma_test = dalloc(mmax);
-    eta = dalloc(mmax);
-    g = dalloc(mmax);
-    lambda = dalloc(BQB_MAX_BUNDLE);
-    F = dalloc(BQB_MAX_BUNDLE);
+    const size_t nn = (size_t)N * N;
+    give((void**)&Cuts, BQB_MAX_TRI_INEQ, sizeof(Triangle_Inequality));
+    give((void**)&List, params.TriIneq, sizeof(Triangle_Inequality));
+    give((void**)&Pent_Cuts, BQB_MAX_PENT_INEQ, sizeof(Pentagonal_Inequality));
+    give((void**)&Pent_List, params.PentIneq, sizeof(Pentagonal_Inequality));
+    give((void**)&Hepta_Cuts, BQB_MAX_HEPTA_INEQ, sizeof(Heptagonal_Inequality));
+    give((void**)&Hepta_List, params.HeptaIneq, sizeof(Heptagonal_Inequality));
+    give((void**)&X, nn, sizeof(double));
+    give((void**)&Z, nn, sizeof(double));
+    give((void**)&X_test, nn, sizeof(double));
+    give((void**)&dual_gamma, mmax, sizeof(double));
+    give((void**)&dgamma, mmax, sizeof(double));
+    give((void**)&gamma_test, mmax, sizeof(double));
+    give((void**)&eta, mmax, sizeof(double));
+    give((void**)&g, mmax, sizeof(double));
+    give((void**)&lambda, BQB_MAX_BUNDLE, sizeof(double));
+    give((void**)&F, BQB_MAX_BUNDLE, sizeof(double));
 }
 
 // Serial best-first B&B to optimality on the GPU bounding path.  adj:
@@ -418,7 +423,7 @@ BQB_API int bqb_solve(const double* adj, int num_vertices, const BiqBinParameter
     srand(2020);
     if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
     memset(BabSol, 0, sizeof(BabSolution));
-    g_LB = 0.0;
+    g_LB.store(0.0);
     g_num_nodes = 0;
     stopped = 0;
     diff = 0.0;
@@ -460,6 +465,174 @@ BQB_API int bqb_solve(const double* adj, int num_vertices, const BiqBinParameter
             free(nd);
         }
     }
+    while (!heap.empty()) free(heap.pop());
+
+    if (out) {
+        out->best_value = Bab_LBGet();
+        out->root_bound = root_bound;
+        out->nodes = g_num_nodes;
+        out->stopped = stopped;
+        out->seconds = wtime() - TIME;
+        out->num_vertices = num_vertices;
+        for (int i = 0; i < BQB_NMAX; ++i) out->solution[i] = (i < BabPbSize) ? BabSol->X[i] : 0;
+    }
+    return 0;
+}
+
+// ---- concurrent bounding ----------------------------------------------------
+// Many nodes are bounded at the same time, each by its own engine (stream,
+// device buffers, host cut lists, random stream) on its own host thread; the
+// GPU runs their kernels side by side on different SMs.  This is the
+// reference's own parallelism (independent B&B nodes on MPI workers) with
+// engines in place of processes.
+
+namespace {
+
+std::mutex g_pool_mu;
+std::vector<bqb::Engine*> g_pool;
+
+// At least k private engines, sized for problems up to N x N.  Engine i
+// draws random numbers from the stream srand(2021 + i) would give.
+std::vector<bqb::Engine*>& engine_pool(int k, int N)
+{
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    while ((int)g_pool.size() < k) g_pool.push_back(bqb::engine_create(2021u + (unsigned)g_pool.size()));
+    for (int i = 0; i < k; ++i) g_pool[i]->ensure_private(N);
+    return g_pool;
+}
+
+}  // namespace
+
+// Bound `count` independent nodes of the problem in SP (set up by
+// process_adj_matrix) with `threads` concurrent engines; bounds[i] receives
+// the bound of nodes[i] (fracsol is filled as SDPbound does).  L_dev
+// (optional): device pointers to each node's subproblem matrix (PP->L as
+// createSubproblem builds it), used instead of building it on the host.
+BQB_API int bqb_bound_nodes(BabNode* nodes, int count, int rank, int threads, const double* const* L_dev,
+                            double* bounds)
+{
+    if (count <= 0) return 0;
+    if (!SP || !SP->L) return 1;
+    bqb::rt();
+    if (threads < 1) threads = 1;
+    if (threads > count) threads = count;
+    std::vector<bqb::Engine*>& pool = engine_pool(threads, SP->n);
+    std::atomic<int> next{0};
+    const int dev = bqb::rt().device;
+    auto work = [&](int t) {
+        bqb::t_pool_worker = t > 0;
+        BQB_CUDA(cudaSetDevice(dev));
+        bqb::Engine& E = *pool[t];
+        Problem& P = E.PP;
+        int i;
+        while ((i = next.fetch_add(1)) < count) {
+            if (L_dev) {
+                P.n = BabPbSize + 1 - countFixedVariables(&nodes[i]);
+                P.L = const_cast<double*>(L_dev[i]);
+            } else {
+                P.L = E.PPL.data();
+                createSubproblem(&nodes[i], SP, &P);
+            }
+            bounds[i] = bqb::sdp_bound(E, &nodes[i], SP, &P, rank);
+            P.L = E.PPL.data();
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < threads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    return 0;
+}
+
+// Best-first B&B to optimality with `threads` nodes bounded concurrently.
+// The root is bounded first with rank 0 (sets diff); then workers pop the
+// node with the largest upper bound, bound it with rank 1 and branch, as the
+// reference's MPI workers do.  With threads <= 1 this is bqb_solve.
+BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBinParameters* prm, int threads,
+                               bqb_solve_result* out)
+{
+    if (threads <= 1) return bqb_solve(adj, num_vertices, prm, out);
+    if (num_vertices < 3 || num_vertices > BQB_NMAX) return 1;
+    if (prm) {
+        params = *prm;
+    } else {
+        bqb_default_params(&params);
+        params.init_bundle_iter = 5;
+        params.violated_TriIneq = 0.05;
+    }
+    std::vector<double> A(adj, adj + (size_t)num_vertices * num_vertices);
+    process_adj_matrix(A.data(), num_vertices);
+    if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
+    srand(2020);
+    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
+    memset(BabSol, 0, sizeof(BabSolution));
+    g_LB.store(0.0);
+    g_num_nodes = 0;
+    stopped = 0;
+    diff = 0.0;
+    alloc_globals(SP->n);
+
+    TIME = wtime();
+    NodeHeap heap;
+    BabNode* root = new_node(nullptr);
+    ++g_num_nodes;
+    root_bound = Evaluate(root, SP, PP, 0);
+    root->upper_bound = root_bound;
+    std::mutex mu;
+    std::condition_variable cv;
+    int active = 0;
+    bool stop = false;
+    auto branch = [&](BabNode* node) {
+        const int ic = getBranchingVariable(node);
+        for (int xic = 0; xic <= 1; ++xic) {
+            BabNode* child = new_node(node);
+            child->xfixed[ic] = 1;
+            child->sol.X[ic] = xic;
+            ++g_num_nodes;
+            heap.push(child);
+        }
+    };
+    if (Bab_LBGet() + 1.0 < root->upper_bound && !params.root)
+        branch(root);
+    free(root);
+
+    std::vector<bqb::Engine*>& pool = engine_pool(threads, SP->n);
+    const int dev = bqb::rt().device;
+    auto work = [&](int t) {
+        bqb::t_pool_worker = t > 0;
+        BQB_CUDA(cudaSetDevice(dev));
+        bqb::Engine& E = *pool[t];
+        Problem& P = E.PP;
+        std::unique_lock<std::mutex> lk(mu);
+        while (true) {
+            cv.wait(lk, [&] { return !heap.empty() || active == 0 || stop; });
+            if (stop || heap.empty()) {
+                cv.notify_all();
+                return;
+            }
+            if (params.time_limit > 0 && (wtime() - TIME) > params.time_limit) {
+                stopped = 1;
+                stop = true;
+                cv.notify_all();
+                return;
+            }
+            BabNode* node = heap.pop();
+            ++active;
+            lk.unlock();
+            P.L = E.PPL.data();
+            createSubproblem(node, SP, &P);
+            node->upper_bound = bqb::sdp_bound(E, node, SP, &P, 1);
+            lk.lock();
+            if (Bab_LBGet() + 1.0 < node->upper_bound) branch(node);
+            free(node);
+            --active;
+            cv.notify_all();
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < threads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
     while (!heap.empty()) free(heap.pop());
 
     if (out) {

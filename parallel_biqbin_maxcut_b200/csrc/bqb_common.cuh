@@ -1,5 +1,6 @@
 // Shared device helpers and runtime plumbing for the B200 bounding path.
 #pragma once
+#include <atomic>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -141,8 +142,9 @@ struct HostBuf {
     }
 };
 
-// Process-wide runtime: one device, one stream (the reference is
-// single-threaded and not re-entrant; so is this layer).
+// Process-wide runtime: one device and the library stream the drop-in entry
+// points use (the reference is single-threaded and so are they); concurrent
+// bounding runs on engines with streams of their own.
 struct Runtime {
     int device = -1;
     int num_sms = 0;
@@ -152,8 +154,19 @@ struct Runtime {
 Runtime& rt();
 
 // Kernel-launch counter (reported by bench.py as gpu_launches).
-extern unsigned long long g_launches;
+extern std::atomic<unsigned long long> g_launches;
 #define BQB_COUNT_LAUNCH() (++::bqb::g_launches)
+
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is a per-function setting shared by every host thread, so it only
+// ever grows (a thread lowering it could invalidate another thread's launch
+// in flight between its own raise and launch).  Allocation-free.
+cudaError_t raise_smem_limit(const void* fn, size_t bytes);
+
+// Set on the bounding pool's worker threads (a fatal error there ends the
+// process with _exit rather than exit).
+extern thread_local bool t_pool_worker;
+#define BQB_SMEM_LIMIT(fn, bytes) BQB_CUDA(::bqb::raise_smem_limit((const void*)(fn), (size_t)(bytes)))
 
 inline void check_launch(const char* what)
 {

@@ -557,8 +557,7 @@ void lambda_eta_launch(BundleDev& b, const double* zeta_in, cudaStream_t s)
     const int kcap = b.cap;
     size_t bytes = le_smem_bytes(kcap > QP_SMEM_K ? QP_SMEM_K : kcap);
     if (kcap > QP_SMEM_K && 3 * (size_t)kcap * sizeof(double) > bytes) bytes = 3 * (size_t)kcap * sizeof(double);
-    BQB_CUDA(cudaFuncSetAttribute((const void*)lambda_eta_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    BQB_SMEM_LIMIT(lambda_eta_kernel, bytes);
     LeArgs a{b.G.p, b.ldg, b.slot.p, b.m, zeta_in, b.Fv.p, b.gam.p, b.lam.p, b.eta.p, b.dgam.p,
              b.gtest.p, b.dstate.p, b.istate.p, b.qp_ws.p, -1};
     lambda_eta_kernel<<<1, LE_THREADS, bytes, s>>>(a);
@@ -572,8 +571,7 @@ void solve_lambda_launch(int k, const double* Q, const double* c, double* lambda
     double* w = ws.ensure((size_t)2 * k * k + 8 * (size_t)k + 8);
     size_t bytes = 2 * (size_t)k * sizeof(double);
     if (k <= QP_SMEM_K) bytes += ((size_t)k * k + 5 * (size_t)k) * sizeof(double);
-    BQB_CUDA(cudaFuncSetAttribute((const void*)solve_lambda_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    BQB_SMEM_LIMIT(solve_lambda_kernel, bytes);
     solve_lambda_kernel<<<1, 32, bytes, s>>>(k, Q, c, lambda, err, w);
     BQB_COUNT_LAUNCH();
     check_launch("solve_lambda_kernel");

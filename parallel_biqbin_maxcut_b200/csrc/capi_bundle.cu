@@ -5,6 +5,7 @@
 
 #include <vector>
 
+#include "engine.h"
 #include "internal.h"
 #include "node.h"
 
@@ -12,10 +13,17 @@ using namespace bqb;
 
 namespace {
 
-NodeDev& dropin_dev()
+// The drop-in bundle entry points work on the reference's globals (like the
+// default engine) with device buffers of their own.
+Engine& dropin_engine()
 {
-    static NodeDev nd;
-    return nd;
+    static Engine* e = [] {
+        Engine* d = new Engine();
+        d->stream = rt().stream;
+        d->is_default = true;
+        return d;
+    }();
+    return *e;
 }
 
 void upload_identity_slots(BundleDev& b, int k, cudaStream_t s)
@@ -39,9 +47,10 @@ void upload_G(BundleDev& b, const double* Gh, int m, int k, cudaStream_t s)
 
 BQB_API void bundle_method(Problem* P, double* t, int bdl_iter)
 {
-    Runtime& R = rt();
-    cudaStream_t s = R.stream;
-    NodeDev& nd = dropin_dev();
+    rt();
+    Engine& E = dropin_engine();
+    cudaStream_t s = E.stream;
+    NodeDev& nd = E.nd;
     const int n = P->n;
     const size_t nn = (size_t)n * n;
     const int m = P->NIneq + P->NPentIneq + P->NHeptaIneq;
@@ -55,7 +64,7 @@ BQB_API void bundle_method(Problem* P, double* t, int bdl_iter)
     nd.out.ensure(4);
     BQB_CUDA(cudaMemcpyAsync(nd.L.p, P->L, nn * sizeof(double), cudaMemcpyHostToDevice, s));
     BQB_CUDA(cudaMemcpyAsync(nd.X.p, X, nn * sizeof(double), cudaMemcpyHostToDevice, s));
-    upload_cuts(nd, P, s);
+    upload_cuts(E, E.host(), P);
     BundleDev& b = nd.b;
     b.ensure_cap(k + bdl_iter + 2, n, s);
     upload_identity_slots(b, k, s);
@@ -76,7 +85,7 @@ BQB_API void bundle_method(Problem* P, double* t, int bdl_iter)
     BQB_CUDA(cudaMemcpyAsync(b.dstate.p, nd.hs.p, BD_WORDS * sizeof(double), cudaMemcpyHostToDevice, s));
     BQB_CUDA(cudaStreamSynchronize(s));
 
-    f = bundle_iterations(nd, bdl_iter, t, s);
+    f = bundle_iterations(E, bdl_iter, t);
 
     const int k2 = nd.hi.p[BI_K];
     const int kold = nd.hi.p[BI_KOLD];
@@ -109,9 +118,10 @@ BQB_API void bundle_method(Problem* P, double* t, int bdl_iter)
 BQB_API void lambda_eta(const Problem* P, double* zeta, double* Gh, double* gam, double* dgam, double* lam,
                         double* et, double* t)
 {
-    Runtime& R = rt();
-    cudaStream_t s = R.stream;
-    NodeDev& nd = dropin_dev();
+    rt();
+    Engine& E = dropin_engine();
+    cudaStream_t s = E.stream;
+    NodeDev& nd = E.nd;
     const int m = P->NIneq + P->NPentIneq + P->NHeptaIneq;
     const int k = P->bundle;
     BundleDev& b = nd.b;

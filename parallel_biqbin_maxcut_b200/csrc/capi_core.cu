@@ -12,21 +12,25 @@
 
 namespace bqb {
 
-// Pack the reference's global cut arrays (first P->NIneq / NPentIneq /
-// NHeptaIneq entries) into device records, dual-vector order.
-std::vector<CutRec> pack_global_cuts(const Problem* P)
+std::vector<CutRec> pack_cuts(const Triangle_Inequality* tc, int mt, const Pentagonal_Inequality* pc, int mp,
+                              const Heptagonal_Inequality* hc, int mh)
 {
     std::vector<CutRec> v;
-    v.reserve((size_t)P->NIneq + P->NPentIneq + P->NHeptaIneq);
-    for (int c = 0; c < P->NIneq; ++c) {
-        const int p[3] = {Cuts[c].i, Cuts[c].j, Cuts[c].k};
-        v.push_back(pack_cut(3, p, tri_negmask(Cuts[c].type)));
+    v.reserve((size_t)mt + mp + mh);
+    for (int c = 0; c < mt; ++c) {
+        const int p[3] = {tc[c].i, tc[c].j, tc[c].k};
+        v.push_back(pack_cut(3, p, tri_negmask(tc[c].type)));
     }
-    for (int c = 0; c < P->NPentIneq; ++c)
-        v.push_back(pack_cut(5, Pent_Cuts[c].permutation, pent_negmask(Pent_Cuts[c].type)));
-    for (int c = 0; c < P->NHeptaIneq; ++c)
-        v.push_back(pack_cut(7, Hepta_Cuts[c].permutation, hept_negmask(Hepta_Cuts[c].type)));
+    for (int c = 0; c < mp; ++c) v.push_back(pack_cut(5, pc[c].permutation, pent_negmask(pc[c].type)));
+    for (int c = 0; c < mh; ++c) v.push_back(pack_cut(7, hc[c].permutation, hept_negmask(hc[c].type)));
     return v;
+}
+
+// The reference's global cut arrays (first P->NIneq / NPentIneq / NHeptaIneq
+// entries).
+std::vector<CutRec> pack_global_cuts(const Problem* P)
+{
+    return pack_cuts(Cuts, P->NIneq, Pent_Cuts, P->NPentIneq, Hepta_Cuts, P->NHeptaIneq);
 }
 
 namespace {
@@ -57,12 +61,12 @@ void check_ipm_status_host(const double* out)
 
 // Device-level basic SDP bound for one problem (used by every caller).
 // xslot (optional, device): write X into dX + (*xslot) * n * n.
-void ipm_device(const double* dL, double* dX, int n, double* dout, cudaStream_t s, const int* xslot)
+void ipm_device(DevBuf<double>& wsbuf, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
+                const int* xslot)
 {
-    CoreState& c = core();
     size_t bytes = 0;
     const int place = ipm_place(n, rt().smem_optin, &bytes);
-    double* ws = c.ws.ensure(ipm_ws_doubles(n, place));
+    double* ws = wsbuf.ensure(ipm_ws_doubles(n, place));
     IpmDesc d{dL, dX, ws, dout, xslot, n, 0};
     ipm_launch_one(d, s);
 }
@@ -82,7 +86,7 @@ BQB_API void ipm_mc_pk(double* L, int n, double* Xout, double* phi, int print)
     double* dout = c.out.ensure(4);
     double* hout = c.hout.ensure(4);
     BQB_CUDA(cudaMemcpyAsync(dL, L, nn * sizeof(double), cudaMemcpyHostToDevice, R.stream));
-    ipm_device(dL, dX, n, dout, R.stream);
+    ipm_device(c.ws, dL, dX, n, dout, R.stream);
     BQB_CUDA(cudaMemcpyAsync(Xout, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaMemcpyAsync(hout, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, R.stream));
     BQB_CUDA(cudaStreamSynchronize(R.stream));
@@ -160,7 +164,7 @@ BQB_API double fct_eval(const Problem* PP_, double* gam, double* Xout, double* g
         BQB_CUDA(cudaMemcpyAsync(dt, gam, m * sizeof(double), cudaMemcpyHostToDevice, R.stream));
         opBt_launch(c.cuts, dL, n, dt, R.stream);
     }
-    ipm_device(dL, dX, n, dout, R.stream);
+    ipm_device(c.ws, dL, dX, n, dout, R.stream);
     double* dy = nullptr;
     if (m > 0) {
         dy = c.y.ensure(m);

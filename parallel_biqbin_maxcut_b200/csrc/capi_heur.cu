@@ -1,7 +1,7 @@
 // Heuristic entry points: runHeuristic, runHeuristic_unpacked, GW_heuristic,
 // mc_1opt, update_best.  The GPU does the factorisation, projection, 1-opt
 // and evaluation; the host keeps the reference's control flow and draws
-// every random number from rand() in the reference's order
+// every random number from the engine's stream in the reference's order
 // (src/heuristic.c:38-39, 103, 142-143), so for the same rand() state and
 // the same X the heuristic values and cuts are the reference's.
 #include <stdlib.h>
@@ -9,8 +9,10 @@
 
 #include <vector>
 
+#include "engine.h"
 #include "globals.h"
 #include "heur.cuh"
+#include "internal.h"
 
 extern "C" double evaluateSolution(int* sol);
 
@@ -50,19 +52,19 @@ void ensure_round_buffers(HeurState& st, int n, int N0, int num)
 }
 
 // Hyperplanes v_i = rand()/RAND_MAX - 0.5, count-major (src/heuristic.c:142-143).
-void draw_hyperplanes(HeurState& st, int n, int num, cudaStream_t s)
+void draw_hyperplanes(HeurState& st, Rng& rng, int n, int num, cudaStream_t s)
 {
     double* hv = st.hV.ensure((size_t)num * n);
     for (int c = 0; c < num; ++c)
-        for (int i = 0; i < n; ++i) hv[(size_t)c * n + i] = ((double)rand() / (double)(RAND_MAX)) - 0.5;
+        for (int i = 0; i < n; ++i) hv[(size_t)c * n + i] = ((double)rng.next() / (double)(RAND_MAX)) - 0.5;
     BQB_CUDA(cudaMemcpyAsync(st.V.p, hv, (size_t)num * n * sizeof(double), cudaMemcpyHostToDevice, s));
 }
 
 // Run one GW round on the factor already in st.Z; copy the best cut to x.
-double gw_round_host(HeurState& st, const double* dPL, int n, const double* dP0L, int N0, int num, int* x,
-                     cudaStream_t s)
+double gw_round_host(HeurState& st, Rng& rng, const double* dPL, int n, const double* dP0L, int N0, int num,
+                     int* x, cudaStream_t s)
 {
-    draw_hyperplanes(st, n, num, s);
+    draw_hyperplanes(st, rng, n, num, s);
     BQB_CUDA(cudaMemsetAsync(st.status.p, 0, 2 * sizeof(int), s));
     gw_round_device(st, dPL, n, dP0L, N0, num, s);
     BQB_CUDA(cudaMemcpyAsync(st.hbest.p, st.best.p, (size_t)N0 * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -78,17 +80,16 @@ double gw_round_host(HeurState& st, const double* dPL, int n, const double* dP0L
 
 // runHeuristic_unpacked (src/heuristic.c:19-115) with device-resident X, P_L
 // and P0_L.  x: host, length N0 - 1.
-double heuristic_device(const double* dX, const double* dPL, int n, const double* dP0L, int N0,
-                        const int* xfixed, const int* sol, int* x, cudaStream_t s)
+double heuristic_device(HeurState& st, Rng& rng, const double* dX, const double* dPL, int n, const double* dP0L,
+                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s)
 {
-    HeurState& st = heur_state();
     const int N = N0 - 1;
     const int num = N0;
     ensure_round_buffers(st, n, N0, num);
     upload_fixed(st, xfixed, sol, N, s);
 
     std::vector<double> xh(n);
-    for (int i = 0; i < n; ++i) xh[i] = 2 * (rand() % 2) - 1;
+    for (int i = 0; i < n; ++i) xh[i] = 2 * (rng.next() % 2) - 1;
     // fh = value of the random cut lifted with the fixed variables
     {
         std::vector<int> tx(N);
@@ -121,7 +122,7 @@ double heuristic_device(const double* dX, const double* dPL, int n, const double
             fatal("runHeuristic_unpacked", "Problem with Cholesky factorization");
             return heur_val;
         }
-        heur_val = gw_round_host(st, dPL, n, dP0L, N0, num, x, s);
+        heur_val = gw_round_host(st, rng, dPL, n, dP0L, N0, num, x, s);
         if (heur_val > fh) {
             done = 0;
             fh = heur_val;
@@ -130,7 +131,7 @@ double heuristic_device(const double* dX, const double* dPL, int n, const double
                 if (!xfixed[i]) xh[idx++] = 2 * x[i] - 1;
             xh[n - 1] = -1.0;
         }
-        const double c = 0.3 + 0.6 * ((double)rand() / (double)(RAND_MAX));
+        const double c = 0.3 + 0.6 * ((double)rng.next() / (double)(RAND_MAX));
         BQB_CUDA(cudaMemcpyAsync(dxh.p, xh.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
         remix_device(st.Z.p, dX, dxh.p, c, n, s);
         BQB_CUDA(cudaStreamSynchronize(s));   // xh is reused on the host
@@ -165,7 +166,8 @@ BQB_API double runHeuristic_unpacked(double* P0_L, int P0_N, double* P_L, int P_
     BQB_CUDA(cudaMemcpyAsync(dX, X, nn * sizeof(double), cudaMemcpyHostToDevice, R.stream));
     BQB_CUDA(cudaMemcpyAsync(dPL, P_L, nn * sizeof(double), cudaMemcpyHostToDevice, R.stream));
     BQB_CUDA(cudaMemcpyAsync(dP0L, P0_L, NN * sizeof(double), cudaMemcpyHostToDevice, R.stream));
-    return heuristic_device(dX, dPL, P_N, dP0L, P0_N, node_xfixed, node_sol_X, x, R.stream);
+    Engine& E = default_engine();
+    return heuristic_device(E.heur, E.rng, dX, dPL, P_N, dP0L, P0_N, node_xfixed, node_sol_X, x, R.stream);
 }
 
 BQB_API double runHeuristic(Problem* P0, Problem* P, BabNode* node, int* x)
@@ -179,7 +181,7 @@ BQB_API double GW_heuristic(double* P0_L, int P0_N, double* P_L, int P_N, int* n
                             int* x, int num)
 {
     Runtime& R = rt();
-    HeurState& st = heur_state();
+    HeurState& st = default_engine().heur;
     HeurStage& h = hstage();
     const size_t nn = (size_t)P_N * P_N, NN = (size_t)P0_N * P0_N;
     ensure_round_buffers(st, P_N, P0_N, num > 0 ? num : 1);
@@ -190,7 +192,7 @@ BQB_API double GW_heuristic(double* P0_L, int P0_N, double* P_L, int P_N, int* n
     BQB_CUDA(cudaMemcpyAsync(dP0L, P0_L, NN * sizeof(double), cudaMemcpyHostToDevice, R.stream));
     upload_fixed(st, node_xfixed, node_sol_X, P0_N - 1, R.stream);
     if (num <= 0) return -BIG_NUMBER;
-    return gw_round_host(st, dPL, P_N, dP0L, P0_N, num, x, R.stream);
+    return gw_round_host(st, default_engine().rng, dPL, P_N, dP0L, P0_N, num, x, R.stream);
 }
 
 // mc_1opt (src/heuristic.c:195-296): x in +-1 form, improved in place;
@@ -198,7 +200,7 @@ BQB_API double GW_heuristic(double* P0_L, int P0_N, double* P_L, int P_N, int* n
 BQB_API double mc_1opt(int* x, double* P_L, int P_N)
 {
     Runtime& R = rt();
-    HeurState& st = heur_state();
+    HeurState& st = default_engine().heur;
     HeurStage& h = hstage();
     const size_t nn = (size_t)P_N * P_N;
     st.x.ensure((size_t)P_N);

@@ -8,6 +8,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include "engine.h"
+#include "node.h"
 #include "separation.h"
 
 namespace bqb {
@@ -25,11 +27,7 @@ struct Key8Hash {
 };
 }  // namespace
 
-TriSepState& trisep_state()
-{
-    static TriSepState s;
-    return s;
-}
+TriSepState& trisep_state() { return default_engine().tri; }
 
 int tri_purge(Triangle_Inequality* cuts, int n_ineq, const double* y)
 {
@@ -185,39 +183,58 @@ BQB_API double updateTriangleInequalities(Problem* P, double* y, int* NumAdded, 
 
 BQB_API double getViolated_PentagonalInequalities(double* Xm, int N, Pentagonal_Inequality* Lst, int* ListSize)
 {
-    return pent_separate(Xm, N, Lst, ListSize);
+    return pent_separate(Xm, N, Lst, ListSize, default_engine().rng);
 }
 
 BQB_API double getViolated_HeptagonalInequalities(double* Xm, int N, Heptagonal_Inequality* Lst, int* ListSize)
 {
-    return hept_separate(Xm, N, Lst, ListSize);
+    return hept_separate(Xm, N, Lst, ListSize, default_engine().rng);
 }
 
-BQB_API double updatePentagonalInequalities(Problem* P, double* y, int* NumAdded, int* NumSubtracted, int triag)
+namespace bqb {
+
+double pent_update(HostState& H, Problem* P, const double* y, int* NumAdded, int* NumSubtracted, int triag, Rng& rng)
 {
-    const int kept = pent_purge(Pent_Cuts, P->NPentIneq, y + triag);
+    const int kept = pent_purge(H.pcuts, P->NPentIneq, y + triag);
     const int subtracted = P->NPentIneq - kept;
     P->NPentIneq = kept;
     int size = 0;
-    const double mn = pent_separate(X, P->n, Pent_List, &size);
-    const int added = pent_append(Pent_Cuts, kept, Pent_List, size);
+    const double mn = pent_separate(H.X, P->n, H.plist, &size, rng);
+    const int added = pent_append(H.pcuts, kept, H.plist, size);
     P->NPentIneq += added;
     *NumAdded = added;
     *NumSubtracted = subtracted;
     return mn;
 }
 
-BQB_API double updateHeptagonalInequalities(Problem* P, double* y, int* NumAdded, int* NumSubtracted,
-                                            int hept_index)
+double hept_update(HostState& H, Problem* P, const double* y, int* NumAdded, int* NumSubtracted, int hept_index,
+                   Rng& rng)
 {
-    const int kept = hept_purge(Hepta_Cuts, P->NHeptaIneq, y + hept_index);
+    const int kept = hept_purge(H.hcuts, P->NHeptaIneq, y + hept_index);
     const int subtracted = P->NHeptaIneq - kept;
     P->NHeptaIneq = kept;
     int size = 0;
-    const double mn = hept_separate(X, P->n, Hepta_List, &size);
-    const int added = hept_append(Hepta_Cuts, kept, Hepta_List, size);
+    const double mn = hept_separate(H.X, P->n, H.hlist, &size, rng);
+    const int added = hept_append(H.hcuts, kept, H.hlist, size);
     P->NHeptaIneq += added;
     *NumAdded = added;
     *NumSubtracted = subtracted;
     return mn;
+}
+
+}  // namespace bqb
+
+BQB_API double updatePentagonalInequalities(Problem* P, double* y, int* NumAdded, int* NumSubtracted, int triag)
+{
+    Engine& E = default_engine();
+    HostState H = E.host();
+    return pent_update(H, P, y, NumAdded, NumSubtracted, triag, E.rng);
+}
+
+BQB_API double updateHeptagonalInequalities(Problem* P, double* y, int* NumAdded, int* NumSubtracted,
+                                            int hept_index)
+{
+    Engine& E = default_engine();
+    HostState H = E.host();
+    return hept_update(H, P, y, NumAdded, NumSubtracted, hept_index, E.rng);
 }

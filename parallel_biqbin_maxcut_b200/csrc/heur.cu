@@ -23,12 +23,6 @@
 
 namespace bqb {
 
-HeurState& heur_state()
-{
-    static HeurState s;
-    return s;
-}
-
 namespace {
 
 constexpr int POTRF_THREADS = 512;
@@ -197,8 +191,7 @@ void potrf_device(double* dZ, int n, int* dstatus, cudaStream_t s)
     const size_t need = ((size_t)((n + 1) & ~1) + (size_t)n * n) * sizeof(double);
     const int in_smem = need <= rt().smem_optin ? 1 : 0;
     const size_t bytes = in_smem ? need : (size_t)((n + 1) & ~1) * sizeof(double);
-    BQB_CUDA(cudaFuncSetAttribute((const void*)potrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
+    BQB_SMEM_LIMIT(potrf_kernel, bytes);
     potrf_kernel<<<1, POTRF_THREADS, bytes, s>>>(dZ, n, dstatus, in_smem);
     BQB_COUNT_LAUNCH();
     check_launch("potrf_kernel");
@@ -222,8 +215,7 @@ void one_opt_device(HeurState& st, const double* dPL, int n, int count, cudaStre
 {
     const int warps = 4;
     const size_t bytes = one_opt_smem(n, warps);
-    BQB_CUDA(cudaFuncSetAttribute((const void*)one_opt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bytes));
+    BQB_SMEM_LIMIT(one_opt_kernel, bytes);
     one_opt_kernel<<<(count + warps - 1) / warps, warps * 32, bytes, s>>>(dPL, n, st.x.p, count, st.vals.p,
                                                                          st.status.p);
     BQB_COUNT_LAUNCH();

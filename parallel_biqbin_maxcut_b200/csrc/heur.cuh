@@ -22,8 +22,6 @@ struct HeurState {
     HostBuf<int> hstat;
 };
 
-HeurState& heur_state();
-
 // Z <- lower Cholesky factor of Z (n x n) in place; *dstatus = 0 ok, 1 not PD.
 void potrf_device(double* dZ, int n, int* dstatus, cudaStream_t s);
 

@@ -13,12 +13,13 @@
 #include <vector>
 
 #include "globals.h"
+#include "rng.h"
 
 namespace bqb {
 
 // declared for the other translation units in separation.h
-double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size);
-double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size);
+double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng);
+double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size, Rng& rng);
 
 namespace {
 constexpr double BIG_NUMBER = 1e9;   // src/biqbin.h:35
@@ -42,8 +43,9 @@ using namespace bqb;
 // (n(n-1)), n inner steps at the start, t *= 0.6 and steps *= 1.1 per round,
 // random transposition (i1 < k, i2 < n), Metropolis acceptance with
 // exp(-delta/t) unless delta/t > 5; stops after a round with no accepted
-// move of size > 0.001.  rand() is consumed in the reference's order.
-BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* ineq)
+// move of size > 0.001.  Random numbers are drawn in the reference's order.
+namespace bqb {
+double qap_sa(const int* H, int k, const double* Xm, int n, int* ineq, Rng& rng)
 {
     const int inner_iter = n;
     const double reduce_temp = 0.6;
@@ -58,7 +60,7 @@ BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* in
     std::vector<int> perm(n), best(n, 0);
     for (int i = 0; i < n; ++i) perm[i] = i;
     for (int i = n - 1; i > 0; --i) {
-        const int r = rand() % i;
+        const int r = rng.next() % i;
         const int tmp = perm[i];
         perm[i] = perm[r];
         perm[r] = tmp;
@@ -72,8 +74,8 @@ BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* in
     while (not_done > 0) {
         not_done = 0;
         for (int it = 0; it < m1; ++it) {
-            int i1 = rand() % k;
-            int i2 = rand() % n;
+            int i1 = rng.next() % k;
+            int i2 = rng.next() % n;
             if (i2 < i1) {
                 const int tmp = i1;
                 i1 = i2;
@@ -97,7 +99,7 @@ BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* in
                 if (dt1 > 5)
                     accept = 0;
                 else
-                    accept = ((double)rand() / ((double)RAND_MAX)) < exp(-dt1) ? 1 : 0;
+                    accept = ((double)rng.next() / ((double)RAND_MAX)) < exp(-dt1) ? 1 : 0;
             } else {
                 accept = 1;
             }
@@ -119,6 +121,14 @@ BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* in
     for (int i = 0; i < k; ++i) ineq[i] = best[i];
     return cost;
 }
+}  // namespace bqb
+
+BQB_API double qap_simulated_annealing(int* H, int k, double* Xm, int n, int* ineq)
+{
+    Rng glibc;
+    return qap_sa(H, k, Xm, n, ineq, glibc);
+}
+
 
 namespace bqb {
 
@@ -127,7 +137,7 @@ namespace bqb {
 // re-scan that starts from BIG_NUMBER and looks for a larger value.
 template <int K, class Ineq>
 static double kgon_separate(const double* Xh, int N, Ineq* list, int* list_size, int trials, int types,
-                            int cap)
+                            int cap, Rng& rng)
 {
     int size = 0, least = 0;
     double least_val = -BIG_NUMBER;
@@ -137,7 +147,7 @@ static double kgon_separate(const double* Xh, int N, Ineq* list, int* list_size,
     for (int trial = 0; trial < trials; ++trial) {
         for (int type = 1; type <= types; ++type) {
             kgon_H(K, type, H);
-            const double v = qap_simulated_annealing(H, K, const_cast<double*>(Xh), N, perm);
+            const double v = qap_sa(H, K, Xh, N, perm, rng);
             min_all = v < min_all ? v : min_all;
             if (!(v < 1.0)) continue;
             if (size < cap) {
@@ -166,14 +176,14 @@ static double kgon_separate(const double* Xh, int N, Ineq* list, int* list_size,
     return min_all;
 }
 
-double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size)
+double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng)
 {
-    return kgon_separate<5>(Xh, N, list, size, params.Pent_Trials, 3, params.PentIneq);
+    return kgon_separate<5>(Xh, N, list, size, params.Pent_Trials, 3, params.PentIneq, rng);
 }
 
-double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size)
+double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size, Rng& rng)
 {
-    return kgon_separate<7>(Xh, N, list, size, params.Hepta_Trials, 4, params.HeptaIneq);
+    return kgon_separate<7>(Xh, N, list, size, params.Hepta_Trials, 4, params.HeptaIneq, rng);
 }
 
 }  // namespace bqb

@@ -6,23 +6,30 @@
 #include "bqb_common.cuh"
 #include "cuts.cuh"
 #include "globals.h"
+#include "heur.cuh"
+#include "rng.h"
 
 namespace bqb {
 
 // Basic SDP bound of one n x n problem already on the device (one launch).
-// dout: 4 doubles (phi, iterations, status, <L,X>).  xslot (optional,
-// device): write X into dX + (*xslot) * n * n.
-void ipm_device(const double* dL, double* dX, int n, double* dout, cudaStream_t s,
+// ws: the caller's IPM scratch (grown as needed).  dout: 4 doubles (phi,
+// iterations, status, <L,X>).  xslot (optional, device): write X into
+// dX + (*xslot) * n * n.
+void ipm_device(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
                 const int* xslot = nullptr);
 
 // Raise the reference's fatal error for a non-zero IPM status word.
 void check_ipm_status_host(const double* out);
 
-// Pack the reference's global cut arrays into device records.
+// Pack cut lists into device records (dual-vector order tri | pent | hept).
+std::vector<CutRec> pack_cuts(const Triangle_Inequality* c, int mt, const Pentagonal_Inequality* p, int mp,
+                              const Heptagonal_Inequality* h, int mh);
+// The same for the reference's global cut arrays with P's counts.
 std::vector<CutRec> pack_global_cuts(const Problem* P);
 
-// runHeuristic_unpacked with device X, P_L and P0_L (capi_heur.cu).
-double heuristic_device(const double* dX, const double* dPL, int n, const double* dP0L, int N0,
-                        const int* xfixed, const int* sol, int* x, cudaStream_t s);
+// runHeuristic_unpacked (src/heuristic.c:19-115) with device X, P_L and
+// P0_L, device state st and random stream rng.  x: host, length N0 - 1.
+double heuristic_device(HeurState& st, Rng& rng, const double* dX, const double* dPL, int n, const double* dP0L,
+                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s);
 
 }  // namespace bqb

@@ -1,13 +1,15 @@
-// Bounding of one B&B node with all matrices resident in HBM.
+// Bounding of one B&B node with all matrices resident in HBM, in an engine.
 //
-// SDPbound restates src/bounding.c:24-342 line for line in its control
-// flow (the same tests, constants and parameter use); every matrix
-// operation runs on the device: the basic IPM, the heuristic, the triangle
-// separation, the bundle iterations (lambda_eta, fct_eval, step
-// bookkeeping) and the subgradient rebuild after the cuts change.  The host
-// keeps the cut lists (the reference's global arrays) and reads back only
-// scalars, the separated triangle list, X's last column (fracsol) and, when
-// pentagonal / heptagonal separation runs, X itself.
+// sdp_bound restates src/bounding.c:24-342 line for line in its control flow
+// (the same tests, constants and parameter use); every matrix operation runs
+// on the device: the basic IPM, the heuristic, the triangle separation, the
+// bundle iterations (lambda_eta, fct_eval, step bookkeeping) and the
+// subgradient rebuild after the cuts change.  The host keeps the cut lists
+// (the reference's global arrays, or the engine's private copies) and reads
+// back only scalars, the separated triangle list, X's last column
+// (fracsol) and, when pentagonal / heptagonal separation runs, X itself.
+// Everything runs on the engine's stream, so engines bound nodes
+// concurrently.
 #include <math.h>
 #include <string.h>
 
@@ -27,28 +29,22 @@ extern double diff;
 
 namespace bqb {
 
-NodeDev& node_dev()
+void upload_cuts(Engine& E, const HostState& H, const Problem* P)
 {
-    static NodeDev nd;
-    return nd;
+    std::vector<CutRec> rec = pack_cuts(H.cuts, P->NIneq, H.pcuts, P->NPentIneq, H.hcuts, P->NHeptaIneq);
+    E.nd.cuts.upload(rec, P->NIneq, P->NPentIneq, P->NHeptaIneq, E.stream);
+    E.nd.b.ensure_m(E.nd.cuts.m, E.stream);
 }
 
-void upload_cuts(NodeDev& nd, const Problem* P, cudaStream_t s)
+double tri_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* added, int* subtracted)
 {
-    std::vector<CutRec> rec = pack_global_cuts(P);
-    nd.cuts.upload(rec, P->NIneq, P->NPentIneq, P->NHeptaIneq, s);
-    nd.b.ensure_m(nd.cuts.m, s);
-}
-
-double tri_update_dev(NodeDev& nd, Problem* P, const double* y, int* added, int* subtracted, cudaStream_t s)
-{
-    const int kept = tri_purge(Cuts, P->NIneq, y);
+    const int kept = tri_purge(H.cuts, P->NIneq, y);
     *subtracted = P->NIneq - kept;
     P->NIneq = kept;
-    TriSepState& st = trisep_state();
     int size = 0;
-    const double mx = trisep_device(st, nd.X.p, P->n, params.TriIneq, params.violated_TriIneq, &size, s);
-    *added = tri_append(Cuts, kept, st.hlist.p, size);
+    const double mx =
+        trisep_device(E.tri, E.nd.X.p, P->n, params.TriIneq, params.violated_TriIneq, &size, E.stream);
+    *added = tri_append(H.cuts, kept, E.tri.hlist.p, size);
     P->NIneq += *added;
     return mx;
 }
@@ -65,9 +61,11 @@ static void fetch_state(NodeDev& nd, cudaStream_t s)
     if (err & 8) fatal("bundle_method", "no free bundle slot");
 }
 
-double bundle_iterations(NodeDev& nd, int bdl_iter, double* t, cudaStream_t s)
+double bundle_iterations(Engine& E, int bdl_iter, double* t)
 {
+    NodeDev& nd = E.nd;
     BundleDev& b = nd.b;
+    cudaStream_t s = E.stream;
     const int n = nd.n;
     const size_t nn = (size_t)n * n;
     nd.hs.ensure(8);
@@ -85,7 +83,7 @@ double bundle_iterations(NodeDev& nd, int bdl_iter, double* t, cudaStream_t s)
         lambda_eta_launch(b, nullptr, s);
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, nd.L.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
         if (nd.cuts.m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gtest.p, s);
-        ipm_device(nd.L0.p, b.Xb.p, n, nd.out.p, s, b.istate.p + BI_NEXT);
+        ipm_device(E.ipm_ws, nd.L0.p, b.Xb.p, n, nd.out.p, s, b.istate.p + BI_NEXT);
         if (nd.cuts.m > 0)
             opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
         bundle_step_launch(b, nd.out.p, nd.L.p, s);
@@ -96,16 +94,12 @@ double bundle_iterations(NodeDev& nd, int bdl_iter, double* t, cudaStream_t s)
     return nd.hs.p[BD_F];
 }
 
-}  // namespace bqb
-
-using namespace bqb;
-
-// SDPbound (src/bounding.c:24-342).
-BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
+// SDPbound (src/bounding.c:24-342) in engine E.
+double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
 {
-    Runtime& R = rt();
-    cudaStream_t s = R.stream;
-    NodeDev& nd = node_dev();
+    cudaStream_t s = E.stream;
+    NodeDev& nd = E.nd;
+    HostState H = E.host();
     const int n = PP_->n;
     const int N0 = SP_->n;
     const int NB = N0 - 1;   // BabPbSize
@@ -120,11 +114,13 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
     double* dout = nd.out.ensure(4);
     // PP->L may be host or device memory (unified addressing decides)
     BQB_CUDA(cudaMemcpyAsync(dL, PP_->L, nn * sizeof(double), cudaMemcpyDefault, s));
-    if (nd.P0L_src != SP_->L || nd.P0N != N0) {
+    const unsigned gen = g_sp_generation.load();
+    if (nd.P0L_src != SP_->L || nd.P0N != N0 || nd.P0L_gen != gen) {
         nd.P0L.ensure((size_t)N0 * N0);
         BQB_CUDA(cudaMemcpyAsync(nd.P0L.p, SP_->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice, s));
         nd.P0L_src = SP_->L;
         nd.P0N = N0;
+        nd.P0L_gen = gen;
     }
     std::vector<int> x(NB > 0 ? NB : 1);
     std::vector<double> col(n);
@@ -141,7 +137,7 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
     };
     auto heuristic = [&]() {
         for (int i = 0; i < NB; ++i) x[i] = node->xfixed[i] ? node->sol.X[i] : 0;
-        heuristic_device(dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
+        heuristic_device(E.heur, E.rng, dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
         updateSolution(x.data());
     };
 
@@ -151,11 +147,11 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
     PP_->NPentIneq = 0;
     PP_->NHeptaIneq = 0;
     int tri_add = 0, tri_sub = 0, pent_add = 0, pent_sub = 0, hept_add = 0, hept_sub = 0;
-    double viol3 = 0.0, viol5 = 0.0, viol7 = 0.0;
-    (void)viol7;
+    double viol3 = 0.0, viol5 = 0.0;
+    double& f = *H.f;
 
     // basic SDP relaxation
-    ipm_device(dL, dX, n, dout, s);
+    ipm_device(E.ipm_ws, dL, dX, n, dout, s);
     BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaStreamSynchronize(s));
     check_ipm_status_host(nd.hs.p);
@@ -168,16 +164,16 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
     if (bound < Bab_LBGet() + 1.0) return bound;
     if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) return bound;
 
-    viol3 = tri_update_dev(nd, PP_, dual_gamma, &tri_add, &tri_sub, s);
-    for (int i = 0; i < PP_->NIneq; ++i) dual_gamma[i] = Cuts[i].y;
+    viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
+    for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
     double t = 0.5 * (bound - Bab_LBGet()) / (PP_->NIneq * viol3 * viol3);
 
     // bundle init: X_bundle(0) = X, G(:,0) = 1 - B(X), F(0) = <L,X>, bundle = 1
-    upload_cuts(nd, PP_, s);
+    upload_cuts(E, H, PP_);
     BundleDev& b = nd.b;
     b.ensure_cap(1 + bdl_iter + 2, n, s);
     const int m0 = nd.cuts.m;
-    BQB_CUDA(cudaMemcpyAsync(b.gam.p, dual_gamma, (size_t)m0 * sizeof(double), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(b.gam.p, H.dual_gamma, (size_t)m0 * sizeof(double), cudaMemcpyHostToDevice, s));
     BQB_CUDA(cudaMemcpyAsync(b.Xb.p, dX, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
     opB_launch(nd.cuts, b.Xb.p, nn, nullptr, 1, n, b.G.p, b.ldg, true, s);
     {
@@ -199,11 +195,10 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
 
     int count = 0;
     bool done = false, prune = false, giveup = false;
-    std::vector<double> hX;
     while (!done) {
         ++count;
         const double oldf = f;
-        f = bundle_iterations(nd, bdl_iter, &t, s);
+        f = bundle_iterations(E, bdl_iter, &t);
         bound = f + fixedvalue;
         prune = bound < Bab_LBGet() + 1.0;
         if (!prune) {
@@ -221,19 +216,18 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
             const int triag = PP_->NIneq;
             const int penta = PP_->NPentIneq;
             const int m = PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq;
-            BQB_CUDA(cudaMemcpyAsync(dual_gamma, b.gam.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaMemcpyAsync(H.dual_gamma, b.gam.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
-            viol3 = tri_update_dev(nd, PP_, dual_gamma, &tri_add, &tri_sub, s);
+            viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
             const bool do_pent = params.include_Pent && (count > params.triag_iter || viol3 < 0.2);
-            const bool do_hept_pre = params.include_Hepta;
-            if (do_pent || do_hept_pre) {
-                BQB_CUDA(cudaMemcpyAsync(X, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+            if (do_pent || params.include_Hepta) {
+                BQB_CUDA(cudaMemcpyAsync(H.X, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
                 BQB_CUDA(cudaStreamSynchronize(s));
             }
-            if (do_pent) viol5 = updatePentagonalInequalities(PP_, dual_gamma, &pent_add, &pent_sub, triag);
+            if (do_pent) viol5 = pent_update(H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag, E.rng);
             if (params.include_Hepta &&
                 ((count > params.triag_iter + params.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4))))
-                viol7 = updateHeptagonalInequalities(PP_, dual_gamma, &hept_add, &hept_sub, triag + penta);
+                hept_update(H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta, E.rng);
         } else {
             tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
         }
@@ -241,13 +235,13 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
         store_fracsol();
 
         if (!done) {
-            for (int i = 0; i < PP_->NIneq; ++i) dual_gamma[i] = Cuts[i].y;
-            for (int i = 0; i < PP_->NPentIneq; ++i) dual_gamma[i + PP_->NIneq] = Pent_Cuts[i].y;
+            for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
+            for (int i = 0; i < PP_->NPentIneq; ++i) H.dual_gamma[i + PP_->NIneq] = H.pcuts[i].y;
             for (int i = 0; i < PP_->NHeptaIneq; ++i)
-                dual_gamma[i + PP_->NIneq + PP_->NPentIneq] = Hepta_Cuts[i].y;
-            upload_cuts(nd, PP_, s);
+                H.dual_gamma[i + PP_->NIneq + PP_->NPentIneq] = H.hcuts[i].y;
+            upload_cuts(E, H, PP_);
             const int m = nd.cuts.m;
-            BQB_CUDA(cudaMemcpyAsync(b.gam.p, dual_gamma, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
+            BQB_CUDA(cudaMemcpyAsync(b.gam.p, H.dual_gamma, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
             // current bundle size (host copy) for capacity and the G rebuild
             BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
@@ -258,7 +252,7 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
             // fct_eval(PP, dual_gamma, X_test, g) into the free slot
             BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
             if (m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gam.p, s);
-            ipm_device(nd.L0.p, b.Xb.p, n, dout, s, b.istate.p + BI_NEXT);
+            ipm_device(E.ipm_ws, nd.L0.p, b.Xb.p, n, dout, s, b.istate.p + BI_NEXT);
             // G(:, i) = 1 - B(X_bundle(i)) for the bundle, then g for the new element
             opB_launch(nd.cuts, b.Xb.p, nn, b.slot.p, k, n, b.G.p, b.ldg, true, s);
             opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
@@ -277,4 +271,16 @@ BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
     bound = f + fixedvalue;
     if (rank == 0) diff = basic_bound - bound;
     return bound;
+}
+
+}  // namespace bqb
+
+using namespace bqb;
+
+// SDPbound (src/bounding.c:24-342) in the default engine: the reference's
+// globals and rand() stream.
+BQB_API double SDPbound(BabNode* node, Problem* SP_, Problem* PP_, int rank)
+{
+    rt();
+    return sdp_bound(default_engine(), node, SP_, PP_, rank);
 }

@@ -1,38 +1,25 @@
-// Device-resident state of the node being bounded, and the bounding driver.
+// The device-resident bounding driver (SDPbound) and its pieces.
 #pragma once
-#include "bundle.cuh"
-#include "cuts.cuh"
-#include "globals.h"
+#include "engine.h"
 
 namespace bqb {
 
-struct NodeDev {
-    int n = 0;
-    DevBuf<double> L;      // PP->L (n x n)
-    DevBuf<double> L0;     // L - B^T(gamma) scratch
-    DevBuf<double> X;      // the reference's global X (current primal matrix)
-    DevBuf<double> out;    // IPM output words
-    DevBuf<double> P0L;    // SP->L (N0 x N0)
-    int P0N = 0;
-    const double* P0L_src = nullptr;
-    DevCuts cuts;
-    BundleDev b;
-    HostBuf<double> hs;    // pinned scratch for small reads
-    HostBuf<int> hi;
-};
+// bdl_iter iterations of src/bundle.c:47-235 on the engine's device-resident
+// bundle; t in/out on the host.  Synchronises once at the end; returns f.
+double bundle_iterations(Engine& E, int bdl_iter, double* t);
 
-NodeDev& node_dev();
-
-// bdl_iter iterations of src/bundle.c:47-235 on the device-resident bundle;
-// t in/out on the host.  Synchronises once at the end and returns f.
-double bundle_iterations(NodeDev& nd, int bdl_iter, double* t, cudaStream_t s);
-
-// Pack the current host cut lists (globals) and upload them with their
-// pair CSR; resize the bundle's m-vectors.
-void upload_cuts(NodeDev& nd, const Problem* P, cudaStream_t s);
+// Pack the cut lists of H (counts from P) and upload them with their pair
+// CSR; resize the bundle's m-vectors.
+void upload_cuts(Engine& E, const HostState& H, const Problem* P);
 
 // updateTriangleInequalities (src/cutting_planes.c:132-214) with the
-// separation run on the device-resident X.
-double tri_update_dev(NodeDev& nd, Problem* P, const double* y, int* added, int* subtracted, cudaStream_t s);
+// separation run on the engine's device-resident X.
+double tri_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* added, int* subtracted);
+
+// update{Pentagonal,Heptagonal}Inequalities (src/cutting_planes.c:316-406,
+// 509-602) on host state H with random stream rng; H.X holds X.
+double pent_update(HostState& H, Problem* P, const double* y, int* added, int* subtracted, int triag, Rng& rng);
+double hept_update(HostState& H, Problem* P, const double* y, int* added, int* subtracted, int hept_index,
+                   Rng& rng);
 
 }  // namespace bqb

@@ -3,6 +3,7 @@
 // program does not define them itself).
 #include <stdarg.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <mutex>
 
@@ -41,15 +42,19 @@ __attribute__((visibility("default"))) int BabPbSize = 0;
 
 namespace bqb {
 
-unsigned long long g_launches = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 static char g_last_error[512] = "";
+static std::mutex g_error_mu;
 static void (*g_abort_hook)(int) = nullptr;
 
 void set_error(const char* where, const char* msg)
 {
+    std::lock_guard<std::mutex> lock(g_error_mu);
     snprintf(g_last_error, sizeof g_last_error, "%s: %s", where, msg);
 }
+
+thread_local bool t_pool_worker = false;
 
 void fatal(const char* where, const char* msg)
 {
@@ -60,7 +65,35 @@ void fatal(const char* where, const char* msg)
         g_abort_hook(10);
         return;
     }
+    if (t_pool_worker) {
+        // exit() from a worker would run the process's destructors under the
+        // feet of the other bounding threads: flush and leave at once
+        fflush(nullptr);
+        _exit(10);
+    }
     exit(10);
+}
+
+cudaError_t raise_smem_limit(const void* fn, size_t bytes)
+{
+    constexpr int kMaxFns = 64;
+    static std::mutex mu;
+    static const void* fns[kMaxFns];
+    static size_t limit[kMaxFns];
+    static int used = 0;
+    std::lock_guard<std::mutex> lock(mu);
+    int i = 0;
+    while (i < used && fns[i] != fn) ++i;
+    if (i == used) {
+        if (used == kMaxFns) return cudaErrorInvalidValue;
+        fns[used] = fn;
+        limit[used] = 0;
+        ++used;
+    }
+    if (bytes <= limit[i]) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) limit[i] = bytes;
+    return e;
 }
 
 static Runtime g_rt;
@@ -84,6 +117,16 @@ static void init_device(int dev)
                  prop.major, prop.minor);
         fatal("bqb_init", buf);
         return;
+    }
+    // How host threads wait for the device: BQB_SYNC = spin | yield | block
+    // (unset: the CUDA runtime's automatic choice).  With many bounding
+    // threads on few cores, yield or block leaves the cores to host work.
+    if (const char* sync = getenv("BQB_SYNC")) {
+        unsigned flags = cudaDeviceScheduleAuto;
+        if (!strcmp(sync, "spin")) flags = cudaDeviceScheduleSpin;
+        if (!strcmp(sync, "yield")) flags = cudaDeviceScheduleYield;
+        if (!strcmp(sync, "block")) flags = cudaDeviceScheduleBlockingSync;
+        BQB_CUDA(cudaSetDeviceFlags(flags));
     }
     g_rt.device = dev;
     g_rt.num_sms = prop.multiProcessorCount;
@@ -127,7 +170,7 @@ __attribute__((visibility("default"))) void bqb_set_abort_hook(void (*hook)(int)
 
 __attribute__((visibility("default"))) unsigned long long bqb_kernel_launches(void)
 {
-    return bqb::g_launches;
+    return bqb::g_launches.load();
 }
 
 __attribute__((visibility("default"))) void bqb_synchronize(void)

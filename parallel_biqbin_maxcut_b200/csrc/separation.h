@@ -2,6 +2,7 @@
 // resident bounding driver.
 #pragma once
 #include "globals.h"
+#include "rng.h"
 #include "trisep.cuh"
 
 namespace bqb {
@@ -21,11 +22,11 @@ int hept_purge(Heptagonal_Inequality* cuts, int n_ineq, const double* y);
 int hept_append(Heptagonal_Inequality* cuts, int kept, const Heptagonal_Inequality* list, int size);
 
 // Host simulated-annealing separation of pentagonal / heptagonal cuts
-// (src/cutting_planes.c:224-309, 416-503), consuming rand() in the
-// reference's order.  X: host, N x N column-major.  Returns the minimum
+// (src/cutting_planes.c:224-309, 416-503), drawing from rng in the
+// reference's order (the default engine's rng is rand() itself).  X: host, N x N column-major.  Returns the minimum
 // value found.
-double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size);
-double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size);
+double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng);
+double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size, Rng& rng);
 
 TriSepState& trisep_state();
 

@@ -282,8 +282,7 @@ double trisep_device(TriSepState& st, const double* dX, int n, int tri_ineq, dou
     tri_scan_kernel<true><<<blocks, 256, 0, s>>>(dX, XT, n, P, violated, cnt, cand, misc);
     BQB_COUNT_LAUNCH();
     const size_t heap_bytes = (size_t)(tri_ineq > 0 ? tri_ineq : 1) * (sizeof(double) + sizeof(int));
-    BQB_CUDA(cudaFuncSetAttribute((const void*)tri_replay_kernel,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heap_bytes));
+    BQB_SMEM_LIMIT(tri_replay_kernel, heap_bytes);
     tri_replay_kernel<<<1, 32, heap_bytes, s>>>(cand, misc, tri_ineq, list, dsize);
     BQB_COUNT_LAUNCH();
     check_launch("trisep");

@@ -64,6 +64,41 @@ def summarize_raw(path: str) -> str:
     return "\n".join(out)
 
 
+def run_ipm(n_vertices: int, repeats: int) -> None:
+    """Bound the root of a seeded G(n, 0.5) +-1 instance `repeats` times
+    through ipm_mc_pk (a small, self-contained case for kernel profiling)."""
+    import ctypes as C
+    import time
+
+    import numpy as np
+
+    from . import _lib, instances
+
+    lib = _lib.load()
+    assert lib.bqb_init(0) == 0, lib.bqb_last_error()
+    A = instances.gnp_pm1(n_vertices, 0.5, seed=1)
+    nv = A.shape[0]
+    lap = np.diag(A.sum(axis=1)) - A
+    L = np.zeros((nv, nv))
+    L[:nv - 1, :nv - 1] = lap[:nv - 1, :nv - 1]
+    rs = L[:nv - 1, :nv - 1].sum(axis=1)
+    L[:nv - 1, nv - 1] = rs
+    L[nv - 1, :nv - 1] = rs
+    L[nv - 1, nv - 1] = rs.sum()
+    L *= 0.25
+    Lc = _lib.colmajor(L)
+    X = np.zeros(nv * nv)
+    phi = C.c_double()
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        lib.ipm_mc_pk(_lib.dptr(Lc), nv, _lib.dptr(X), C.byref(phi), 0)
+        print(f"n={nv} phi={phi.value:.6f} wall={1e3 * (time.perf_counter() - t0):.3f} ms")
+
+
 if __name__ == "__main__":
-    mode, path = sys.argv[1], sys.argv[2]
-    print(summarize_launches(path) if mode == "launches" else summarize_raw(path))
+    mode = sys.argv[1]
+    if mode == "ipm":
+        run_ipm(int(sys.argv[2]), int(sys.argv[3]))
+    else:
+        path = sys.argv[2]
+        print(summarize_launches(path) if mode == "launches" else summarize_raw(path))
