@@ -233,6 +233,20 @@ int bqb_solve_parallel(const double *adj, int num_vertices, const BiqBinParamete
 int bqb_bound_nodes(BabNode *nodes, int count, int rank, int threads, const double *const *L_dev,
                     double *bounds);
 
+/* Pentagonal (k = 5) / heptagonal (k = 7) separation chains on the GPU:
+ * `chains` independent runs of the annealing of qap_simulated_annealing
+ * (src/qap_simulated_annealing.c:12-160), chain c for type (c % types) + 1
+ * of src/cutting_planes.c:239-244 / 431-438, each drawing from its own
+ * SplitMix64 stream started at seed + (c + 1) * 0xD1B54A32D192ED03 instead
+ * of rand().  X: host, n x n column-major.  cost[c] and perm[7c .. 7c+k-1]
+ * receive each chain's best value and permutation.  Returns 0, 1 if a chain
+ * was stopped at the 80-round limit, 2 on bad arguments.  This is the
+ * separation extra engines run (bqb_bound_nodes, bqb_solve_parallel); no
+ * reference counterpart (the reference runs the chains one after another
+ * on rand()).  Not re-entrant. */
+int bqb_kgon_sa(const double *X, int n, int k, int types, int chains, unsigned long long seed, double *cost,
+                int *perm);
+
 /* Bind the library to a CUDA device (default 0) and create its stream.
  * Called implicitly by every entry point; returns 0 on success. */
 int bqb_init(int device);

@@ -111,6 +111,7 @@ SIGNATURES = {
     "bqb_solve_parallel": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "bqb_bound_nodes": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_void_p), D]),
+    "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),
     "bqb_kernel_launches": (C.c_ulonglong, []),

@@ -222,7 +222,71 @@ double hept_update(HostState& H, Problem* P, const double* y, int* NumAdded, int
     return mn;
 }
 
+namespace {
+
+template <int K>
+double kgon_separate_dev(Engine& E, int n, int types, int trials, int* chains_out)
+{
+    const int chains = trials > 0 ? trials * types : 0;
+    *chains_out = chains;
+    if (chains == 0 || n < K) return BIG_NUMBER;
+    const uint64_t seed = E.sa_seed + E.sa_calls++;
+    kgon_sa_device(E.sa, E.nd.X.p, n, K, types, chains, seed, E.stream);
+    return 0.0;
+}
+
+}  // namespace
+
+double pent_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* NumAdded, int* NumSubtracted,
+                       int triag)
+{
+    const int kept = pent_purge(H.pcuts, P->NPentIneq, y + triag);
+    const int subtracted = P->NPentIneq - kept;
+    P->NPentIneq = kept;
+    int size = 0, chains = 0;
+    double mn = kgon_separate_dev<5>(E, P->n, 3, params.Pent_Trials, &chains);
+    if (chains > 0 && P->n >= 5) mn = pent_collect(E.sa.hcost.p, E.sa.hperm.p, chains, H.plist, &size);
+    const int added = pent_append(H.pcuts, kept, H.plist, size);
+    P->NPentIneq += added;
+    *NumAdded = added;
+    *NumSubtracted = subtracted;
+    return mn;
+}
+
+double hept_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* NumAdded, int* NumSubtracted,
+                       int hept_index)
+{
+    const int kept = hept_purge(H.hcuts, P->NHeptaIneq, y + hept_index);
+    const int subtracted = P->NHeptaIneq - kept;
+    P->NHeptaIneq = kept;
+    int size = 0, chains = 0;
+    double mn = kgon_separate_dev<7>(E, P->n, 4, params.Hepta_Trials, &chains);
+    if (chains > 0 && P->n >= 7) mn = hept_collect(E.sa.hcost.p, E.sa.hperm.p, chains, H.hlist, &size);
+    const int added = hept_append(H.hcuts, kept, H.hlist, size);
+    P->NHeptaIneq += added;
+    *NumAdded = added;
+    *NumSubtracted = subtracted;
+    return mn;
+}
+
 }  // namespace bqb
+
+// GPU annealing chains on a host matrix (test and inspection entry point).
+BQB_API int bqb_kgon_sa(const double* Xm, int n, int k, int types, int chains, unsigned long long seed,
+                        double* cost, int* perm)
+{
+    if (n < k || (k != 5 && k != 7) || types < 1 || chains < 0) return 2;
+    if (chains == 0) return 0;
+    Runtime& R = rt();
+    static KgonSaState st;
+    static DevBuf<double> dX;
+    double* d = dX.ensure((size_t)n * n);
+    BQB_CUDA(cudaMemcpyAsync(d, Xm, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, R.stream));
+    kgon_sa_device(st, d, n, k, types, chains, seed, R.stream);
+    memcpy(cost, st.hcost.p, (size_t)chains * sizeof(double));
+    memcpy(perm, st.hperm.p, (size_t)chains * 7 * sizeof(int));
+    return st.hstat.p[0] ? 1 : 0;
+}
 
 BQB_API double updatePentagonalInequalities(Problem* P, double* y, int* NumAdded, int* NumSubtracted, int triag)
 {

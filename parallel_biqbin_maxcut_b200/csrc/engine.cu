@@ -46,6 +46,7 @@ Engine* engine_create(unsigned seed)
     Engine* e = new Engine();
     BQB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     e->rng.seed(seed);
+    e->sa_seed = (uint64_t)seed << 32;
     return e;
 }
 
@@ -112,6 +113,12 @@ void engine_destroy(Engine* e)
     free_host(h.hbest);
     free_host(h.hval);
     free_host(h.hstat);
+    free_dev(e->sa.cost);
+    free_dev(e->sa.perm);
+    free_dev(e->sa.status);
+    free_host(e->sa.hcost);
+    free_host(e->sa.hperm);
+    free_host(e->sa.hstat);
     TriSepState& t = e->tri;
     free_dev(t.XT);
     free_dev(t.cnt);

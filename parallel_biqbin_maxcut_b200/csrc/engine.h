@@ -14,6 +14,7 @@
 #include "cuts.cuh"
 #include "globals.h"
 #include "heur.cuh"
+#include "kgon_sa.cuh"
 #include "rng.h"
 #include "trisep.cuh"
 
@@ -56,6 +57,9 @@ struct Engine {
     NodeDev nd;
     HeurState heur;
     TriSepState tri;
+    KgonSaState sa;          // GPU k-gonal separation (extra engines)
+    uint64_t sa_seed = 0;    // its chains' seed base ...
+    uint64_t sa_calls = 0;   // ... and the separation calls made so far
     DevBuf<double> ipm_ws;
     // private host state (extra engines only)
     std::vector<Triangle_Inequality> cuts_v;

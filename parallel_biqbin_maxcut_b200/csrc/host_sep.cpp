@@ -20,6 +20,8 @@ namespace bqb {
 // declared for the other translation units in separation.h
 double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng);
 double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size, Rng& rng);
+double pent_collect(const double* cost, const int* perm, int chains, Pentagonal_Inequality* list, int* size);
+double hept_collect(const double* cost, const int* perm, int chains, Heptagonal_Inequality* list, int* size);
 
 namespace {
 constexpr double BIG_NUMBER = 1e9;   // src/biqbin.h:35
@@ -136,44 +138,78 @@ namespace bqb {
 // (heptagonal), restated with its exact update rule, including the
 // re-scan that starts from BIG_NUMBER and looks for a larger value.
 template <int K, class Ineq>
-static double kgon_separate(const double* Xh, int N, Ineq* list, int* list_size, int trials, int types,
-                            int cap, Rng& rng)
-{
+struct KgonList {
+    Ineq* list;
+    int cap;
     int size = 0, least = 0;
     double least_val = -BIG_NUMBER;
     double min_all = BIG_NUMBER;
+    KgonList(Ineq* l, int c) : list(l), cap(c) {}
+    void offer(int type, double v, const int* perm)
+    {
+        min_all = v < min_all ? v : min_all;
+        if (!(v < 1.0)) return;
+        if (size < cap) {
+            list[size].type = type;
+            list[size].value = v;
+            for (int a = 0; a < K; ++a) list[size].permutation[a] = perm[a];
+            if (size == 0 || v > least_val) {
+                least_val = v;
+                least = size;
+            }
+            ++size;
+        } else if (v < least_val) {
+            list[least].type = type;
+            list[least].value = v;
+            for (int a = 0; a < K; ++a) list[least].permutation[a] = perm[a];
+            least_val = BIG_NUMBER;
+            for (int q = 0; q < size; ++q)
+                if (list[q].value > least_val) {
+                    least_val = list[q].value;
+                    least = q;
+                }
+        }
+    }
+};
+
+template <int K, class Ineq>
+static double kgon_separate(const double* Xh, int N, Ineq* list, int* list_size, int trials, int types,
+                            int cap, Rng& rng)
+{
+    KgonList<K, Ineq> L(list, cap);
     int H[49];
     int perm[7];
     for (int trial = 0; trial < trials; ++trial) {
         for (int type = 1; type <= types; ++type) {
             kgon_H(K, type, H);
             const double v = qap_sa(H, K, Xh, N, perm, rng);
-            min_all = v < min_all ? v : min_all;
-            if (!(v < 1.0)) continue;
-            if (size < cap) {
-                list[size].type = type;
-                list[size].value = v;
-                for (int a = 0; a < K; ++a) list[size].permutation[a] = perm[a];
-                if (size == 0 || v > least_val) {
-                    least_val = v;
-                    least = size;
-                }
-                ++size;
-            } else if (v < least_val) {
-                list[least].type = type;
-                list[least].value = v;
-                for (int a = 0; a < K; ++a) list[least].permutation[a] = perm[a];
-                least_val = BIG_NUMBER;
-                for (int q = 0; q < size; ++q)
-                    if (list[q].value > least_val) {
-                        least_val = list[q].value;
-                        least = q;
-                    }
-            }
+            L.offer(type, v, perm);
         }
     }
-    *list_size = size;
-    return min_all;
+    *list_size = L.size;
+    return L.min_all;
+}
+
+// Chain results of the GPU annealing (chain c = (trial, type) pair
+// c / types, c % types + 1) offered to the list in the reference's loop order.
+template <int K, class Ineq>
+static double kgon_collect(const double* cost, const int* perm, int chains, int types, Ineq* list,
+                           int* list_size, int cap)
+{
+    KgonList<K, Ineq> L(list, cap);
+    for (int c = 0; c < chains; ++c) L.offer(c % types + 1, cost[c], perm + (size_t)7 * c);
+    *list_size = L.size;
+    return L.min_all;
+}
+
+double pent_collect(const double* cost, const int* perm, int chains, Pentagonal_Inequality* list, int* size)
+{
+    return kgon_collect<5>(cost, perm, chains, 3, list, size, params.PentIneq);
+}
+
+double hept_collect(const double* cost, const int* perm, int chains, Heptagonal_Inequality* list, int* size)
+{
+    return kgon_collect<7>(cost, perm, chains, 4, list, size, params.HeptaIneq);
 }
 
 double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng)

@@ -220,14 +220,22 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             BQB_CUDA(cudaStreamSynchronize(s));
             viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
             const bool do_pent = params.include_Pent && (count > params.triag_iter || viol3 < 0.2);
-            if (do_pent || params.include_Hepta) {
+            // the default engine anneals on the host from the rand() stream
+            // (the reference's cuts); extra engines run the chains on the GPU
+            if ((do_pent || params.include_Hepta) && E.is_default) {
                 BQB_CUDA(cudaMemcpyAsync(H.X, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
                 BQB_CUDA(cudaStreamSynchronize(s));
             }
-            if (do_pent) viol5 = pent_update(H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag, E.rng);
+            if (do_pent)
+                viol5 = E.is_default ? pent_update(H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag, E.rng)
+                                     : pent_update_dev(E, H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag);
             if (params.include_Hepta &&
-                ((count > params.triag_iter + params.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4))))
-                hept_update(H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta, E.rng);
+                ((count > params.triag_iter + params.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4)))) {
+                if (E.is_default)
+                    hept_update(H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta, E.rng);
+                else
+                    hept_update_dev(E, H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta);
+            }
         } else {
             tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
         }

@@ -19,6 +19,12 @@ double tri_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int*
 // update{Pentagonal,Heptagonal}Inequalities (src/cutting_planes.c:316-406,
 // 509-602) on host state H with random stream rng; H.X holds X.
 double pent_update(HostState& H, Problem* P, const double* y, int* added, int* subtracted, int triag, Rng& rng);
+// The same updates with the separation run by the GPU annealing chains on
+// the engine's device X (extra engines).
+double pent_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* added, int* subtracted,
+                       int triag);
+double hept_update_dev(Engine& E, HostState& H, Problem* P, const double* y, int* added, int* subtracted,
+                       int hept_index);
 double hept_update(HostState& H, Problem* P, const double* y, int* added, int* subtracted, int hept_index,
                    Rng& rng);
 

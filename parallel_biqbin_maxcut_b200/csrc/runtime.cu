@@ -137,6 +137,12 @@ static void init_device(int dev)
 Runtime& rt()
 {
     std::call_once(g_once, [] {
+        // Concurrent engines each launch on their own stream; the runtime
+        // maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware queues
+        // (8 unless set), and streams sharing a queue serialise.  Ask for
+        // the maximum unless the host program chose (only effective before
+        // the device's context exists).
+        setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
         const char* env = getenv("BQB_DEVICE");
         init_device(env ? atoi(env) : 0);
     });

@@ -28,6 +28,11 @@ int hept_append(Heptagonal_Inequality* cuts, int kept, const Heptagonal_Inequali
 double pent_separate(const double* Xh, int N, Pentagonal_Inequality* list, int* size, Rng& rng);
 double hept_separate(const double* Xh, int N, Heptagonal_Inequality* list, int* size, Rng& rng);
 
+// The same lists from the GPU annealing chains (kgon_sa.cuh): chain c's
+// value cost[c] and permutation perm[7c ..] offered in chain order.
+double pent_collect(const double* cost, const int* perm, int chains, Pentagonal_Inequality* list, int* size);
+double hept_collect(const double* cost, const int* perm, int chains, Heptagonal_Inequality* list, int* size);
+
 TriSepState& trisep_state();
 
 }  // namespace bqb
