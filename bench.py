@@ -513,7 +513,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--nodes-per-step", type=int, default=512)
-    ap.add_argument("--threads", type=int, default=64, help="concurrent bounding engines per GPU")
+    ap.add_argument("--threads", type=int, default=32, help="concurrent bounding engines per GPU")
     ap.add_argument("--dropin-nodes", type=int, default=16,
                     help="nodes timed through the serial drop-in Evaluate (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
