@@ -10,15 +10,15 @@ parameters.  First the root is bounded with rank 0 (this sets the incumbent
 and `diff` as the reference's master does); then every subproblem is bounded
 as a worker bounds a node (rank 1): IPM, heuristic, prune / give-up tests,
 cutting planes and bundle iterations to the reference's stopping rules.
-A step bounds one batch of subproblems with --threads concurrent bounding
-engines (bqb_bound_nodes: one host thread, CUDA stream and set of buffers
-per engine, nodes handed out dynamically); the metric is nodes/s.
+A step bounds one batch of subproblems with the fused node kernel
+(bqb_bound_nodes_fused: one persistent kernel, one CTA per SM, each CTA
+bounding whole nodes on the device); the metric is nodes/s.
 
-  value : bqb_bound_nodes on device-resident subproblem matrices (inputs in
-          HBM)
-  e2e   : bqb_bound_nodes with host nodes: subproblem construction on the
-          host (createSubproblem) and every host<->device copy inside the
-          timed region
+  value : device time of the fused kernel (CUDA events around its launch),
+          plus any node it hands back to the engines
+  e2e   : the same C-ABI call from host node structs, every host<->device
+          copy inside the timed region
+  engines : bqb_bound_nodes with --threads concurrent engines (one step)
   dropin_serial : the reference-facing Evaluate(node, SP, PP, 1), one node
           at a time on the library stream, as the reference's worker calls it
 
@@ -177,18 +177,6 @@ class GpuArm:
         self.root_bound = lib.Evaluate(C.byref(root), self.SP, self.PP, 0)
         self.lb = lib.Bab_LBGet()
         self.nodes = [make_node(xf, sol) for xf, sol in self.subs]
-        # device-resident subproblem matrices (PP->L of every node)
-        self.n = []
-        self.dL = []
-        tmp = np.zeros(self.N0 * self.N0)
-        for nd in self.nodes:
-            self.PP.contents.L = tmp.ctypes.data_as(C.POINTER(C.c_double))
-            lib.createSubproblem(C.byref(nd), self.SP, self.PP)
-            n = self.PP.contents.n
-            t = torch.from_numpy(tmp[: n * n].copy()).to(f"cuda:{device}")
-            self.n.append(n)
-            self.dL.append(t)
-        self.restore_host_L()
         self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
         torch.cuda.synchronize()
 
@@ -198,18 +186,8 @@ class GpuArm:
             C.memmove(C.byref(arr[q]), C.byref(self.nodes[i]), C.sizeof(_lib.BabNode))
         return arr
 
-    def device_ptrs(self, idx):
-        return (C.c_void_p * len(idx))(*[self.dL[i].data_ptr() for i in idx])
-
-    def bound_device(self, arr, ptrs, threads):
-        """value leg: concurrent engines on device-resident PP->L."""
-        out = np.zeros(len(arr))
-        rc = self.lib.bqb_bound_nodes(arr, len(arr), 1, threads, ptrs, _lib.dptr(out))
-        assert rc == 0, self.lib.bqb_last_error()
-        return out
-
     def bound_e2e(self, idx, threads):
-        """e2e leg: the same C-ABI call with host nodes; every subproblem is
+        """engines leg: bqb_bound_nodes with host nodes; every subproblem is
         built on the host (createSubproblem) and copied in, and the bounds
         and fractional solutions come back to the host."""
         arr = self.node_array(idx)
@@ -250,14 +228,14 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
     arm = GpuArm(local)
+    lib = arm.lib
     B = args.nodes_per_step
     T = args.threads
     # rank r bounds its own share of the subproblems (weak scaling: per-GPU
     # work fixed); each step is a batch of B subproblems
     order = [(i * 7919 + rank * 131) % N_SUB for i in range(B * (args.warmup + args.steps))]
     batches = [order[s * B:(s + 1) * B] for s in range(args.warmup + args.steps)]
-    arrays = [arm.node_array(b) for b in batches]
-    ptrs = [arm.device_ptrs(b) for b in batches]
+    timed = range(args.warmup, args.warmup + args.steps)
 
     def barrier():
         torch.cuda.synchronize()
@@ -272,52 +250,60 @@ def run_gpu(args):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also sizes every engine's device buffers)
-    for s in range(args.warmup):
-        arm.bound_device(arm.node_array(batches[s]), ptrs[s], T)
-    stream = torch.cuda.current_stream()
+    def fused(arr):
+        lib.bqb_reset_incumbent(arm.lb)   # every batch starts from the root's incumbent
+        out = np.zeros(len(arr))
+        rc = lib.bqb_bound_nodes_fused(arr, len(arr), 1, _lib.dptr(out))
+        assert rc == 0, lib.bqb_last_error()
+        return out
 
-    # ---- value: device-resident inputs ----
-    # bqb_bound_nodes returns when every engine stream is idle; the events on
-    # the (idle) current stream bracket the whole call on the device clock
-    arm.lib.bqb_stats_reset()
-    arm.lib.bqb_stats_enable(1)
+    stream = torch.cuda.current_stream()
+    # warm-up (sizes the kernel's arena and every buffer)
+    for s in range(args.warmup):
+        fused(arm.node_array(batches[s]))
+
+    # ---- value: the fused kernel (+ any node it hands back to an engine),
+    # device time from CUDA events around the launch on its stream ----
+    arrays = [arm.node_array(b) for b in batches]
+    lib.bqb_stats_reset()
+    lib.bqb_fused_stats_reset()
     clocks = ClockSampler(local)
-    launches0 = arm.lib.bqb_kernel_launches()
+    launches0 = lib.bqb_kernel_launches()
     barrier()
     clocks.start()
-    ms = 0.0
     bounds_dev = []
-    for s in range(args.warmup, args.warmup + args.steps):
+    for s in timed:
         arm.l2_flush()
         torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        bounds_dev.append(arm.bound_device(arrays[s], ptrs[s], T))
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        ms += ev0.elapsed_time(ev1)
+        bounds_dev.append(fused(arrays[s]))
     barrier()
     clk = clocks.stop()
-    launches = arm.lib.bqb_kernel_launches() - launches0
+    launches = lib.bqb_kernel_launches() - launches0
     stats = (C.c_double * 6)()
-    arm.lib.bqb_ipm_stats(stats)
-    arm.lib.bqb_stats_enable(0)
+    lib.bqb_ipm_stats(stats)
+    fst = (C.c_double * 5)()
+    lib.bqb_fused_stats(fst)
+    prof = (C.c_double * 11)()
+    lib.bqb_fused_profile(prof)
+    phase_names = ["subproblem", "ipm", "heuristic", "tri_scan", "tri_list", "kgon", "cut_upload", "opBt",
+                   "opB", "lambda_eta", "bundle_step"]
+    tot_cta_s = max(sum(prof), 1e-30)
+    ms = fst[2] + fst[4]
     ms_max = max_over_ranks(ms)
     total_nodes = B * args.steps * ws
     value = total_nodes / (ms_max / 1e3)
 
-    # ---- e2e: host nodes through the same C-ABI call ----
+    # ---- e2e: the same C-ABI call from host node structs, every copy in
+    # the timed region (events on the idle current stream around the call) ----
     barrier()
     ms_e2e = 0.0
-    for s in range(args.warmup, args.warmup + args.steps):
+    for s in timed:
         arm.l2_flush()
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        arm.bound_e2e(batches[s], T)
+        fused(arm.node_array(batches[s]))
         t1.record(stream)
         torch.cuda.synchronize()
         ms_e2e += t0.elapsed_time(t1)
@@ -325,8 +311,26 @@ def run_gpu(args):
     ms_e2e = max_over_ranks(ms_e2e)
     e2e = total_nodes / (ms_e2e / 1e3)
     b0 = batches[args.warmup]
-    h2d = sum(arm.n[i] ** 2 * 8 + 3 * 4 * (NV - 1) for i in b0)
-    d2h = B * 8 + B * (NV - 1) * 8
+    N = NV - 1
+    h2d = B * 2 * N * 4 + 8
+    d2h = B * (8 + N * 8 + 8 + N * 4 + 4)
+
+    # ---- concurrent engines (bqb_bound_nodes, host nodes) ----
+    eng = None
+    if T > 0 and args.engine_nodes > 0:
+        ne = min(args.engine_nodes, B)
+        lib.bqb_reset_incumbent(arm.lb)
+        arm.bound_e2e(batches[0][:ne], T)   # warm the engine pool
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        lib.bqb_reset_incumbent(arm.lb)
+        e0.record(stream)
+        arm.bound_e2e(b0[:ne], T)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        eng = {"value": ne / (e0.elapsed_time(e1) / 1e3), "unit": "nodes/s", "engines": T, "nodes": ne,
+               "call": "bqb_bound_nodes, host nodes, one step (after one warm-up step)"}
 
     # ---- the plain drop-in (one node at a time, library stream) ----
     drop = None
@@ -335,6 +339,7 @@ def run_gpu(args):
         barrier()
         d0 = torch.cuda.Event(enable_timing=True)
         d1 = torch.cuda.Event(enable_timing=True)
+        lib.bqb_reset_incumbent(arm.lb)
         d0.record(stream)
         arm.dropin_serial(idx)
         d1.record(stream)
@@ -343,23 +348,21 @@ def run_gpu(args):
                 "nodes": len(idx), "call": "Evaluate(node, SP, PP, 1), host buffers, serial"}
 
     pk = peaks()
-    kernel_ms = stats[4]
+    kernel_ms = fst[2]
     flops = FLOP_PER_ITER_N3 * stats[0]
-    nl = max(stats[5], 1)
     achieved = flops / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else 0.0
-    aggregate = flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
     peak = pk["bf16_tflops_sustained"]
-    roof = {"kernel": "ipm_reg_one_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
+    roof = {"kernel": "nodek_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
             "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
                            f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
-            "launches": int(stats[5]), "avg_launch_us": 1e3 * kernel_ms / nl,
+            "launches": int(fst[0]), "avg_launch_us": 1e3 * kernel_ms / max(fst[0], 1),
+            "flops_counted": "IPM only: sum over IPM solves of iterations * 6 n^3",
             "ipm_iterations": int(stats[2]), "ipm_problems": int(stats[1]),
             "linesearch_factorizations": int(stats[3]),
-            "flop_per_iteration": f"{FLOP_PER_ITER_N3} n^3",
-            "aggregate_ipm_tflops": aggregate,
-            "aggregate_note": "all IPM flops of the value leg / its device time (engines run concurrently)",
-            "kernel_busy_share": kernel_ms / ms if ms > 0 else None}
+            "fallback_nodes": int(fst[3]), "fallback_ms": fst[4],
+            "phase_share": {nm: round(prof[i] / tot_cta_s, 4) for i, nm in enumerate(phase_names)},
+            "phase_cta_seconds": {nm: round(prof[i], 3) for i, nm in enumerate(phase_names)}}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -371,16 +374,15 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "nodes_per_step": B, "nodes_per_step_total": B * ws,
-                       "engines": T, "l2": "flushed (256 MB write) before every step",
-                       "precision": "FP64 throughout",
-                       "mode": f"{T} concurrent bounding engines (bqb_bound_nodes)",
+                       "l2": "flushed (256 MB write) before every step", "precision": "FP64 throughout",
+                       "mode": "fused node kernel (bqb_bound_nodes_fused): one CTA bounds a whole node",
                        "root_bound": arm.root_bound, "incumbent": arm.lb,
                        "mean_bound": float(np.mean(np.concatenate(bounds_dev))),
-                       "parallelism": f"replicas over nodes x{ws}",
-                       "sync": os.environ.get("BQB_SYNC", "auto")},
+                       "parallelism": f"replicas over nodes x{ws}"},
             "e2e": {"value": e2e, "unit": "nodes/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps,
-                    "call": "bqb_bound_nodes with host nodes (subproblems built on the host)"},
+                    "call": "bqb_bound_nodes_fused with host node structs"},
+            "engines": eng,
             "dropin_serial": drop,
             "gpu_launches": int(launches),
             "roofline": roof,
@@ -514,6 +516,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--nodes-per-step", type=int, default=512)
     ap.add_argument("--threads", type=int, default=32, help="concurrent bounding engines per GPU")
+    ap.add_argument("--engine-nodes", type=int, default=128,
+                    help="nodes timed through the concurrent engines (0: skip)")
     ap.add_argument("--dropin-nodes", type=int, default=16,
                     help="nodes timed through the serial drop-in Evaluate (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

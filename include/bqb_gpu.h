@@ -233,6 +233,36 @@ int bqb_solve_parallel(const double *adj, int num_vertices, const BiqBinParamete
 int bqb_bound_nodes(BabNode *nodes, int count, int rank, int threads, const double *const *L_dev,
                     double *bounds);
 
+/* The same bounds as bqb_bound_nodes, computed by one persistent kernel in
+ * which every CTA (one per SM) bounds whole nodes on the device: the
+ * subproblem, the basic IPM, the heuristic, the separations and cut-list
+ * updates and the bundle iterations of SDPbound (src/bounding.c:24-342)
+ * with no host round trip.  The incumbent enters as Bab_LBGet(); heuristic
+ * improvements are passed to Bab_LBUpd after the kernel, in node order.
+ * nodes[i].fracsol and bounds[i] are filled as SDPbound fills them.  The
+ * heuristic and the annealing chains draw from counter-based streams of
+ * their own.  Nodes beyond the kernel's capacities (N0 > 128, bundle
+ * larger than 64, more cuts than the slot holds) or meeting a numerical
+ * failure are bounded again by bqb_bound_nodes.  Returns 0, or 1 when SP
+ * is not set up.  No reference counterpart. */
+int bqb_bound_nodes_fused(BabNode *nodes, int count, int rank, double *bounds);
+/* Nodes bqb_bound_nodes_fused handed back to engines so far. */
+long long bqb_fused_fallbacks(void);
+/* Set the incumbent value Bab_LBGet returns (lower or higher; BabSol is
+ * left unchanged), so that a benchmark or a test can bound every batch from
+ * the same incumbent.  No reference counterpart. */
+void bqb_reset_incumbent(double value);
+/* Timing of bqb_bound_nodes_fused since the last reset: out[5] = {calls,
+ * nodes, fused-kernel milliseconds (CUDA events), nodes bounded again by
+ * engines, milliseconds of that}. */
+void bqb_fused_stats(double *out);
+void bqb_fused_stats_reset(void);
+/* Seconds spent per phase inside the fused kernel since the last reset,
+ * summed over its CTAs: out[11] = {subproblem, IPM, heuristic, triangle
+ * scan, triangle list update, k-gonal separation, cut upload, B^T, B,
+ * lambda_eta, bundle step}. */
+void bqb_fused_profile(double *out);
+
 /* Pentagonal (k = 5) / heptagonal (k = 7) separation chains on the GPU:
  * `chains` independent runs of the annealing of qap_simulated_annealing
  * (src/qap_simulated_annealing.c:12-160), chain c for type (c % types) + 1

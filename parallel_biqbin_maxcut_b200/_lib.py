@@ -111,6 +111,12 @@ SIGNATURES = {
     "bqb_solve_parallel": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "bqb_bound_nodes": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_void_p), D]),
+    "bqb_bound_nodes_fused": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, D]),
+    "bqb_fused_fallbacks": (C.c_longlong, []),
+    "bqb_fused_stats": (None, [D]),
+    "bqb_fused_stats_reset": (None, []),
+    "bqb_fused_profile": (None, [D]),
+    "bqb_reset_incumbent": (None, [C.c_double]),
     "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),

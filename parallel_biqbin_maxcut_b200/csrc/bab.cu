@@ -138,6 +138,14 @@ BQB_API int Bab_LBUpd(double new_lb, BabSolution* bs)
 
 BQB_API int Bab_numEvalNodes(void) { return g_num_nodes; }
 
+// Set the incumbent value (the solution is left as it is), lower or higher:
+// lets a benchmark or a test start every batch from the same incumbent.
+BQB_API void bqb_reset_incumbent(double value)
+{
+    std::lock_guard<std::mutex> lock(g_lb_mu);
+    g_LB.store(value);
+}
+
 // ---- src/bab_functions.c:96-134 --------------------------------------------
 BQB_API double evaluateSolution(int* sol)
 {

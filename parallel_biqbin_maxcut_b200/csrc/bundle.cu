@@ -15,499 +15,47 @@
 // bundle_xcomb_kernel: X = X_bundle * lambda after a serious step.
 #include <math.h>
 
-#include "bundle.cuh"
+#include "bundle_body.cuh"
 
 namespace bqb {
 
 namespace {
 
-constexpr double BIG_NUMBER = 1e9;
-constexpr int LE_THREADS = 256;
-constexpr int QP_SMEM_K = 90;   // k up to this keeps Q and the KKT factor in shared memory
-
-__device__ __forceinline__ double Qat(const double* Q, int k, int a, int b)
-{
-    return a >= b ? Q[a + (size_t)b * k] : Q[b + (size_t)a * k];
-}
-
-// One warp.  Q: k x k (lower triangle read), c: k, lam: k (out).
-// ws: 2k*k... layout A[k*k], then vectors.  Returns false on a non-PD A.
-__device__ bool warp_qp(int k, const double* Q, const double* c, double* lam, double* ws)
-{
-    const int lane = threadIdx.x & 31;
-    double* A = ws;
-    double* Qlam = A + (size_t)k * k;
-    double* z = Qlam + k;
-    double* dlam = z + k;
-    double* u = dlam + k;
-    double* w = u + k;
-
-    for (int b = lane; b < k; b += 32) lam[b] = 1.0 / k;
-    __syncwarp();
-    double part_min = BIG_NUMBER;
-    for (int a = lane; a < k; a += 32) {
-        double acc = 0.0;
-        for (int b = 0; b < k; ++b) acc += Qat(Q, k, a, b) * lam[b];
-        Qlam[a] = acc;
-        const double tv = acc + c[a];
-        z[a] = tv;
-        part_min = fmin(part_min, tv);
-    }
-    double mintmp = part_min;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mintmp = fmin(mintmp, __shfl_xor_sync(0xffffffffu, mintmp, o));
-    double y;
-    __syncwarp();
-    if (mintmp > 1) {
-        y = 0.0;
-    } else {
-        y = mintmp - 1.0;
-        for (int a = lane; a < k; a += 32) z[a] = z[a] - y;
-    }
-    __syncwarp();
-    double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
-    for (int a = lane; a < k; a += 32) {
-        s1 += z[a] * lam[a];
-        s2 += lam[a];
-        s3 += lam[a] * Qlam[a];
-        s4 += lam[a] * c[a];
-    }
-    s1 = warp_sum(s1);
-    s2 = warp_sum(s2);
-    s3 = warp_sum(s3);
-    s4 = warp_sum(s4);
-    double mu = 0.5 * (s1 / k);
-    double res_p = 1.0 - s2;
-    double gap = (s4 + 0.5 * s3) - (y - 0.5 * s3);
-    int cnt = 0;
-    while (fabs(gap) > 1e-5) {
-        ++cnt;
-        // A = Q + Diag(z ./ lambda) (lower), r = c - y + Qlam
-        for (int a = lane; a < k; a += 32) {
-            for (int b = 0; b <= a; ++b) A[a + (size_t)b * k] = Qat(Q, k, a, b);
-            A[a + (size_t)a * k] += z[a] / lam[a];
-            u[a] = 1.0;
-            w[a] = c[a] - y + Qlam[a];
-        }
-        __syncwarp();
-        // Cholesky of A
-        for (int j = 0; j < k; ++j) {
-            const double d = A[j + (size_t)j * k];
-            if (!(d > 0.0)) return false;
-            const double sq = sqrt(d);
-            __syncwarp();
-            for (int i = j + 1 + lane; i < k; i += 32) A[i + (size_t)j * k] /= sq;
-            if (lane == 0) A[j + (size_t)j * k] = sq;
-            __syncwarp();
-            for (int i = j + 1 + lane; i < k; i += 32) {
-                const double lij = A[i + (size_t)j * k];
-                for (int cc = j + 1; cc <= i; ++cc) A[i + (size_t)cc * k] -= lij * A[cc + (size_t)j * k];
-            }
-            __syncwarp();
-        }
-        // forward and backward substitution for u and w together
-        for (int j = 0; j < k; ++j) {
-            const double ljj = A[j + (size_t)j * k];
-            const double uj = u[j] / ljj, wj = w[j] / ljj;
-            __syncwarp();
-            if (lane == 0) {
-                u[j] = uj;
-                w[j] = wj;
-            }
-            for (int i = j + 1 + lane; i < k; i += 32) {
-                const double l = A[i + (size_t)j * k];
-                u[i] -= l * uj;
-                w[i] -= l * wj;
-            }
-            __syncwarp();
-        }
-        for (int j = k - 1; j >= 0; --j) {
-            const double ljj = A[j + (size_t)j * k];
-            const double uj = u[j] / ljj, wj = w[j] / ljj;
-            __syncwarp();
-            if (lane == 0) {
-                u[j] = uj;
-                w[j] = wj;
-            }
-            for (int i = lane; i < j; i += 32) {
-                const double l = A[j + (size_t)i * k];
-                u[i] -= l * uj;
-                w[i] -= l * wj;
-            }
-            __syncwarp();
-        }
-        double su = 0.0, sw = 0.0;
-        for (int a = lane; a < k; a += 32) {
-            su += u[a];
-            sw += w[a];
-        }
-        su = warp_sum(su);
-        sw = warp_sum(sw);
-        const double dy = (res_p + sw) / su;
-        double ap = -BIG_NUMBER, ad = -BIG_NUMBER;
-        for (int a = lane; a < k; a += 32) {
-            const double dl = u[a] * dy - w[a];
-            dlam[a] = dl;
-            const double dz = 1.0 / lam[a] * (mu - lam[a] * z[a] - z[a] * dl);
-            u[a] = dz;   // u now holds dz
-            ap = fmax(ap, -dl / lam[a]);
-            ad = fmax(ad, -dz / z[a]);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ap = fmax(ap, __shfl_xor_sync(0xffffffffu, ap, o));
-            ad = fmax(ad, __shfl_xor_sync(0xffffffffu, ad, o));
-        }
-        ap = (ap > 0) ? ((0.99 / ap < 1.0) ? 0.99 / ap : 1.0) : 1.0;
-        ad = (ad > 0) ? ((0.99 / ad < 1.0) ? 0.99 / ad : 1.0) : 1.0;
-        y += ad * dy;
-        __syncwarp();
-        for (int a = lane; a < k; a += 32) {
-            lam[a] = fma(ap, dlam[a], lam[a]);
-            z[a] = fma(ad, u[a], z[a]);
-        }
-        __syncwarp();
-        double t1 = 0.0, t2 = 0.0, t3 = 0.0, t4 = 0.0;
-        for (int a = lane; a < k; a += 32) {
-            double acc = 0.0;
-            for (int b = 0; b < k; ++b) acc += Qat(Q, k, a, b) * lam[b];
-            Qlam[a] = acc;
-            t1 += lam[a];
-            t2 += lam[a] * z[a];
-            t3 += lam[a] * acc;
-            t4 += lam[a] * c[a];
-        }
-        t1 = warp_sum(t1);
-        t2 = warp_sum(t2);
-        t3 = warp_sum(t3);
-        t4 = warp_sum(t4);
-        __syncwarp();
-        res_p = 1 - t1;
-        mu = (t2 / k) * 0.4;
-        if (ap + ad > 1.8) mu *= 0.2;
-        gap = (t4 + 0.5 * t3) - (y - 0.5 * t3);
-        if (cnt > 30) break;
-    }
-    return true;
-}
-
-__device__ __forceinline__ const double* gcol(const double* G, int ldg, const int* slot, int b)
-{
-    return G + (size_t)(slot ? slot[b] : b) * ldg;
-}
-
-struct LeArgs {
-    const double* G;
-    int ldg;
-    const int* slot;
-    int m;
-    const double* zeta_in;
-    const double* Fv;
-    const double* gam;
-    double* lam;
-    double* eta;
-    double* dgam;
-    double* gtest;
-    double* dstate;
-    int* istate;
-    double* qp_ws_global;
-    int k_fixed;   // >= 0: use this k instead of istate[BI_K]
-};
-
 __global__ void __launch_bounds__(LE_THREADS) lambda_eta_kernel(LeArgs a)
 {
     extern __shared__ __align__(16) double sm[];
-    __shared__ double red[64];
-    __shared__ int flag;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const int k = a.k_fixed >= 0 ? a.k_fixed : a.istate[BI_K];
-    const int m = a.m;
-    double t = a.dstate[BD_T];
-    const bool qp_in_smem = k <= QP_SMEM_K;
-    double* zeta = sm;
-    double* c = zeta + k;
-    double* lam = c + k;
-    double* Q = qp_in_smem ? lam + k : a.qp_ws_global;
-    double* qpws = qp_in_smem ? Q + (size_t)k * k : a.qp_ws_global + (size_t)k * k;
-
-    // zeta
-    for (int b = warp; b < k; b += nw) {
-        if (a.zeta_in) {
-            if (lane == 0) zeta[b] = a.zeta_in[b];
-            continue;
-        }
-        const double* Gb = gcol(a.G, a.ldg, a.slot, b);
-        double acc = 0.0;
-        for (int i = lane; i < m; i += 32) acc = fma(Gb[i], a.gam[i], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) zeta[b] = -a.Fv[b] - acc;
-    }
-    // Q = t G'G (lower)
-    for (int p = warp; p < k * (k + 1) / 2; p += nw) {
-        int r = (int)((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
-        while (r * (r + 1) / 2 > p) --r;
-        while ((r + 1) * (r + 2) / 2 <= p) ++r;
-        const int col = p - r * (r + 1) / 2;
-        const double* Gr = gcol(a.G, a.ldg, a.slot, r);
-        const double* Gc = gcol(a.G, a.ldg, a.slot, col);
-        double acc = 0.0;
-        for (int i = lane; i < m; i += 32) acc = fma(Gr[i], Gc[i], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) Q[r + (size_t)col * k] = t * acc;
-    }
-    for (int i = tid; i < m; i += blockDim.x) a.eta[i] = 0.0;
-    if (tid == 0) flag = 0;
-    __syncthreads();
-
-    double dir_prev = 0.0;
-    int cnt = 0;
-    while (true) {
-        ++cnt;
-        for (int b = warp; b < k; b += nw) {
-            const double* Gb = gcol(a.G, a.ldg, a.slot, b);
-            double acc = 0.0;
-            for (int i = lane; i < m; i += 32) acc = fma(Gb[i], a.eta[i], acc);
-            acc = warp_sum(acc);
-            if (lane == 0) c[b] = zeta[b] + (-t) * acc;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            const bool ok = warp_qp(k, Q, c, lam, qpws);
-            if (!ok && lane == 0) flag = 1;
-        }
-        __syncthreads();
-        if (flag) break;
-        double acc2 = 0.0;
-        for (int i = tid; i < m; i += blockDim.x) {
-            double tmp = 0.0;
-            for (int b = 0; b < k; ++b) tmp = fma(gcol(a.G, a.ldg, a.slot, b)[i], lam[b], tmp);
-            double e = -a.gam[i] / t + tmp;
-            e = (e > 0) ? e : 0;
-            a.eta[i] = e;
-            const double dg = t * (e - tmp);
-            a.dgam[i] = dg;
-            acc2 += dg * dg;
-        }
-        const double dir_curr = sqrt(block_sum(acc2, red));
-        bool done = fabs(dir_curr - dir_prev) / (1.0 + dir_curr) < 1e-5;
-        if (cnt >= 50) {
-            done = true;
-            t *= 0.95;
-        }
-        dir_prev = dir_curr;
-        if (done) break;
-    }
-    if (flag) {
-        if (tid == 0) atomicOr(&a.istate[BI_ERR], 2);
-        return;
-    }
-    for (int b = tid; b < k; b += blockDim.x) a.lam[b] = lam[b];
-    if (a.gtest)
-        for (int i = tid; i < m; i += blockDim.x) a.gtest[i] = a.gam[i] + a.dgam[i];
-    if (tid == 0) a.dstate[BD_T] = t;
+    lambda_eta_body(a, sm);
 }
 
 __global__ void solve_lambda_kernel(int k, const double* Q, const double* c, double* lam, int* err,
                                     double* ws_global)
 {
     extern __shared__ __align__(16) double sm[];
-    const bool in_smem = k <= QP_SMEM_K;
-    double* cl = sm;
-    double* ll = cl + k;
-    double* ws = in_smem ? ll + k : ws_global;
-    for (int b = threadIdx.x; b < k; b += 32) cl[b] = c[b];
-    __syncwarp();
-    const bool ok = warp_qp(k, Q, cl, ll, ws);
-    __syncwarp();
-    for (int b = threadIdx.x; b < k; b += 32) lam[b] = ll[b];
-    if (threadIdx.x == 0) *err = ok ? 0 : 1;
+    solve_lambda_body(k, Q, c, lam, err, ws_global, sm);
 }
 
-struct StepArgs {
-    const double* G;
-    int ldg;
-    int m;
-    int n;
-    int cap;
-    const double* L;
-    const double* Xb;
-    const double* phi_out;
-    double* Fv;
-    int* slot;
-    int* slot_old;
-    const double* lam;
-    double* gam;
-    const double* gtest;
-    double* dstate;
-    int* istate;
-};
-
-__global__ void __launch_bounds__(256) bundle_step_kernel(StepArgs a)
-{
-    __shared__ double red[64];
-    __shared__ double zlam[1];
-    __shared__ int s_serious;
-    __shared__ unsigned char used[BQB_MAX_BUNDLE + 8];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const int k = a.istate[BI_K];
-    const int next = a.istate[BI_NEXT];
-    const int n = a.n;
-    const double f = a.dstate[BD_F];
-    double t = a.dstate[BD_T];
-    const double phi = a.phi_out[0];
-    if ((int)a.phi_out[2] != 0 && tid == 0) atomicOr(&a.istate[BI_ERR], 4);
-
-    // f_test = phi + sum(gamma_test)
-    double sg = 0.0;
-    for (int i = tid; i < a.m; i += blockDim.x) sg += a.gtest[i];
-    const double ftest = phi + block_sum(sg, red);
-    // del = f - (F + G'gamma_test)'lambda
-    if (tid == 0) zlam[0] = 0.0;
-    __syncthreads();
-    double dl = 0.0;
-    for (int b = warp; b < k; b += nw) {
-        const double* Gb = a.G + (size_t)a.slot[b] * a.ldg;
-        double acc = 0.0;
-        for (int i = lane; i < a.m; i += 32) acc = fma(Gb[i], a.gtest[i], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) dl += (a.Fv[b] + acc) * a.lam[b];
-    }
-    const double del = f - block_sum(dl, red);
-    // F of the new element: <L, X_test> over the upper triangle, 2x off-diagonal
-    const double* Xt = a.Xb + (size_t)next * n * n;
-    double fv = 0.0;
-    for (int i = warp; i < n; i += nw) {
-        for (int j = i + lane; j < n; j += 32) {
-            const size_t e = j + (size_t)i * n;
-            fv += (i == j) ? a.L[e] * Xt[e] : 2 * a.L[e] * Xt[e];
-        }
-    }
-    const double Fnew = block_sum(fv, red);
-
-    if (tid == 0) {
-        double lmax = -BIG_NUMBER;
-        for (int b = 0; b < k; ++b) lmax = (a.lam[b] > lmax) ? a.lam[b] : lmax;
-        const bool serious = (f - ftest > 0.05 * del);
-        s_serious = serious ? 1 : 0;
-        for (int b = 0; b < k; ++b) a.slot_old[b] = a.slot[b];
-        int kept = 0;
-        const int scan = serious ? k : k - 1;
-        for (int b = 0; b < scan; ++b) {
-            if (a.lam[b] < 0.01 * lmax) continue;
-            a.slot[kept] = a.slot_old[b];
-            a.Fv[kept] = a.Fv[b];
-            ++kept;
-        }
-        int bundle;
-        if (serious) {
-            bundle = kept;
-            if (bundle == BQB_MAX_BUNDLE) a.istate[BI_ERR] |= 1;
-            a.slot[bundle] = next;
-            a.Fv[bundle] = Fnew;
-            ++bundle;
-            a.dstate[BD_F] = ftest;
-            t *= 1.01;
-        } else {
-            const double Flast = a.Fv[k - 1];
-            const int slast = a.slot_old[k - 1];
-            bundle = kept + 1;   // PP->bundle -= subtracted
-            if (bundle == BQB_MAX_BUNDLE) a.istate[BI_ERR] |= 1;
-            a.slot[bundle] = slast;
-            a.Fv[bundle] = Flast;
-            a.slot[bundle - 1] = next;
-            a.Fv[bundle - 1] = Fnew;
-            ++bundle;
-            t /= 1.01;
-        }
-        for (int q = 0; q < a.cap; ++q) used[q] = 0;
-        for (int b = 0; b < bundle; ++b) used[a.slot[b]] = 1;
-        int nf = -1;
-        for (int q = 0; q < a.cap; ++q)
-            if (!used[q]) {
-                nf = q;
-                break;
-            }
-        if (nf < 0) {
-            a.istate[BI_ERR] |= 8;
-            nf = next;
-        }
-        a.istate[BI_KOLD] = k;
-        a.istate[BI_K] = bundle;
-        a.istate[BI_SERIOUS] = serious ? 1 : 0;
-        a.istate[BI_LAST] = next;
-        a.istate[BI_NEXT] = nf;
-        a.dstate[BD_T] = t;
-        a.dstate[BD_FTEST] = ftest;
-        a.dstate[BD_DEL] = del;
-    }
-    __syncthreads();
-    if (s_serious)
-        for (int i = tid; i < a.m; i += blockDim.x) a.gam[i] = a.gtest[i];
-}
+__global__ void __launch_bounds__(LE_THREADS) bundle_step_kernel(StepArgs a) { bundle_step_body(a); }
 
 __global__ void bundle_xcomb_kernel(const double* __restrict__ Xb, const int* __restrict__ slot_old,
                                     const double* __restrict__ lam, const int* __restrict__ istate,
                                     double* __restrict__ X, size_t nn)
 {
-    if (!istate[BI_SERIOUS]) return;
-    const int k = istate[BI_KOLD];
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (size_t)gridDim.x * blockDim.x) {
-        double acc = 0.0;
-        for (int b = 0; b < k; ++b) acc = fma(Xb[(size_t)slot_old[b] * nn + e], lam[b], acc);
-        X[e] = acc;
-    }
+    bundle_xcomb_body(Xb, slot_old, lam, istate, X, nn, (size_t)blockIdx.x * blockDim.x + threadIdx.x,
+                      (size_t)gridDim.x * blockDim.x);
 }
 
-__global__ void bundle_fval_kernel(const double* __restrict__ L, const double* __restrict__ Xb, int n,
-                                   const int* __restrict__ slot_ptr, const int* __restrict__ pos_ptr,
-                                   double* __restrict__ Fv)
+__global__ void __launch_bounds__(LE_THREADS) bundle_fval_kernel(const double* __restrict__ L,
+                                                                 const double* __restrict__ Xb, int n,
+                                                                 const int* __restrict__ slot_ptr,
+                                                                 const int* __restrict__ pos_ptr,
+                                                                 double* __restrict__ Fv)
 {
-    __shared__ double red[64];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const double* Xt = Xb + (size_t)(*slot_ptr) * n * n;
-    double fv = 0.0;
-    for (int i = warp; i < n; i += nw)
-        for (int j = i + lane; j < n; j += 32) {
-            const size_t e = j + (size_t)i * n;
-            fv += (i == j) ? L[e] * Xt[e] : 2 * L[e] * Xt[e];
-        }
-    const double s = block_sum(fv, red);
-    if (threadIdx.x == 0) Fv[*pos_ptr] = s;
+    bundle_fval_body(L, Xb, n, slot_ptr, pos_ptr, Fv);
 }
 
-// Append the element evaluated into slot NEXT at bundle position K
-// (src/bounding.c:291-318: overflow test, then ++bundle), pick the next
-// free slot.
 __global__ void bundle_append_kernel(int* __restrict__ slot, int* __restrict__ istate, int cap)
 {
-    __shared__ unsigned char used[BQB_MAX_BUNDLE + 8];
-    if (threadIdx.x != 0) return;
-    const int k = istate[BI_K];
-    const int next = istate[BI_NEXT];
-    if (k == BQB_MAX_BUNDLE) istate[BI_ERR] |= 1;
-    slot[k] = next;
-    istate[BI_LAST] = next;
-    istate[BI_K] = k + 1;
-    for (int q = 0; q < cap; ++q) used[q] = 0;
-    for (int b = 0; b <= k; ++b) used[slot[b]] = 1;
-    int nf = -1;
-    for (int q = 0; q < cap; ++q)
-        if (!used[q]) {
-            nf = q;
-            break;
-        }
-    if (nf < 0) {
-        istate[BI_ERR] |= 8;
-        nf = next;
-    }
-    istate[BI_NEXT] = nf;
-}
-
-size_t le_smem_bytes(int k)
-{
-    const size_t base = 3 * (size_t)k;
-    if (k <= QP_SMEM_K) return (base + (size_t)k * k + (size_t)k * k + 5 * (size_t)k) * sizeof(double);
-    return base * sizeof(double);
+    bundle_append_body(slot, istate, cap);
 }
 
 }  // namespace
@@ -581,7 +129,7 @@ void bundle_step_launch(BundleDev& b, const double* phi_out, const double* L, cu
 {
     StepArgs a{b.G.p, b.ldg, b.m, b.n, b.cap, L, b.Xb.p, phi_out, b.Fv.p, b.slot.p, b.slot_old.p,
                b.lam.p, b.gam.p, b.gtest.p, b.dstate.p, b.istate.p};
-    bundle_step_kernel<<<1, 256, 0, s>>>(a);
+    bundle_step_kernel<<<1, LE_THREADS, 0, s>>>(a);
     BQB_COUNT_LAUNCH();
     check_launch("bundle_step_kernel");
 }
@@ -605,7 +153,7 @@ void bundle_append_launch(BundleDev& b, cudaStream_t s)
 
 void bundle_fval_launch(BundleDev& b, const double* L, const int* slot_ptr, const int* pos_ptr, cudaStream_t s)
 {
-    bundle_fval_kernel<<<1, 256, 0, s>>>(L, b.Xb.p, b.n, slot_ptr, pos_ptr, b.Fv.p);
+    bundle_fval_kernel<<<1, LE_THREADS, 0, s>>>(L, b.Xb.p, b.n, slot_ptr, pos_ptr, b.Fv.p);
     BQB_COUNT_LAUNCH();
     check_launch("bundle_fval_kernel");
 }

@@ -19,41 +19,6 @@
 
 namespace bqb {
 
-unsigned tri_negmask(int type)
-{
-    // type 1: (1,1,1); 2: (1,1,-1); 3: (1,-1,1); 4: (-1,1,1)
-    switch (type) {
-        case 1: return 0u;
-        case 2: return 4u;
-        case 3: return 2u;
-        default: return 1u;
-    }
-}
-
-unsigned pent_negmask(int type)
-{
-    // H1 = ee', e = 1; H2: e0 = -1; H3: e0 = e1 = -1
-    return type == 1 ? 0u : (type == 2 ? 1u : 3u);
-}
-
-unsigned hept_negmask(int type)
-{
-    // H1: none; H2: e0; H3: e0, e1; H4: e0, e1, e2
-    return type == 1 ? 0u : (type == 2 ? 1u : (type == 3 ? 3u : 7u));
-}
-
-CutRec pack_cut(int k, const int* p, unsigned negmask)
-{
-    unsigned q[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int a = 0; a < k; ++a) q[a] = (unsigned)p[a] & 0xffffu;
-    CutRec r;
-    r.x = q[0] | (q[1] << 16);
-    r.y = q[2] | (q[3] << 16);
-    r.z = q[4] | (q[5] << 16);
-    r.w = q[6] | ((unsigned)k << 16) | ((negmask & 0x7fu) << 24);
-    return r;
-}
-
 void PairCSR::build(const std::vector<CutRec>& cuts)
 {
     struct E { uint32_t key, code; };
@@ -124,34 +89,8 @@ __global__ void __launch_bounds__(256) opB_kernel(const CutRec* __restrict__ cut
     const int j = blockIdx.y;
     if (c >= m) return;
     const double* X = Xbase + (size_t)(slot ? slot[j] : j) * ldx_mat;
-    const CutRec r = cuts[c];
-    const unsigned p[7] = {r.x & 0xffffu, r.x >> 16, r.y & 0xffffu, r.y >> 16,
-                           r.z & 0xffffu, r.z >> 16, r.w & 0xffffu};
-    const int k = (int)((r.w >> 16) & 0xffu);
-    const unsigned neg = (r.w >> 24) & 0x7fu;
-    double acc = 0.0;
-    bool first = true;
-    for (int a = 0; a < k; ++a) {
-        for (int b = a + 1; b < k; ++b) {
-            // coefficient inside the bracket is -e_a e_b
-            const bool plus = ((neg >> a) ^ (neg >> b)) & 1u;
-            const double x = X[p[a] + (size_t)p[b] * n];
-            if (first) {
-                acc = plus ? x : -x;
-                first = false;
-            } else {
-                acc = plus ? acc + x : acc - x;
-            }
-        }
-    }
     double* y = Y + c + (size_t)(slot ? slot[j] : j) * ldy;
-    const double y0 = init_one ? 1.0 : *y;
-    if (k == 3)
-        *y = y0 - acc;
-    else if (k == 5)
-        *y = y0 - 0.5 * acc;
-    else
-        *y = y0 - (1.0 / 3.0) * acc;
+    *y = cut_apply(cuts[c], X, n, init_one ? 1.0 : *y);
 }
 
 __global__ void __launch_bounds__(256) opBt_kernel(const uint32_t* __restrict__ pair_uv,
@@ -166,22 +105,7 @@ __global__ void __launch_bounds__(256) opBt_kernel(const uint32_t* __restrict__ 
     const unsigned u = uv & 0xffffu, v = uv >> 16;
     const size_t e1 = u + (size_t)v * n, e2 = v + (size_t)u * n;
     double x1 = X[e1], x2 = X[e2];
-    const unsigned b = offsets[q], eidx = offsets[q + 1];
-    for (unsigned i = b; i < eidx; ++i) {
-        const unsigned code = contrib[i];
-        const int c = (int)(code >> 1);
-        const double tc = t[c];
-        const double temp = c < m_tri ? 0.5 * tc : (c < m_tp ? 0.25 * tc : (1.0 / 6.0) * tc);
-        // X -= B^T(t): coefficient of X_uv in B is -scale e_u e_v, so the
-        // entry moves by +e_u e_v * temp
-        if (code & 1u) {
-            x1 -= temp;
-            x2 -= temp;
-        } else {
-            x1 += temp;
-            x2 += temp;
-        }
-    }
+    pair_apply(contrib, offsets[q], offsets[q + 1], m_tri, m_tp, t, &x1, &x2);
     X[e1] = x1;
     X[e2] = x2;
 }

@@ -47,4 +47,8 @@ void ipm_launch_one(const IpmDesc& d, cudaStream_t s);
 // status instead of raising it.
 cudaError_t ipm_launch_prepared(const IpmDesc& d, int place, size_t smem_bytes, cudaStream_t s);
 
+// Device address of the IPM work counters (for kernels in other files that
+// run the IPM body).
+double* ipm_stats_device();
+
 }  // namespace bqb

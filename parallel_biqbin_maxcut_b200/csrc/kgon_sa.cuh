@@ -13,6 +13,7 @@
 // reference's list rule, so only the random numbers differ from the
 // reference's separation.
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 #include "bqb_common.cuh"
@@ -41,6 +42,119 @@ struct KgonSaState {
     HostBuf<int> hperm;
     HostBuf<int> hstat;
 };
+
+__device__ __forceinline__ uint32_t sa_next(uint64_t& state)
+{
+    uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (uint32_t)(z >> 33);
+}
+
+// Starting temperature k^2 (n + sum_{i<j} 2|X_ij|) / (n (n-1)), summed by
+// the calling thread in the reference's loop order.
+__device__ inline double kgon_temperature(const double* Xs, int n, int K)
+{
+    double sumX = n;
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) sumX = __dadd_rn(sumX, __dmul_rn(2.0, fabs(Xs[j + (size_t)i * n])));
+    double t = (double)(K * K);
+    t = __dmul_rn(t, sumX);
+    return __ddiv_rn(t, (double)(n * (n - 1)));
+}
+
+// One annealing chain (chain index c, type (c % types) + 1) run by the
+// calling thread.  Its permutation lives at P[i * pstride + lane].
+// Writes cost_out[c], perm_out[7c .. 7c+6]; sets *status on the round limit.
+__device__ inline void kgon_chain(const double* __restrict__ Xs, int n, int K, int types, int c,
+                                  unsigned long long seed, double t0, unsigned short* P, int pstride, int lane,
+                                  double* __restrict__ cost_out, int* __restrict__ perm_out, int* status)
+{
+    const int type = c % types + 1;
+    // H(a, b) = e_a e_b with e_a = -1 for a < type - 1, else +1
+    auto e = [&](int a) { return a < type - 1 ? -1 : 1; };
+    auto PA = [&](int i) -> unsigned short& { return P[(size_t)i * pstride + lane]; };
+    auto XA = [&](int a, int b) { return Xs[a + (size_t)n * b]; };
+
+    uint64_t rs = seed + (uint64_t)(c + 1) * SA_CHAIN_STRIDE;
+    for (int i = 0; i < n; ++i) PA(i) = (unsigned short)i;
+    for (int i = n - 1; i > 0; --i) {
+        const int r = (int)(sa_next(rs) % (uint32_t)i);
+        const unsigned short tmp = PA(i);
+        PA(i) = PA(r);
+        PA(r) = tmp;
+    }
+    double t1 = t0;
+    int m1 = n;
+    double sol = K;
+    for (int i = 0; i < K; ++i)
+        for (int j = i + 1; j < K; ++j)
+            sol = __dadd_rn(sol, __dmul_rn((double)(2 * e(j) * e(i)), XA(PA(j), PA(i))));
+    double cost = 1e9;
+    int best[7] = {0, 0, 0, 0, 0, 0, 0};
+    int not_done = 1, rounds = 0;
+    while (not_done > 0 && rounds < SA_MAX_ROUNDS) {
+        not_done = 0;
+        for (int it = 0; it < m1; ++it) {
+            int i1 = (int)(sa_next(rs) % (uint32_t)K);
+            int i2 = (int)(sa_next(rs) % (uint32_t)n);
+            if (i2 < i1) {
+                const int tmp = i1;
+                i1 = i2;
+                i2 = tmp;
+            }
+            const int p1 = PA(i1), p2 = PA(i2);
+            double delta = 0.0;
+            for (int i = 0; i < K; ++i) {
+                const int pi = PA(i);
+                const double d = __dsub_rn(XA(pi, p2), XA(pi, p1));
+                delta = __dadd_rn(delta, e(i) * e(i1) > 0 ? d : -d);
+            }
+            if (i2 < K)
+                for (int i = 0; i < K; ++i) {
+                    const int pi = PA(i);
+                    const double d = __dsub_rn(XA(pi, p1), XA(pi, p2));
+                    delta = __dadd_rn(delta, e(i) * e(i2) > 0 ? d : -d);
+                }
+            delta = __dmul_rn(delta, 2.0);
+            const double tv1 = __dsub_rn(2.0, __dmul_rn(2.0, XA(p2, p1)));
+            double tv2 = 1.0;
+            if (i2 < K) tv2 = __dadd_rn(tv2, __dadd_rn((double)(-2 * e(i1) * e(i2)), 1.0));
+            delta = __dadd_rn(delta, __dmul_rn(tv1, tv2));
+            const double sol_temp = __dadd_rn(sol, delta);
+            int accept;
+            if (delta > 0) {
+                const double dt1 = __ddiv_rn(delta, t1);
+                if (dt1 > 5)
+                    accept = 0;
+                else
+                    accept = __ddiv_rn((double)sa_next(rs), (double)SA_RAND_MAX) < exp(-dt1) ? 1 : 0;
+            } else {
+                accept = 1;
+            }
+            if (accept) {
+                if (fabs(delta) > 0.001) not_done = 1;
+                PA(i1) = (unsigned short)p2;
+                PA(i2) = (unsigned short)p1;
+                sol = sol_temp;
+                if (sol < cost) {
+                    cost = sol;
+#pragma unroll
+                    for (int a = 0; a < 7; ++a)
+                        if (a < K) best[a] = PA(a);
+                }
+            }
+        }
+        t1 = __dmul_rn(t1, 0.6);
+        m1 = (int)round(__dmul_rn((double)m1, 1.1));
+        ++rounds;
+    }
+    if (not_done > 0) atomicOr(status, 1);
+    cost_out[c] = cost;
+#pragma unroll
+    for (int a = 0; a < 7; ++a) perm_out[(size_t)c * 7 + a] = a < K ? best[a] : 0;
+}
 
 // Run `chains` chains of the k-gonal annealing on the n x n matrix dX
 // (device, column-major).  Chain c anneals type (c % types) + 1, i.e. the

@@ -1,0 +1,91 @@
+// Fused node bounding: one CTA bounds a whole B&B node on the device.
+#pragma once
+#include <stdint.h>
+
+#include <vector>
+
+#include "bqb_common.cuh"
+
+namespace bqb {
+
+// Arrays of one CTA's slot in the fused kernel's arena (byte offsets in
+// FusedCfg::off).
+enum NkArray : int {
+    NK_L, NK_L0, NK_X, NK_IPMWS, NK_OUT, NK_XB, NK_G, NK_FV, NK_LAM, NK_GAM, NK_GTEST, NK_DGAM, NK_ETA,
+    NK_DSTATE, NK_QPWS, NK_SLOT, NK_SLOTOLD, NK_ISTATE,
+    NK_TRICODE, NK_TRIY, NK_PENTKEY, NK_PENTY, NK_HEPTKEY, NK_HEPTY, NK_REC,
+    NK_CSROFF, NK_CSRCUR, NK_CONTRIB, NK_HASH,
+    NK_TSCNT, NK_TSCAND, NK_TSLIST,
+    NK_SACOST, NK_SAPERM, NK_KLIST, NK_KLISTV,
+    NK_HZ, NK_HV, NK_HX, NK_HVAL, NK_HSOL, NK_HBEST, NK_XH, NK_FREE, NK_FIXED,
+    NK_COUNT
+};
+
+// Per-node status bits of the fused kernel.  A node with any bit set is
+// bounded again by an engine on the host (bqb_bound_nodes), which either
+// handles the case (capacities) or reports the reference's error.
+enum NkStatus : int {
+    NKS_BUNDLE_CAP = 1,    // more bundle elements than the slot holds
+    NKS_CUT_CAP = 2,       // more cuts than the slot holds
+    NKS_QP = 4,            // lambda_eta / solve_lambda failure
+    NKS_IPM = 8,           // IPM failure
+    NKS_HEUR = 16,         // heuristic Cholesky failure or 1-opt overflow
+    NKS_SIZE = 32,         // subproblem too large for the fused kernel
+};
+
+// Phases timed inside the fused kernel (globaltimer, thread 0 of each CTA).
+enum NkPhase : int {
+    NKP_SUB, NKP_IPM, NKP_HEUR, NKP_TRISEP, NKP_TRILIST, NKP_KGON, NKP_CUTS, NKP_OPBT, NKP_OPB, NKP_LAMBDA,
+    NKP_STEP, NKP_COUNT
+};
+
+struct FusedCfg {
+    // problem
+    const double* P0L;   // SP->L, N0 x N0
+    int N0;
+    int count;           // nodes in this launch
+    int rank;
+    double diff;
+    // reference parameters (src/biqbin.h:49-84)
+    int init_bundle_iter, max_bundle_iter, triag_iter, pent_iter, hept_iter, max_outer_iter, extra_iter;
+    double violated_TriIneq;
+    int TriIneq, PentIneq, HeptaIneq, Pent_Trials, Hepta_Trials, include_Pent, include_Hepta, use_diff;
+    unsigned long long seed;
+    // slot capacities
+    int bcap;            // bundle slots (physical)
+    int mt_cap, mp_cap, mh_cap;
+    int hash_size;       // power of two >= 2 mt_cap
+    int sa_chains;       // max(Pent_Trials * 3, Hepta_Trials * 4)
+    size_t smem_bytes;   // dynamic shared memory of the launch
+    // node I/O (device)
+    const int* xfixed;   // count x (N0 - 1)
+    const int* solx;     // count x (N0 - 1)
+    double* bound;       // count
+    double* fracsol;     // count x (N0 - 1)
+    double* hval;        // count: best value the node's heuristic calls reported
+    int* hsol;           // count x (N0 - 1): its 0/1 solution
+    int* status;         // count
+    int* next;           // node counter
+    unsigned long long* lb;   // incumbent, order-preserving bits of a double
+    double* ipm_stats;
+    unsigned long long* prof;   // NKP_COUNT phase times (ns, summed over CTAs)
+    // slot arena
+    unsigned char* arena;
+    size_t slot_bytes;
+    size_t off[NK_COUNT];
+};
+
+// Largest N0 the fused kernel handles (register-resident IPM).
+constexpr int NK_NMAX = 128;
+
+// Shared-memory bytes the fused kernel needs for problems up to N0 with
+// TriIneq = T and bcap bundle slots.
+size_t nk_smem_bytes(int N0, int T, int bcap, size_t smem_optin);
+
+// Lay out the arena: fills cfg.off and cfg.slot_bytes from the capacities
+// in cfg; returns the bytes of one slot.
+size_t nk_layout(FusedCfg& cfg);
+
+void nk_launch(const FusedCfg& cfg, int slots, cudaStream_t s);
+
+}  // namespace bqb

@@ -1,0 +1,90 @@
+"""Fused node bounding (bqb_bound_nodes_fused): one CTA bounds a whole node
+on the device.
+
+Parity: with the incumbent held at the optimum (the heuristic can then never
+change it) and pentagonal / heptagonal separation off (the only other use of
+random numbers), a node's bound does not depend on the random streams, and
+the fused kernel runs the engine path's arithmetic (same IPM, lambda_eta,
+bundle step and cut-operator code at the same thread count, the same
+triangle list), so its bounds and fractional solutions must equal the serial
+drop-in SDPbound (src/bounding.c) up to floating-point contraction: the
+shared device bodies are compiled into two kernels, and the compiler may fuse
+a multiply and an add into an FMA in one and not in the other, a last-bit
+difference that the bundle iterations carry to about 1e-8 relative (most
+nodes agree bit for bit).  Tolerance: 1e-7 relative on bounds, 1e-6 absolute
+on fractional solutions.  With the random streams in play every bound must
+still be an upper bound of the node."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import O, instances
+from parallel_biqbin_maxcut_b200 import _lib
+
+NV = 60
+
+
+def _nodes(count, kmax, seed, nv=NV):
+    out = (_lib.BabNode * count)()
+    for q, (xf, sol) in enumerate(instances.random_fixings(nv, count, kmax, seed)):
+        out[q].xfixed[: nv - 1] = [int(v) for v in xf]
+        out[q].sol[: nv - 1] = [int(v) for v in sol]
+        out[q].level = int(xf.sum())
+    return out
+
+
+def _copy(nodes):
+    c = (_lib.BabNode * len(nodes))()
+    C.memmove(c, nodes, C.sizeof(nodes))
+    return c
+
+
+def _serial(lib, nodes):
+    SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+    PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
+    return np.array([lib.Evaluate(C.byref(nodes[i]), SP, PP, 1) for i in range(len(nodes))])
+
+
+@pytest.fixture(scope="module")
+def solved(lib):
+    A = instances.gnp_pm1(NV, 0.5, 11)
+    r = _lib.solve(A, include_Pent=0, include_Hepta=0)
+    assert lib.Bab_LBGet() == r["best_value"]
+    return A, r
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kmax,seed", [(25, 31), (45, 32)])
+def test_fused_bounds_equal_serial(lib, solved, kmax, seed):
+    nodes = _nodes(40, kmax, seed)
+    ser = _copy(nodes)
+    want = _serial(lib, ser)
+    f0 = lib.bqb_fused_fallbacks()
+    got = np.zeros(len(nodes))
+    assert lib.bqb_bound_nodes_fused(nodes, len(nodes), 1, _lib.dptr(got)) == 0
+    assert lib.bqb_fused_fallbacks() == f0
+    np.testing.assert_allclose(got, want, rtol=1e-7, atol=0)
+    assert np.mean(got == want) >= 0.5
+    for i in range(len(nodes)):
+        np.testing.assert_allclose(nodes[i].fracsol[: NV - 1], ser[i].fracsol[: NV - 1], rtol=0, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_fused_bounds_with_kgon_separation(lib, solved):
+    A, _ = solved
+    _lib.set_params(lib, _lib.make_params())
+    try:
+        nodes = _nodes(24, 45, seed=33)
+        b = np.zeros(len(nodes))
+        assert lib.bqb_bound_nodes_fused(nodes, len(nodes), 1, _lib.dptr(b)) == 0
+        SPL = O.build_SP_L(A)
+        rng = np.random.default_rng(6)
+        for i in range(len(nodes)):
+            xf = np.array(nodes[i].xfixed[: NV - 1])
+            sol = np.array(nodes[i].sol[: NV - 1])
+            for _ in range(20):
+                x = np.where(xf == 1, sol, rng.integers(0, 2, NV - 1))
+                assert O.evaluateSolution(SPL, x) <= b[i] + 1e-6
+    finally:
+        _lib.set_params(lib, _lib.make_params(include_Pent=0, include_Hepta=0))
