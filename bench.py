@@ -272,10 +272,14 @@ def run_gpu(args):
     barrier()
     clocks.start()
     bounds_dev = []
+    node_ms = []
     for s in timed:
         arm.l2_flush()
         torch.cuda.synchronize()
         bounds_dev.append(fused(arrays[s]))
+        nt = np.zeros(B)
+        lib.bqb_fused_node_times(_lib.dptr(nt), B)
+        node_ms.append(nt)
     barrier()
     clk = clocks.stop()
     launches = lib.bqb_kernel_launches() - launches0
@@ -361,6 +365,11 @@ def run_gpu(args):
             "ipm_iterations": int(stats[2]), "ipm_problems": int(stats[1]),
             "linesearch_factorizations": int(stats[3]),
             "fallback_nodes": int(fst[3]), "fallback_ms": fst[4],
+            "node_ms": {"mean": float(np.mean(np.concatenate(node_ms))),
+                        "p90": float(np.percentile(np.concatenate(node_ms), 90)),
+                        "max": float(np.max(np.concatenate(node_ms))),
+                        "sum_over_slots": float(np.sum(np.concatenate(node_ms)) / 1e3 / max(fst[0], 1)),
+                        "note": "device time per node; sum_over_slots = CTA-seconds of node work per step"},
             "phase_share": {nm: round(prof[i] / tot_cta_s, 4) for i, nm in enumerate(phase_names)},
             "phase_cta_seconds": {nm: round(prof[i], 3) for i, nm in enumerate(phase_names)}}
 

@@ -262,6 +262,9 @@ void bqb_fused_stats_reset(void);
  * scan, triangle list update, k-gonal separation, cut upload, B^T, B,
  * lambda_eta, bundle step}. */
 void bqb_fused_profile(double *out);
+/* Device milliseconds each node of the last bqb_bound_nodes_fused call took
+ * (node order of that call); writes at most `count`, returns how many. */
+int bqb_fused_node_times(double *out, int count);
 
 /* Pentagonal (k = 5) / heptagonal (k = 7) separation chains on the GPU:
  * `chains` independent runs of the annealing of qap_simulated_annealing

@@ -116,6 +116,7 @@ SIGNATURES = {
     "bqb_fused_stats": (None, [D]),
     "bqb_fused_stats_reset": (None, []),
     "bqb_fused_profile": (None, [D]),
+    "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),
     "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
     "bqb_init": (C.c_int, [C.c_int]),

@@ -11,6 +11,7 @@
 // path exactly.
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -34,11 +35,14 @@ struct FusedState {
     cudaStream_t stream = nullptr;
     DevBuf<unsigned char> arena;
     DevBuf<double> P0L, bound, fracsol, hval;
-    DevBuf<int> xf, sx, hsol, status, next;
+    DevBuf<int> xf, sx, hsol, status, next, order;
+    DevBuf<unsigned long long> node_ns;
+    std::vector<double> last_node_ms;
     DevBuf<unsigned long long> lb, prof;
     HostBuf<int> hfix;
     HostBuf<double> hb, hfs, hhv;
-    HostBuf<int> hhs, hst;
+    HostBuf<int> hhs, hst, hord;
+    HostBuf<unsigned long long> hns;
     const double* P0L_src = nullptr;
     int P0N = 0;
     unsigned P0L_gen = 0;
@@ -144,6 +148,23 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
         memcpy(hf + (size_t)i * N, nodes[i].xfixed, N * sizeof(int));
         memcpy(hf + cN + (size_t)i * N, nodes[i].sol.X, N * sizeof(int));
     }
+    // heaviest nodes first (longest-processing-time order): a node's work
+    // grows with its subproblem size, so free vertices decide the order
+    {
+        std::vector<int> ord(count);
+        std::vector<int> nfree(count);
+        for (int i = 0; i < count; ++i) {
+            ord[i] = i;
+            int nf = 0;
+            for (int j = 0; j < N; ++j) nf += nodes[i].xfixed[j] ? 0 : 1;
+            nfree[i] = nf;
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return nfree[a] > nfree[b]; });
+        int* ho = F.hord.ensure(count);
+        memcpy(ho, ord.data(), count * sizeof(int));
+        F.order.ensure(count);
+        BQB_CUDA(cudaMemcpyAsync(F.order.p, ho, count * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
     F.xf.ensure(cN);
     F.sx.ensure(cN);
     BQB_CUDA(cudaMemcpyAsync(F.xf.p, hf, cN * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -153,6 +174,7 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     F.hval.ensure(count);
     F.hsol.ensure(cN);
     F.status.ensure(count);
+    F.node_ns.ensure(count);
     F.next.ensure(1);
     F.lb.ensure(1);
     F.arena.ensure(slot_bytes * slots);
@@ -167,6 +189,8 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     c.hval = F.hval.p;
     c.hsol = F.hsol.p;
     c.status = F.status.p;
+    c.node_ns = F.node_ns.p;
+    c.order = F.order.p;
     c.next = F.next.p;
     c.lb = F.lb.p;
     c.ipm_stats = ipm_stats_device();
@@ -194,7 +218,11 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     BQB_CUDA(cudaMemcpyAsync(hhv, F.hval.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaMemcpyAsync(hhs, F.hsol.p, cN * sizeof(int), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaMemcpyAsync(hst, F.status.p, count * sizeof(int), cudaMemcpyDeviceToHost, s));
+    unsigned long long* hns = F.hns.ensure(count);
+    BQB_CUDA(cudaMemcpyAsync(hns, F.node_ns.p, count * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaStreamSynchronize(s));
+    F.last_node_ms.assign(count, 0.0);
+    for (int i = 0; i < count; ++i) F.last_node_ms[i] = 1e-6 * (double)hns[i];
     float kms = 0.f;
     BQB_CUDA(cudaEventElapsedTime(&kms, F.ev0, F.ev1));
     F.st_calls += 1;
@@ -257,6 +285,17 @@ BQB_API void bqb_fused_stats(double* out)
     out[2] = F.st_kernel_ms;
     out[3] = F.st_fallback_nodes;
     out[4] = F.st_fallback_ms;
+}
+
+// Device milliseconds of every node of the last bqb_bound_nodes_fused call
+// (as many as that call had, at most `count`); returns how many were written.
+BQB_API int bqb_fused_node_times(double* out, int count)
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    const int m = (int)F.last_node_ms.size() < count ? (int)F.last_node_ms.size() : count;
+    for (int i = 0; i < m; ++i) out[i] = F.last_node_ms[i];
+    return m;
 }
 
 BQB_API void bqb_fused_stats_reset(void)

@@ -1288,9 +1288,13 @@ __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
     k.N = c.N0 - 1;
     while (true) {
         int node = 0;
-        if (threadIdx.x == 0) node = atomicAdd(c.next, 1);
+        if (threadIdx.x == 0) {
+            const int q = atomicAdd(c.next, 1);
+            node = q < c.count ? c.order[q] : c.count;
+        }
         node = bcast_i(node);
         if (node >= c.count) break;
+        const unsigned long long t_node = threadIdx.x == 0 ? nk_now() : 0ull;
         k.node = node;
         k.xf = c.xfixed + (size_t)node * k.N;
         k.sx = c.solx + (size_t)node * k.N;
@@ -1312,6 +1316,7 @@ __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
         if (threadIdx.x == 0) {
             c.bound[node] = b;
             c.status[node] = k.status;
+            c.node_ns[node] = nk_now() - t_node;
         }
         __syncthreads();
     }

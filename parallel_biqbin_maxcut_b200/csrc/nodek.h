@@ -65,6 +65,8 @@ struct FusedCfg {
     double* hval;        // count: best value the node's heuristic calls reported
     int* hsol;           // count x (N0 - 1): its 0/1 solution
     int* status;         // count
+    unsigned long long* node_ns;   // count: device time of each node's bound
+    const int* order;    // count: the order in which CTAs take the nodes
     int* next;           // node counter
     unsigned long long* lb;   // incumbent, order-preserving bits of a double
     double* ipm_stats;
