@@ -246,6 +246,19 @@ int bqb_bound_nodes(BabNode *nodes, int count, int rank, int threads, const doub
  * failure are bounded again by bqb_bound_nodes.  Returns 0, or 1 when SP
  * is not set up.  No reference counterpart. */
 int bqb_bound_nodes_fused(BabNode *nodes, int count, int rank, double *bounds);
+/* The same as a submission and a collection, so that several batches are
+ * in flight at once (up to 8, each on its own stream and device arena):
+ * the CTAs of a later batch take the SMs an earlier batch's last nodes
+ * leave idle.  bqb_fused_submit copies the nodes' fixings and returns a
+ * ticket >= 0 (-1: eight submissions are uncollected; -2: SP not set up;
+ * -3: the problem is outside the fused kernel's range, use
+ * bqb_bound_nodes; -4: count <= 0).  The incumbent each batch starts from
+ * is Bab_LBGet() at its submission.  bqb_fused_collect waits for a ticket
+ * and fills bounds[i] and nodes[i].fracsol of the array that was submitted
+ * (nodes the kernel hands back are bounded again by engines here);
+ * returns 0, or 1 for an unknown ticket. */
+long long bqb_fused_submit(const BabNode *nodes, int count, int rank);
+int bqb_fused_collect(long long ticket, BabNode *nodes, double *bounds);
 /* Nodes bqb_bound_nodes_fused handed back to engines so far. */
 long long bqb_fused_fallbacks(void);
 /* Set the incumbent value Bab_LBGet returns (lower or higher; BabSol is

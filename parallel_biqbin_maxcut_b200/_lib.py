@@ -113,6 +113,8 @@ SIGNATURES = {
                                   C.POINTER(C.c_void_p), D]),
     "bqb_bound_nodes_fused": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, D]),
     "bqb_fused_fallbacks": (C.c_longlong, []),
+    "bqb_fused_submit": (C.c_longlong, [C.POINTER(BabNode), C.c_int, C.c_int]),
+    "bqb_fused_collect": (C.c_int, [C.c_longlong, C.POINTER(BabNode), D]),
     "bqb_fused_stats": (None, [D]),
     "bqb_fused_stats_reset": (None, []),
     "bqb_fused_profile": (None, [D]),

@@ -1,14 +1,19 @@
-// Host side of the fused node kernel (nodek.cu): bqb_bound_nodes_fused.
+// Host side of the fused node kernel (nodek.cu).
 //
-// One call bounds a batch of nodes of the problem set up by
+// One submission bounds a batch of nodes of the problem set up by
 // process_adj_matrix: the nodes' fixings go to the device, one persistent
-// kernel bounds them all (one CTA per SM, nodes pulled from a counter),
-// bounds, fractional solutions and the best heuristic solution of every
-// node come back.  The incumbent enters as Bab_LBGet() and every improvement
-// found on the device is passed to Bab_LBUpd in node order afterwards.
-// Nodes the kernel flags (slot capacities, numerical failures) are bounded
-// again by an engine (bqb_bound_nodes), which follows the reference's code
-// path exactly.
+// kernel bounds them all (one CTA per SM, heaviest nodes first, nodes pulled
+// from a counter), and bounds, fractional solutions and the best heuristic
+// solution of every node come back.  The incumbent enters as Bab_LBGet()
+// and every improvement found on the device is passed to Bab_LBUpd in node
+// order when the batch is collected.  Nodes the kernel flags (slot
+// capacities, numerical failures) are bounded again by engines
+// (bqb_bound_nodes), which follow the reference's code path exactly.
+//
+// Submissions go to a ring of NK_PIPES pipes, each with its own stream,
+// arena and buffers, so several launches are in flight at once: when the
+// last, heaviest nodes of one batch hold a few SMs, the next batch's CTAs
+// take the rest.  bqb_bound_nodes_fused is a submission collected at once.
 #include <string.h>
 
 #include <algorithm>
@@ -30,27 +35,35 @@ extern double diff;
 namespace bqb {
 namespace {
 
+constexpr int NK_PIPES = 8;
+
+struct FusedPipe {
+    bool busy = false;
+    int count = 0, rank = 0, N = 0;
+    unsigned long long ticket = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf<unsigned char> arena;
+    DevBuf<double> bound, fracsol, hval;
+    DevBuf<int> xf, sx, hsol, status, next, order;
+    DevBuf<unsigned long long> lb, node_ns;
+    HostBuf<int> hfix, hhs, hst, hord;
+    HostBuf<double> hb, hfs, hhv;
+    HostBuf<unsigned long long> hns, hlb;
+};
+
 struct FusedState {
     std::mutex mu;
-    cudaStream_t stream = nullptr;
-    DevBuf<unsigned char> arena;
-    DevBuf<double> P0L, bound, fracsol, hval;
-    DevBuf<int> xf, sx, hsol, status, next, order;
-    DevBuf<unsigned long long> node_ns;
-    std::vector<double> last_node_ms;
-    DevBuf<unsigned long long> lb, prof;
-    HostBuf<int> hfix;
-    HostBuf<double> hb, hfs, hhv;
-    HostBuf<int> hhs, hst, hord;
-    HostBuf<unsigned long long> hns;
+    FusedPipe pipe[NK_PIPES];
+    unsigned long long next_ticket = 0;
+    DevBuf<double> P0L;
+    DevBuf<unsigned long long> prof;
     const double* P0L_src = nullptr;
     int P0N = 0;
     unsigned P0L_gen = 0;
     unsigned long long seed = 0x5eed0f0cb200ull;
-    unsigned long long calls = 0;
     long long fallbacks = 0;
-    // timing of the fused kernel (CUDA events on its stream)
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<double> last_node_ms;
     double st_calls = 0, st_nodes = 0, st_kernel_ms = 0, st_fallback_nodes = 0, st_fallback_ms = 0;
 };
 
@@ -74,26 +87,9 @@ int next_pow2(int v)
     return p;
 }
 
-}  // namespace
-}  // namespace bqb
-
-using namespace bqb;
-
-// Fused bounding of `count` nodes (see include/bqb_gpu.h).
-BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* bounds)
+// The reference parameters and slot capacities of a launch.
+void fill_cfg(FusedCfg& c, int N0, int count, int rank, unsigned long long seed, size_t smem_optin)
 {
-    if (count <= 0) return 0;
-    if (!SP || !SP->L) return 1;
-    Runtime& R = rt();
-    const int N0 = SP->n;
-    if (N0 > NK_NMAX || N0 < 3) return bqb_bound_nodes(nodes, count, rank, 16, nullptr, bounds);
-    FusedState& F = fstate();
-    std::lock_guard<std::mutex> lock(F.mu);
-    if (!F.stream) BQB_CUDA(cudaStreamCreateWithFlags(&F.stream, cudaStreamNonBlocking));
-    cudaStream_t s = F.stream;
-    const int N = N0 - 1;
-
-    FusedCfg c;
     memset(&c, 0, sizeof c);
     c.N0 = N0;
     c.count = count;
@@ -115,7 +111,7 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     c.include_Pent = params.include_Pent;
     c.include_Hepta = params.include_Hepta;
     c.use_diff = params.use_diff;
-    c.seed = F.seed + 0x9E3779B97F4A7C15ull * (++F.calls);
+    c.seed = seed;
     c.bcap = 64;
     int mt = 8 * (params.TriIneq > 0 ? params.TriIneq : 1);
     if (mt < 8192) mt = 8192;
@@ -127,124 +123,149 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     const int pc = params.Pent_Trials > 0 ? 3 * params.Pent_Trials : 0;
     const int hc = params.Hepta_Trials > 0 ? 4 * params.Hepta_Trials : 0;
     c.sa_chains = pc > hc ? pc : hc;
-    c.smem_bytes = nk_smem_bytes(N0, params.TriIneq, c.bcap, R.smem_optin);
-    if (c.smem_bytes > R.smem_optin) return bqb_bound_nodes(nodes, count, rank, 16, nullptr, bounds);
+    c.smem_bytes = nk_smem_bytes(N0, params.TriIneq, c.bcap, smem_optin);
+}
+
+bool fused_supported(int N0, size_t smem_optin)
+{
+    if (N0 > NK_NMAX || N0 < 3) return false;
+    FusedCfg c;
+    fill_cfg(c, N0, 1, 1, 0, smem_optin);
+    return c.smem_bytes <= smem_optin;
+}
+
+// Launch a batch on pipe P (the caller holds F.mu).
+void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int rank)
+{
+    Runtime& R = rt();
+    const int N0 = SP->n;
+    const int N = N0 - 1;
+    if (!P.stream) {
+        BQB_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+        BQB_CUDA(cudaEventCreate(&P.ev0));
+        BQB_CUDA(cudaEventCreate(&P.ev1));
+    }
+    cudaStream_t s = P.stream;
+    FusedCfg c;
+    fill_cfg(c, N0, count, rank, F.seed + 0x9E3779B97F4A7C15ull * (F.next_ticket + 1), R.smem_optin);
     const size_t slot_bytes = nk_layout(c);
     int slots = R.num_sms;
     if (slots > count) slots = count;
 
-    // problem and node data
     const unsigned gen = g_sp_generation.load();
     if (F.P0L_src != SP->L || F.P0N != N0 || F.P0L_gen != gen) {
+        // every pipe reads P0L: let the launches in flight finish first
+        for (int q = 0; q < NK_PIPES; ++q)
+            if (F.pipe[q].busy) BQB_CUDA(cudaStreamSynchronize(F.pipe[q].stream));
         F.P0L.ensure((size_t)N0 * N0);
-        BQB_CUDA(cudaMemcpyAsync(F.P0L.p, SP->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaMemcpy(F.P0L.p, SP->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice));
         F.P0L_src = SP->L;
         F.P0N = N0;
         F.P0L_gen = gen;
     }
+    if (!F.prof.p) {
+        F.prof.ensure(NKP_COUNT);
+        BQB_CUDA(cudaMemset(F.prof.p, 0, NKP_COUNT * sizeof(unsigned long long)));
+    }
     const size_t cN = (size_t)count * N;
-    int* hf = F.hfix.ensure(2 * cN);
+    int* hf = P.hfix.ensure(2 * cN);
+    std::vector<int> ord(count), nfree(count);
     for (int i = 0; i < count; ++i) {
         memcpy(hf + (size_t)i * N, nodes[i].xfixed, N * sizeof(int));
         memcpy(hf + cN + (size_t)i * N, nodes[i].sol.X, N * sizeof(int));
+        int nf = 0;
+        for (int j = 0; j < N; ++j) nf += nodes[i].xfixed[j] ? 0 : 1;
+        nfree[i] = nf;
+        ord[i] = i;
     }
     // heaviest nodes first (longest-processing-time order): a node's work
-    // grows with its subproblem size, so free vertices decide the order
-    {
-        std::vector<int> ord(count);
-        std::vector<int> nfree(count);
-        for (int i = 0; i < count; ++i) {
-            ord[i] = i;
-            int nf = 0;
-            for (int j = 0; j < N; ++j) nf += nodes[i].xfixed[j] ? 0 : 1;
-            nfree[i] = nf;
-        }
-        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return nfree[a] > nfree[b]; });
-        int* ho = F.hord.ensure(count);
-        memcpy(ho, ord.data(), count * sizeof(int));
-        F.order.ensure(count);
-        BQB_CUDA(cudaMemcpyAsync(F.order.p, ho, count * sizeof(int), cudaMemcpyHostToDevice, s));
-    }
-    F.xf.ensure(cN);
-    F.sx.ensure(cN);
-    BQB_CUDA(cudaMemcpyAsync(F.xf.p, hf, cN * sizeof(int), cudaMemcpyHostToDevice, s));
-    BQB_CUDA(cudaMemcpyAsync(F.sx.p, hf + cN, cN * sizeof(int), cudaMemcpyHostToDevice, s));
-    F.bound.ensure(count);
-    F.fracsol.ensure(cN);
-    F.hval.ensure(count);
-    F.hsol.ensure(cN);
-    F.status.ensure(count);
-    F.node_ns.ensure(count);
-    F.next.ensure(1);
-    F.lb.ensure(1);
-    F.arena.ensure(slot_bytes * slots);
-    BQB_CUDA(cudaMemsetAsync(F.next.p, 0, sizeof(int), s));
-    const unsigned long long lb0 = host_ordered(Bab_LBGet());
-    BQB_CUDA(cudaMemcpyAsync(F.lb.p, &lb0, sizeof lb0, cudaMemcpyHostToDevice, s));
+    // grows with its subproblem size
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return nfree[a] > nfree[b]; });
+    int* ho = P.hord.ensure(count);
+    memcpy(ho, ord.data(), count * sizeof(int));
+    P.xf.ensure(cN);
+    P.sx.ensure(cN);
+    P.order.ensure(count);
+    P.bound.ensure(count);
+    P.fracsol.ensure(cN);
+    P.hval.ensure(count);
+    P.hsol.ensure(cN);
+    P.status.ensure(count);
+    P.node_ns.ensure(count);
+    P.next.ensure(1);
+    P.lb.ensure(1);
+    P.arena.ensure(slot_bytes * slots);
+    unsigned long long* hlb = P.hlb.ensure(1);
+    hlb[0] = host_ordered(Bab_LBGet());
+    BQB_CUDA(cudaMemcpyAsync(P.xf.p, hf, cN * sizeof(int), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(P.sx.p, hf + cN, cN * sizeof(int), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(P.order.p, ho, count * sizeof(int), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(P.lb.p, hlb, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemsetAsync(P.next.p, 0, sizeof(int), s));
     c.P0L = F.P0L.p;
-    c.xfixed = F.xf.p;
-    c.solx = F.sx.p;
-    c.bound = F.bound.p;
-    c.fracsol = F.fracsol.p;
-    c.hval = F.hval.p;
-    c.hsol = F.hsol.p;
-    c.status = F.status.p;
-    c.node_ns = F.node_ns.p;
-    c.order = F.order.p;
-    c.next = F.next.p;
-    c.lb = F.lb.p;
+    c.xfixed = P.xf.p;
+    c.solx = P.sx.p;
+    c.bound = P.bound.p;
+    c.fracsol = P.fracsol.p;
+    c.hval = P.hval.p;
+    c.hsol = P.hsol.p;
+    c.status = P.status.p;
+    c.node_ns = P.node_ns.p;
+    c.order = P.order.p;
+    c.next = P.next.p;
+    c.lb = P.lb.p;
     c.ipm_stats = ipm_stats_device();
-    if (!F.prof.p) {
-        F.prof.ensure(NKP_COUNT);
-        BQB_CUDA(cudaMemsetAsync(F.prof.p, 0, NKP_COUNT * sizeof(unsigned long long), s));
-    }
     c.prof = F.prof.p;
-    c.arena = F.arena.p;
-    if (!F.ev0) {
-        BQB_CUDA(cudaEventCreate(&F.ev0));
-        BQB_CUDA(cudaEventCreate(&F.ev1));
-    }
-    BQB_CUDA(cudaEventRecord(F.ev0, s));
+    c.arena = P.arena.p;
+    BQB_CUDA(cudaEventRecord(P.ev0, s));
     nk_launch(c, slots, s);
-    BQB_CUDA(cudaEventRecord(F.ev1, s));
+    BQB_CUDA(cudaEventRecord(P.ev1, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hb.ensure(count), P.bound.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hfs.ensure(cN), P.fracsol.p, cN * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hhv.ensure(count), P.hval.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hhs.ensure(cN), P.hsol.p, cN * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hst.ensure(count), P.status.p, count * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(P.hns.ensure(count), P.node_ns.p, count * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, s));
+    P.busy = true;
+    P.count = count;
+    P.rank = rank;
+    P.N = N;
+    P.ticket = F.next_ticket++;
+}
 
-    double* hb = F.hb.ensure(count);
-    double* hfs = F.hfs.ensure(cN);
-    double* hhv = F.hhv.ensure(count);
-    int* hhs = F.hhs.ensure(cN);
-    int* hst = F.hst.ensure(count);
-    BQB_CUDA(cudaMemcpyAsync(hb, F.bound.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
-    BQB_CUDA(cudaMemcpyAsync(hfs, F.fracsol.p, cN * sizeof(double), cudaMemcpyDeviceToHost, s));
-    BQB_CUDA(cudaMemcpyAsync(hhv, F.hval.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
-    BQB_CUDA(cudaMemcpyAsync(hhs, F.hsol.p, cN * sizeof(int), cudaMemcpyDeviceToHost, s));
-    BQB_CUDA(cudaMemcpyAsync(hst, F.status.p, count * sizeof(int), cudaMemcpyDeviceToHost, s));
-    unsigned long long* hns = F.hns.ensure(count);
-    BQB_CUDA(cudaMemcpyAsync(hns, F.node_ns.p, count * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+// Wait for pipe P and hand its results to the caller's nodes (the caller
+// holds F.mu).
+int collect(FusedState& F, FusedPipe& P, BabNode* nodes, double* bounds)
+{
+    cudaStream_t s = P.stream;
     BQB_CUDA(cudaStreamSynchronize(s));
-    F.last_node_ms.assign(count, 0.0);
-    for (int i = 0; i < count; ++i) F.last_node_ms[i] = 1e-6 * (double)hns[i];
+    P.busy = false;
+    const int count = P.count, N = P.N;
     float kms = 0.f;
-    BQB_CUDA(cudaEventElapsedTime(&kms, F.ev0, F.ev1));
+    BQB_CUDA(cudaEventElapsedTime(&kms, P.ev0, P.ev1));
     F.st_calls += 1;
     F.st_nodes += count;
     F.st_kernel_ms += kms;
+    F.last_node_ms.assign(count, 0.0);
+    for (int i = 0; i < count; ++i) F.last_node_ms[i] = 1e-6 * (double)P.hns.p[i];
 
     std::vector<int> redo;
     for (int i = 0; i < count; ++i) {
-        if (hst[i]) {
+        if (P.hst.p[i]) {
             redo.push_back(i);
             continue;
         }
-        bounds[i] = hb[i];
-        memcpy(nodes[i].fracsol, hfs + (size_t)i * N, N * sizeof(double));
+        bounds[i] = P.hb.p[i];
+        memcpy(nodes[i].fracsol, P.hfs.p + (size_t)i * N, N * sizeof(double));
     }
     // incumbent updates in node order (updateSolution's test and update)
     for (int i = 0; i < count; ++i) {
-        if (!(hhv[i] > Bab_LBGet())) continue;
+        if (!(P.hhv.p[i] > Bab_LBGet())) continue;
         BabSolution bs;
         memset(&bs, 0, sizeof bs);
-        memcpy(bs.X, hhs + (size_t)i * N, N * sizeof(int));
-        Bab_LBUpd(hhv[i], &bs);
+        memcpy(bs.X, P.hhs.p + (size_t)i * N, N * sizeof(int));
+        Bab_LBUpd(P.hhv.p[i], &bs);
     }
     if (!redo.empty()) {
         F.fallbacks += (long long)redo.size();
@@ -252,12 +273,12 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
         std::vector<double> sb(redo.size());
         for (size_t q = 0; q < redo.size(); ++q) sub[q] = nodes[redo[q]];
         const int th = redo.size() < 16 ? (int)redo.size() : 16;
-        BQB_CUDA(cudaEventRecord(F.ev0, s));
-        const int rc = bqb_bound_nodes(sub.data(), (int)sub.size(), rank, th, nullptr, sb.data());
-        BQB_CUDA(cudaEventRecord(F.ev1, s));
-        BQB_CUDA(cudaEventSynchronize(F.ev1));
+        BQB_CUDA(cudaEventRecord(P.ev0, s));
+        const int rc = bqb_bound_nodes(sub.data(), (int)sub.size(), P.rank, th, nullptr, sb.data());
+        BQB_CUDA(cudaEventRecord(P.ev1, s));
+        BQB_CUDA(cudaEventSynchronize(P.ev1));
         float fms = 0.f;
-        BQB_CUDA(cudaEventElapsedTime(&fms, F.ev0, F.ev1));
+        BQB_CUDA(cudaEventElapsedTime(&fms, P.ev0, P.ev1));
         F.st_fallback_nodes += (double)redo.size();
         F.st_fallback_ms += fms;
         if (rc) return rc;
@@ -269,13 +290,60 @@ BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* b
     return 0;
 }
 
+}  // namespace
+}  // namespace bqb
+
+using namespace bqb;
+
+// Start bounding `count` nodes (see include/bqb_gpu.h).
+BQB_API long long bqb_fused_submit(const BabNode* nodes, int count, int rank)
+{
+    if (count <= 0) return -4;
+    if (!SP || !SP->L) return -2;
+    Runtime& R = rt();
+    if (!fused_supported(SP->n, R.smem_optin)) return -3;
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    for (int q = 0; q < NK_PIPES; ++q) {
+        FusedPipe& P = F.pipe[(F.next_ticket + q) % NK_PIPES];
+        if (P.busy) continue;
+        submit(F, P, nodes, count, rank);
+        return (long long)P.ticket;
+    }
+    set_error("bqb_fused_submit", "every pipe holds an uncollected submission");
+    return -1;
+}
+
+// Wait for a submission and fill bounds[i] and nodes[i].fracsol.
+BQB_API int bqb_fused_collect(long long ticket, BabNode* nodes, double* bounds)
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    for (int q = 0; q < NK_PIPES; ++q) {
+        FusedPipe& P = F.pipe[q];
+        if (P.busy && (long long)P.ticket == ticket) return collect(F, P, nodes, bounds);
+    }
+    set_error("bqb_fused_collect", "unknown or already collected ticket");
+    return 1;
+}
+
+// Fused bounding of `count` nodes, collected before returning.
+BQB_API int bqb_bound_nodes_fused(BabNode* nodes, int count, int rank, double* bounds)
+{
+    if (count <= 0) return 0;
+    if (!SP || !SP->L) return 1;
+    if (!fused_supported(SP->n, rt().smem_optin)) return bqb_bound_nodes(nodes, count, rank, 16, nullptr, bounds);
+    const long long t = bqb_fused_submit(nodes, count, rank);
+    if (t < 0) return t == -1 ? 2 : 1;
+    return bqb_fused_collect(t, nodes, bounds);
+}
+
 // Nodes the fused kernel handed back to an engine since the process started.
 BQB_API long long bqb_fused_fallbacks(void) { return fstate().fallbacks; }
 
-// out[5] = {calls, nodes, fused kernel ms, nodes bounded again by engines,
-// their ms} since the last reset (CUDA events on the fused stream; the
-// fallback interval brackets the engines' work from that stream, which the
-// engines synchronise before returning).
+// out[5] = {collected submissions, nodes, fused kernel ms (summed over
+// submissions; overlapping launches each count their own time), nodes
+// bounded again by engines, their ms} since the last reset.
 BQB_API void bqb_fused_stats(double* out)
 {
     FusedState& F = fstate();
@@ -287,8 +355,8 @@ BQB_API void bqb_fused_stats(double* out)
     out[4] = F.st_fallback_ms;
 }
 
-// Device milliseconds of every node of the last bqb_bound_nodes_fused call
-// (as many as that call had, at most `count`); returns how many were written.
+// Device milliseconds of every node of the last collected submission (as
+// many as it had, at most `count`); returns how many were written.
 BQB_API int bqb_fused_node_times(double* out, int count)
 {
     FusedState& F = fstate();

@@ -90,3 +90,25 @@ def test_fused_bounds_with_kgon_separation(lib, solved):
                 assert O.evaluateSolution(SPL, x) <= b[i] + 1e-6
     finally:
         _lib.set_params(lib, _lib.make_params(include_Pent=0, include_Hepta=0))
+
+
+@pytest.mark.gpu
+def test_fused_submit_collect_pipelined(lib, solved):
+    """Eight batches in flight give the same bounds as one batch at a time
+    (the incumbent is the optimum, so no batch can change another's)."""
+    batches = [_nodes(20, 30, seed=40 + q) for q in range(8)]
+    singles = []
+    for b in batches:
+        c = _copy(b)
+        out = np.zeros(len(c))
+        assert lib.bqb_bound_nodes_fused(c, len(c), 1, _lib.dptr(out)) == 0
+        singles.append(out)
+    outs = [np.zeros(len(b)) for b in batches]
+    tickets = [lib.bqb_fused_submit(b, len(b), 1) for b in batches]
+    assert all(t >= 0 for t in tickets)
+    assert lib.bqb_fused_submit(batches[0], len(batches[0]), 1) == -1   # every pipe busy
+    for t, b, o in zip(reversed(tickets), reversed(batches), reversed(outs)):
+        assert lib.bqb_fused_collect(t, b, _lib.dptr(o)) == 0
+    assert lib.bqb_fused_collect(tickets[0], batches[0], _lib.dptr(outs[0])) == 1   # already collected
+    for o, s in zip(outs, singles):
+        np.testing.assert_array_equal(o, s)
