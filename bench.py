@@ -66,6 +66,16 @@ WORKLOAD = "G(100,0.5) ±1 weights; 512 subproblems, k~U[0,40] fixed (n=60..100)
 FLOP_PER_ITER_N3 = 6.0
 
 
+# Time-to-optimality instance: the batched configuration's graph itself,
+# G(100, 0.5) with +-1 weights (seed 1), solved from scratch to optimality
+# with the shipped parameters.
+TTO_NAME = "G(100,0.5) +-1 weights, seed 1, full B&B, shipped params"
+
+
+def tto_instance():
+    return np.ascontiguousarray(instances.gnp_pm1(NV, 0.5, seed=1))
+
+
 def workload():
     A = instances.gnp_pm1(NV, 0.5, seed=1)
     subs = instances.random_fixings(NV, N_SUB, KMAX, seed=2)
@@ -179,6 +189,21 @@ class GpuArm:
         self.nodes = [make_node(xf, sol) for xf, sol in self.subs]
         self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
         torch.cuda.synchronize()
+
+    def lib_sms(self) -> int:
+        import torch
+        return torch.cuda.get_device_properties(self.device).multi_processor_count
+
+    def reset_problem(self):
+        """Set the bench workload's problem up again (after a solver run)."""
+        lib = self.lib
+        _lib.set_params(lib, _lib.make_params(**workload_params()))
+        lib.process_adj_matrix(_lib.dptr(self.A.copy()), self.N0)
+        self.glob = _lib.GlobalArrays(lib, self.N0)
+        C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(self.babsol)
+        self.SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+        self.PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
+        self.PP_L_host = C.cast(self.PP.contents.L, C.c_void_p).value
 
     def node_array(self, idx):
         arr = (_lib.BabNode * len(idx))()
@@ -368,6 +393,25 @@ def run_gpu(args):
         drop = {"value": len(idx) / (d0.elapsed_time(d1) / 1e3), "unit": "nodes/s",
                 "nodes": len(idx), "call": "Evaluate(node, SP, PP, 1), host buffers, serial"}
 
+    # ---- time to optimality: fused batches vs the plain drop-in ----
+    tto = None
+    if args.tto and rank == 0:
+        A = tto_instance()
+        t0 = time.perf_counter()
+        rf = _lib.solve(A, fused_batch=2 * arm.lib_sms(), fused_depth=4)
+        t_f = time.perf_counter() - t0
+        tto = {"instance": TTO_NAME, "fused": {"seconds": t_f, "optimum": rf["best_value"], "nodes": rf["nodes"],
+                                               "call": "bqb_solve_fused (batches of 2 x SMs, 4 in flight)"}}
+        if args.tto_plain:
+            t0 = time.perf_counter()
+            rp = _lib.solve(A)
+            t_p = time.perf_counter() - t0
+            tto["plain_dropin"] = {"seconds": t_p, "optimum": rp["best_value"], "nodes": rp["nodes"],
+                                   "call": "bqb_solve (serial best-first, one node at a time)"}
+            tto["speedup_vs_plain"] = t_p / t_f
+        # restore the bench's problem (the solver set up its own)
+        arm.reset_problem()
+
     pk = peaks()
     kernel_ms = fst[2]
     flops = FLOP_PER_ITER_N3 * stats[0]
@@ -413,6 +457,7 @@ def run_gpu(args):
                     "call": "bqb_fused_submit/collect with host node structs"},
             "engines": eng,
             "dropin_serial": drop,
+            "time_to_optimality": tto,
             "gpu_launches": int(launches),
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -472,6 +517,25 @@ class RefPool:
             c.send(idx)
         return [c.recv()[1] for c in self.conns]
 
+    def run_dynamic(self, indices):
+        """Hand the nodes out one at a time to whichever process is idle (as
+        the reference's MPI master hands open nodes to free workers)."""
+        from multiprocessing.connection import wait
+        todo = list(indices)
+        busy = {}
+        for c in self.conns:
+            if not todo:
+                break
+            c.send([todo.pop(0)])
+            busy[c] = True
+        while busy:
+            for c in wait(list(busy)):
+                c.recv()
+                del busy[c]
+                if todo:
+                    c.send([todo.pop(0)])
+                    busy[c] = True
+
     def close(self):
         for c in self.conns:
             c.send(None)
@@ -508,31 +572,47 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources)"}))
         return
     P = max(1, min(os.cpu_count() or 1, args.ref_procs))
-    per = max(1, args.ref_nodes_per_proc)
+    B = max(1, args.ref_nodes_per_step)
     pool = RefPool(P)
-    step = 0
-
-    def assign(s):
-        base = s * P * per
-        return [[((base + w * per + q) * 7919) % N_SUB for q in range(per)] for w in range(P)]
-
-    for _ in range(args.warmup):
-        pool.run(assign(step))
-        step += 1
+    # the GPU arm's node order; warm-up and timed steps are B nodes each, the
+    # timed steps handed out as one stream (nodes of the next step start as
+    # soon as a process is free, as the GPU arm's pipelined launches do)
+    order = [(i * 7919) % N_SUB for i in range(B * (args.warmup + args.steps))]
+    pool.run_dynamic(order[:B * args.warmup])
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        pool.run(assign(step))
-        step += 1
+    pool.run_dynamic(order[B * args.warmup:])
     wall = time.perf_counter() - t0
     pool.close()
-    nodes = P * per * args.steps
+    nodes = B * args.steps
     v = nodes / wall
+    tto = None
+    if args.tto:
+        import tempfile
+        A = tto_instance()
+        with tempfile.TemporaryDirectory() as td:
+            inst, prm = os.path.join(td, "g.rudy"), os.path.join(td, "params")
+            instances.write_rudy(inst, A)
+            instances.write_params(prm, _lib.PARAMS_FILE)
+            env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
+            t0 = time.perf_counter()
+            outp = subprocess.run([refbind.REF_BAB, inst, prm], capture_output=True, text=True, env=env,
+                                  timeout=1800).stdout
+            t_r = time.perf_counter() - t0
+        import re
+        mv = re.search(r"Maximum value = (\S+)", outp)
+        mn = re.search(r"Nodes = (\d+)", outp)
+        tto = {"instance": TTO_NAME, "reference_serial": {
+            "seconds": t_r, "optimum": float(mv.group(1)) if mv else None, "nodes": int(mn.group(1)) if mn else None,
+            "call": "the reference's serial best-first B&B (oracle/_ref/bqb_ref_bab), 1 core, OpenBLAS 1 thread"}}
     line = {"metric": METRIC, "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "nodes_per_step": P * per, "processes": P},
+            "time_to_optimality": tto,
+            "config": {"workload": WORKLOAD, "nodes_per_step": B, "processes": P,
+                       "dispatch": "dynamic: one node at a time to the next idle process, steps back to back"},
             "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": P, "kind": "reference",
-                             "sample": f"{P * per} subproblems per step ({per} per process), {P} processes"},
+                             "sample": f"{B} subproblems per step, {args.steps} steps, {P} processes "
+                                       f"(the reference's Evaluate, OpenBLAS 1 thread each)"},
             "e2e": {"value": v, "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -546,6 +626,10 @@ def main():
     ap.add_argument("--nodes-per-step", type=int, default=512)
     ap.add_argument("--threads", type=int, default=32, help="concurrent bounding engines per GPU")
     ap.add_argument("--depth", type=int, default=8, help="fused launches in flight (1..8)")
+    ap.add_argument("--no-tto", dest="tto", action="store_false",
+                    help="skip the time-to-optimality run")
+    ap.add_argument("--tto-plain", action="store_true",
+                    help="also time the plain drop-in solver to optimality (about 40 s)")
     ap.add_argument("--engine-nodes", type=int, default=128,
                     help="nodes timed through the concurrent engines (0: skip)")
     ap.add_argument("--dropin-nodes", type=int, default=16,
@@ -553,7 +637,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=64)
-    ap.add_argument("--ref-nodes-per-proc", type=int, default=1)
+    ap.add_argument("--ref-nodes-per-step", type=int, default=256,
+                    help="subproblems per step of the reference arm (bounded CPU sample)")
     args = ap.parse_args()
     faulthandler.enable(all_threads=True)
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")

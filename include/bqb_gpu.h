@@ -221,6 +221,19 @@ int bqb_solve(const double *adj, int num_vertices, const BiqBinParameters *prm, 
 int bqb_solve_parallel(const double *adj, int num_vertices, const BiqBinParameters *prm, int threads,
                        bqb_solve_result *out);
 
+/* The same B&B with the nodes bounded in batches by the fused node kernel
+ * (bqb_fused_submit / bqb_fused_collect): after the root (rank 0, library
+ * globals), batches of at most `batch` open nodes with the largest parent
+ * bounds, up to `depth` (<= 8) batches in flight, every node bounded with
+ * rank 1 and branched as the reference's workers branch
+ * (src/bab_functions.c:224-336).  Children are queued with their parent's
+ * bound as priority; a node whose parent bound no longer exceeds the
+ * incumbent by more than 1 is pruned unbounded.  Problems above 128
+ * vertices go to bqb_solve_parallel.  Returns 0, 1 on bad input, 2 when a
+ * submission fails. */
+int bqb_solve_fused(const double *adj, int num_vertices, const BiqBinParameters *prm, int batch, int depth,
+                    bqb_solve_result *out);
+
 /* Bound `count` independent nodes of the problem set up by
  * process_adj_matrix (SP) with `threads` concurrent engines: bounds[i] is
  * SDPbound(nodes[i], SP, <engine subproblem>, rank) (src/bounding.c:24-342)

@@ -109,6 +109,7 @@ SIGNATURES = {
     "bqb_read_params": (C.c_int, [C.c_char_p, C.POINTER(Params)]),
     "bqb_solve": (C.c_int, [D, C.c_int, C.c_void_p, C.c_void_p]),
     "bqb_solve_parallel": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "bqb_solve_fused": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "bqb_bound_nodes": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_void_p), D]),
     "bqb_bound_nodes_fused": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, D]),
@@ -204,16 +205,21 @@ def make_params(**overrides) -> Params:
     return p
 
 
-def solve(adj: np.ndarray, threads: int = 1, **param_overrides) -> dict:
+def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: int = 4,
+          **param_overrides) -> dict:
     """Solve Max-Cut on ``adj`` to optimality (best-first B&B, GPU bounding;
-    ``threads`` > 1 bounds that many nodes concurrently)."""
+    ``threads`` > 1 bounds that many nodes concurrently on engines;
+    ``fused_batch`` > 0 bounds batches of up to that many nodes with the
+    fused node kernel, ``fused_depth`` batches in flight)."""
     lib = load()
     A = np.ascontiguousarray(adj, dtype=np.float64)
     p = make_params(**param_overrides)
     res = SolveResult()
     pp = C.cast(C.pointer(p), C.c_void_p)
     rp = C.cast(C.pointer(res), C.c_void_p)
-    if threads > 1:
+    if fused_batch > 0:
+        rc = lib.bqb_solve_fused(dptr(A), A.shape[0], pp, int(fused_batch), int(fused_depth), rp)
+    elif threads > 1:
         rc = lib.bqb_solve_parallel(dptr(A), A.shape[0], pp, int(threads), rp)
     else:
         rc = lib.bqb_solve(dptr(A), A.shape[0], pp, rp)

@@ -654,3 +654,116 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
     }
     return 0;
 }
+
+// ---- B&B with fused batches ------------------------------------------------
+extern "C" {
+long long bqb_fused_submit(const BabNode* nodes, int count, int rank);
+int bqb_fused_collect(long long ticket, BabNode* nodes, double* bounds);
+}
+
+// Best-first B&B whose nodes are bounded in batches by the fused node kernel
+// (bqb_fused_submit / bqb_fused_collect), up to `depth` batches in flight.
+// The root is bounded first with rank 0 on the library globals (sets diff);
+// then batches of at most `batch` open nodes with the largest parent bounds
+// are bounded with rank 1, and every node whose bound exceeds the incumbent
+// by more than 1 is branched (src/bab_functions.c:224-336).  A child is
+// queued with its parent's bound as priority, and a node whose parent bound
+// no longer exceeds the incumbent by more than 1 is pruned without being
+// bounded (the parent bound is a valid bound of the child).  Problems the
+// fused kernel does not take (N0 > 128) go to bqb_solve_parallel.
+BQB_API int bqb_solve_fused(const double* adj, int num_vertices, const BiqBinParameters* prm, int batch, int depth,
+                            bqb_solve_result* out)
+{
+    if (num_vertices < 3 || num_vertices > BQB_NMAX) return 1;
+    if (num_vertices > 128) return bqb_solve_parallel(adj, num_vertices, prm, 16, out);
+    if (batch < 1) batch = 1;
+    if (depth < 1) depth = 1;
+    if (depth > 8) depth = 8;
+    if (prm) {
+        params = *prm;
+    } else {
+        bqb_default_params(&params);
+        params.init_bundle_iter = 5;
+        params.violated_TriIneq = 0.05;
+    }
+    std::vector<double> A(adj, adj + (size_t)num_vertices * num_vertices);
+    process_adj_matrix(A.data(), num_vertices);
+    if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
+    srand(2020);
+    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
+    memset(BabSol, 0, sizeof(BabSolution));
+    g_LB.store(0.0);
+    g_num_nodes = 0;
+    stopped = 0;
+    diff = 0.0;
+    alloc_globals(SP->n);
+
+    TIME = wtime();
+    NodeHeap heap;
+    BabNode* root = new_node(nullptr);
+    ++g_num_nodes;
+    root_bound = Evaluate(root, SP, PP, 0);
+    root->upper_bound = root_bound;
+    auto branch = [&](const BabNode* node, double bound) {
+        const int ic = getBranchingVariable(const_cast<BabNode*>(node));
+        for (int xic = 0; xic <= 1; ++xic) {
+            BabNode* child = new_node(node);
+            child->xfixed[ic] = 1;
+            child->sol.X[ic] = xic;
+            child->upper_bound = bound;
+            ++g_num_nodes;
+            heap.push(child);
+        }
+    };
+    if (Bab_LBGet() + 1.0 < root->upper_bound && !params.root) branch(root, root->upper_bound);
+    free(root);
+
+    struct Flight {
+        long long ticket;
+        std::vector<BabNode> nodes;
+        std::vector<double> bounds;
+    };
+    std::vector<Flight> flight;
+    int rc = 0;
+    while (!heap.empty() || !flight.empty()) {
+        if (params.time_limit > 0 && (wtime() - TIME) > params.time_limit) stopped = 1;
+        while (!stopped && (int)flight.size() < depth && !heap.empty()) {
+            Flight f;
+            while ((int)f.nodes.size() < batch && !heap.empty()) {
+                BabNode* nd = heap.pop();
+                if (Bab_LBGet() + 1.0 < nd->upper_bound) f.nodes.push_back(*nd);
+                free(nd);
+            }
+            if (f.nodes.empty()) continue;
+            f.bounds.assign(f.nodes.size(), 0.0);
+            f.ticket = bqb_fused_submit(f.nodes.data(), (int)f.nodes.size(), 1);
+            if (f.ticket < 0) {
+                rc = 2;
+                break;
+            }
+            flight.push_back(std::move(f));
+        }
+        if (rc || flight.empty()) break;
+        Flight f = std::move(flight.front());
+        flight.erase(flight.begin());
+        rc = bqb_fused_collect(f.ticket, f.nodes.data(), f.bounds.data());
+        if (rc) break;
+        for (size_t i = 0; i < f.nodes.size(); ++i) {
+            f.nodes[i].upper_bound = f.bounds[i];
+            if (!stopped && Bab_LBGet() + 1.0 < f.bounds[i]) branch(&f.nodes[i], f.bounds[i]);
+        }
+    }
+    while (!heap.empty()) free(heap.pop());
+    for (Flight& f : flight) bqb_fused_collect(f.ticket, f.nodes.data(), f.bounds.data());
+
+    if (out) {
+        out->best_value = Bab_LBGet();
+        out->root_bound = root_bound;
+        out->nodes = g_num_nodes;
+        out->stopped = stopped;
+        out->seconds = wtime() - TIME;
+        out->num_vertices = num_vertices;
+        for (int i = 0; i < BQB_NMAX; ++i) out->solution[i] = (i < BabPbSize) ? BabSol->X[i] : 0;
+    }
+    return rc;
+}

@@ -112,3 +112,20 @@ def test_fused_submit_collect_pipelined(lib, solved):
     assert lib.bqb_fused_collect(tickets[0], batches[0], _lib.dptr(outs[0])) == 1   # already collected
     for o, s in zip(outs, singles):
         np.testing.assert_array_equal(o, s)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,nv,seed", [("unit", 60, 2), ("pm1", 50, 4), ("qubo", 40, 6)])
+def test_fused_solve_optimum(lib, kind, nv, seed):
+    """B&B with fused batches reaches the serial solver's optimum."""
+    if kind == "unit":
+        A = instances.gnp_unit(nv, 0.5, seed)
+    elif kind == "pm1":
+        A = instances.gnp_pm1(nv, 0.5, seed)
+    else:
+        A = instances.qubo_to_maxcut(instances.qubo_dense(nv, 0.1, seed))
+    serial = _lib.solve(A)
+    fused = _lib.solve(A, fused_batch=64, fused_depth=4)
+    assert fused["best_value"] == serial["best_value"]
+    assert fused["root_bound"] == serial["root_bound"]
+    assert O.evaluateSolution(O.build_SP_L(A), fused["x"]) == fused["best_value"]
