@@ -64,6 +64,9 @@ WORKLOAD = "G(100,0.5) ±1 weights; 512 subproblems, k~U[0,40] fixed (n=60..100)
 # Cholesky factorizations 2n^3/3): 6.0 n^3; the reference's count with its
 # second POSV is 6.33 n^3.  The smaller count is used.
 FLOP_PER_ITER_N3 = 6.0
+# DRAM traffic of the fused kernel per node, measured with ncu on a small case
+# (16 nodes of a G(60, 0.5) +-1 instance: 1.39 MB in one launch).
+NODEK_DRAM_BYTES_PER_NODE = 1.39e6 / 16
 
 
 # Time-to-optimality instance: the batched configuration's graph itself,
@@ -418,7 +421,9 @@ def run_gpu(args):
     achieved = flops / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else 0.0
     peak = pk["bf16_tflops_sustained"]
     roof = {"kernel": "nodek_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": NODEK_DRAM_BYTES_PER_NODE * B,
+            "traffic_note": "DRAM bytes per launch: 87 KB per node from the ncu capture of a small case "
+                            "(profiles/nodek_kernel_G60_16nodes.md, n = 60) times the nodes of a launch",
             "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
                            f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
             "launches": int(fst[0]), "avg_launch_us": 1e3 * kernel_ms / max(fst[0], 1),

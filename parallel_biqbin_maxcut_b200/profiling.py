@@ -5,6 +5,10 @@
         `ncu --metrics gpu__time_duration.sum --csv --log-file ...` list
     python -m parallel_biqbin_maxcut_b200.profiling raw <report.csv>
         selected counters from `ncu -i report.ncu-rep --page raw --csv`
+    python -m parallel_biqbin_maxcut_b200.profiling ipm <n> <repeats>
+        bound the root of a G(n, 0.5) +-1 instance (IPM kernel case)
+    python -m parallel_biqbin_maxcut_b200.profiling fused <n> <count> <kmax>
+        bound `count` subproblems with the fused node kernel (nodek case)
 """
 from __future__ import annotations
 
@@ -95,10 +99,46 @@ def run_ipm(n_vertices: int, repeats: int) -> None:
         print(f"n={nv} phi={phi.value:.6f} wall={1e3 * (time.perf_counter() - t0):.3f} ms")
 
 
+def run_fused(n_vertices: int, count: int, kmax: int) -> None:
+    """Bound `count` subproblems (k ~ U[0, kmax] fixed vertices) of a seeded
+    G(n, 0.5) +-1 instance with the fused node kernel, once (a small,
+    self-contained case for profiling nodek_kernel)."""
+    import ctypes as C
+
+    import numpy as np
+
+    from . import _lib, instances
+
+    lib = _lib.load()
+    assert lib.bqb_init(0) == 0, lib.bqb_last_error()
+    A = np.ascontiguousarray(instances.gnp_pm1(n_vertices, 0.5, seed=1))
+    _lib.set_params(lib, _lib.make_params(adjust_TriIneq=0, TriIneq=3 * n_vertices))
+    lib.process_adj_matrix(_lib.dptr(A.copy()), n_vertices)
+    glob = _lib.GlobalArrays(lib, n_vertices)
+    sol = (C.c_int * _lib.NMAX)()
+    C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(sol)
+    SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+    PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
+    C.CDLL("libc.so.6").srand(2020)
+    root = _lib.BabNode()
+    rb = lib.Evaluate(C.byref(root), SP, PP, 0)
+    nodes = (_lib.BabNode * count)()
+    for q, (xf, sx) in enumerate(instances.random_fixings(n_vertices, count, kmax, seed=2)):
+        nodes[q].xfixed[: n_vertices - 1] = [int(v) for v in xf]
+        nodes[q].sol[: n_vertices - 1] = [int(v) for v in sx]
+    b = np.zeros(count)
+    assert lib.bqb_bound_nodes_fused(nodes, count, 1, _lib.dptr(b)) == 0, lib.bqb_last_error()
+    print(f"n={n_vertices} root={rb:.6f} nodes={count} mean_bound={b.mean():.6f} "
+          f"fallbacks={lib.bqb_fused_fallbacks()}")
+    del glob
+
+
 if __name__ == "__main__":
     mode = sys.argv[1]
     if mode == "ipm":
         run_ipm(int(sys.argv[2]), int(sys.argv[3]))
+    elif mode == "fused":
+        run_fused(int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]))
     else:
         path = sys.argv[2]
         print(summarize_launches(path) if mode == "launches" else summarize_raw(path))
