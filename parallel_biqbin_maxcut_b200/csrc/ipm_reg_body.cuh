@@ -49,7 +49,8 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
     double* dX = ws;
     double* dX1 = ws + nn;
     double* Zi = zi_in_smem ? F + nn : ws + 2 * nn;
-    double* cbuf = stage;   // 2 * RM_NMAX pivot-column buffers (the stage is idle then)
+    double* cbuf = stage;   // 2 * RM_BUF pivot-column buffers (the stage is idle then)
+    static_assert(CTA_KC * STG_LD >= 2 * RM_BUF, "pivot buffers exceed the GEMM stage");
 
     // ---- initial point (src/ipm_mc_pk.c:65-99) ----
     for (int c = tid; c < n; c += nt) {

@@ -67,71 +67,89 @@ __device__ __forceinline__ void rm_store_lower(const RegMat& M, double* A, int n
     }
 }
 
-// Publish column k (rows < n) into buf: done by the 32 owner threads.
-__device__ __forceinline__ void rm_publish_col(const RegMat& M, int n, int k, double* buf)
+// Pivot-column buffers of RM_BUF doubles: the column (zeros where the step
+// must not act) and the pivot at RM_NMAX.
+constexpr int RM_BUF = RM_NMAX + 2;
+
+// Owner warp of column k: publish rows r > k of column k (zeros elsewhere,
+// so the update needs no index tests) and the pivot.
+__device__ __forceinline__ void rm_publish_tail(const RegMat& M, int k, double* buf)
 {
     if ((threadIdx.x >> 5) != (k & 15)) return;
     const int kb = k >> 4;
+    double v[4];
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        if (b != kb) continue;
+    for (int a = 0; a < 4; ++a) v[a] = 0.0;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int r = rm_row(a);
-            if (r < n) buf[r] = M.m[a][b];
-        }
+    for (int b = 0; b < 8; ++b)
+        if (b == kb)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) v[a] = M.m[a][b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = rm_row(a);
+        buf[r] = r > k ? v[a] : 0.0;
+        if (r == k) buf[RM_NMAX] = v[a];
     }
 }
 
 // Cholesky A = L L^T (L in the lower triangle of M; the upper triangle is
-// left with symmetric leftovers).  col2: 2 * RM_NMAX doubles of shared
+// left with symmetric leftovers).  col2: 2 * RM_BUF doubles of shared
 // memory.  Returns false, uniformly, at the first non-positive pivot.
-// Step k: the owners publish column k unscaled (a_ik, with a_kk the pivot);
-// every thread applies A_ij -= a_ik a_jk / a_kk to its entries with i,j > k;
-// the owners turn their column into L_ik = a_ik / sqrt(a_kk).
+// Step k: the owners publish rows r > k of column k (zeros for r <= k, and
+// the padding rows hold zeros, so the update needs no index tests) and the
+// pivot a_kk; every thread applies A_ij -= (a_ik / a_kk) a_jk to its 32
+// entries (a no-op where either factor is zero); the owners turn their
+// column into L_ik = a_ik / sqrt(a_kk).
 __device__ __forceinline__ bool rm_potrf(RegMat& M, int n, double* col2)
 {
-    rm_publish_col(M, n, 0, col2);
+    (void)n;
+    rm_publish_tail(M, 0, col2);
     __syncthreads();
+    const int lane = threadIdx.x & 31, tc = threadIdx.x >> 5;
     for (int k = 0; k < n; ++k) {
-        const double* col = col2 + (k & 1) * RM_NMAX;
-        const double d = col[k];
+        const double* col = col2 + (k & 1) * RM_BUF;
+        const double d = col[RM_NMAX];
         if (!(d > 0.0)) return false;
-        const double inv = 1.0 / d;
-        const double rs = 1.0 / sqrt(d);
-        const int kb = k >> 4;
-        const bool owner = (threadIdx.x >> 5) == (k & 15);
+        const double rs = rsqrt(d);   // 1/sqrt(d); the pivots stay well conditioned here
+        const double inv = rs * rs;
         double cr[4], cc[8];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int r = rm_row(a);
-            cr[a] = (r > k && r < n) ? col[r] * inv : 0.0;
-        }
+        for (int a = 0; a < 4; ++a) cr[a] = col[lane + 32 * a] * inv;
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const int c = rm_col(b);
-            cc[b] = (c > k && c < n) ? col[c] : 0.0;
-        }
+        for (int b = 0; b < 8; ++b) cc[b] = col[tc + 16 * b];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 8; ++b) M.m[a][b] = fma(-cr[a], cc[b], M.m[a][b]);
-        if (owner) {
+        if (tc == (k & 15)) {
+            const int kb = k >> 4;
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                if (b != kb) continue;
+            for (int b = 0; b < 8; ++b)
+                if (b == kb)
 #pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const int r = rm_row(a);
-                    if (r > k) M.m[a][b] = col[r] * rs;
-                    else if (r == k) M.m[a][b] = d * rs;   // sqrt(d)
-                }
-            }
+                    for (int a = 0; a < 4; ++a) {
+                        const int r = lane + 32 * a;
+                        if (r > k) M.m[a][b] = col[r] * rs;
+                        else if (r == k) M.m[a][b] = d * rs;   // sqrt(d)
+                    }
         }
-        if (k + 1 < n) rm_publish_col(M, n, k + 1, col2 + ((k + 1) & 1) * RM_NMAX);
+        if (k + 1 < n) rm_publish_tail(M, k + 1, col2 + ((k + 1) & 1) * RM_BUF);
         __syncthreads();
     }
     return true;
+}
+
+// Owner warp of column k: publish the whole column (rows beyond n hold 0).
+__device__ __forceinline__ void rm_publish_full(const RegMat& M, int k, double* buf)
+{
+    if ((threadIdx.x >> 5) != (k & 15)) return;
+    const int kb = k >> 4;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+        if (b == kb)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) buf[rm_row(a)] = M.m[a][b];
 }
 
 // In-place inverse of a symmetric positive definite matrix (full storage),
@@ -139,43 +157,51 @@ __device__ __forceinline__ bool rm_potrf(RegMat& M, int n, double* col2)
 // c = A(:,k) before the step, A_ij -= c_i c_j / d (i,j != k),
 // A_ik = A_ki = c_i / d, A_kk = -1/d; the result is -inv(A), negated at the
 // end.  The pivots are the Schur complements of A, so a non-positive pivot
-// means "not positive definite" (returned uniformly).  The update uses the
-// product c_i c_j, which is the same for (i,j) and (j,i): the result is
-// exactly symmetric.
+// means "not positive definite" (returned uniformly).  Each thread scales
+// its eight column values by 1/d once and applies A_ij -= c_i (c_j / d) with
+// one FMA per entry; then the lane holding row k (one per warp) and the
+// owner warp of column k overwrite the pivot row and column.  (i,j) and
+// (j,i) round c_i (c_j / d) and c_j (c_i / d): symmetric up to the last bit.
 __device__ __forceinline__ bool rm_spd_inverse(RegMat& M, int n, double* col2)
 {
-    rm_publish_col(M, n, 0, col2);
+    rm_publish_full(M, 0, col2);
     __syncthreads();
+    const int lane = threadIdx.x & 31, tc = threadIdx.x >> 5;
     for (int k = 0; k < n; ++k) {
-        const double* col = col2 + (k & 1) * RM_NMAX;
+        const double* col = col2 + (k & 1) * RM_BUF;
         const double d = col[k];
         if (!(d > 0.0)) return false;
         const double inv = 1.0 / d;
-        double cr[4], cc[8];
+        double cr[4], sc[8];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int r = rm_row(a);
-            cr[a] = (r < n) ? col[r] : 0.0;
-        }
+        for (int a = 0; a < 4; ++a) cr[a] = col[lane + 32 * a];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const int c = rm_col(b);
-            cc[b] = (c < n) ? col[c] : 0.0;
-        }
+        for (int b = 0; b < 8; ++b) sc[b] = col[tc + 16 * b] * inv;   // c_j / d
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const int r = rm_row(a);
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const int c = rm_col(b);
-                double v = fma(-(cr[a] * cc[b]), inv, M.m[a][b]);
-                if (r == k) v = cc[b] * inv;
-                if (c == k) v = cr[a] * inv;
-                if (r == k && c == k) v = -inv;
-                M.m[a][b] = v;
+            for (int b = 0; b < 8; ++b) M.m[a][b] = fma(-cr[a], sc[b], M.m[a][b]);
+        // row k (one lane per warp): c_j / d
+        {
+            const bool rowk = lane == (k & 31);
+            const int ak = k >> 5;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const bool hit = rowk && a == ak;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) M.m[a][b] = hit ? sc[b] : M.m[a][b];
             }
         }
-        if (k + 1 < n) rm_publish_col(M, n, k + 1, col2 + ((k + 1) & 1) * RM_NMAX);
+        // column k (the owner warp): c_i / d, and -1/d on the diagonal
+        if (tc == (k & 15)) {
+            const int kb = k >> 4;
+#pragma unroll
+            for (int b = 0; b < 8; ++b)
+                if (b == kb)
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) M.m[a][b] = (lane + 32 * a == k) ? -inv : cr[a] * inv;
+        }
+        if (k + 1 < n) rm_publish_full(M, k + 1, col2 + ((k + 1) & 1) * RM_BUF);
         __syncthreads();
     }
 #pragma unroll
@@ -184,5 +210,4 @@ __device__ __forceinline__ bool rm_spd_inverse(RegMat& M, int n, double* col2)
         for (int b = 0; b < 8; ++b) M.m[a][b] = -M.m[a][b];
     return true;
 }
-
 }  // namespace bqb
