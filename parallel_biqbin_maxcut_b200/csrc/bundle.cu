@@ -118,7 +118,7 @@ void solve_lambda_launch(int k, const double* Q, const double* c, double* lambda
     static DevBuf<double> ws;
     double* w = ws.ensure((size_t)2 * k * k + 8 * (size_t)k + 8);
     size_t bytes = 2 * (size_t)k * sizeof(double);
-    if (k <= QP_SMEM_K) bytes += ((size_t)k * k + 5 * (size_t)k) * sizeof(double);
+    if (k <= QP_SMEM_K) bytes += ((size_t)k * k + 6 * (size_t)k) * sizeof(double);
     BQB_SMEM_LIMIT(solve_lambda_kernel, bytes);
     solve_lambda_kernel<<<1, 32, bytes, s>>>(k, Q, c, lambda, err, w);
     BQB_COUNT_LAUNCH();

@@ -20,7 +20,8 @@ __device__ __forceinline__ double Qat(const double* Q, int k, int a, int b)
 }
 
 // One warp.  Q: k x k (lower triangle read), c: k, lam: k (out).
-// ws: 2k*k... layout A[k*k], then vectors.  Returns false on a non-PD A.
+// ws: A[k*k], then six k-vectors (Q lambda, z, dlambda, u, w, and the
+// reciprocals of the factor's diagonal).  Returns false on a non-PD A.
 __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* lam, double* ws)
 {
     const int lane = threadIdx.x & 31;
@@ -30,6 +31,7 @@ __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* 
     double* dlam = z + k;
     double* u = dlam + k;
     double* w = u + k;
+    double* dinv = w + k;   // reciprocals of the factor's diagonal
 
     for (int b = lane; b < k; b += 32) lam[b] = 1.0 / k;
     __syncwarp();
@@ -79,14 +81,18 @@ __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* 
             w[a] = c[a] - y + Qlam[a];
         }
         __syncwarp();
-        // Cholesky of A
+        // Cholesky of A; one reciprocal square root per pivot, the column and
+        // the substitutions below multiply by it
         for (int j = 0; j < k; ++j) {
             const double d = A[j + (size_t)j * k];
             if (!(d > 0.0)) return false;
-            const double sq = sqrt(d);
+            const double rj = rsqrt(d);
             __syncwarp();
-            for (int i = j + 1 + lane; i < k; i += 32) A[i + (size_t)j * k] /= sq;
-            if (lane == 0) A[j + (size_t)j * k] = sq;
+            for (int i = j + 1 + lane; i < k; i += 32) A[i + (size_t)j * k] *= rj;
+            if (lane == 0) {
+                A[j + (size_t)j * k] = d * rj;
+                dinv[j] = rj;
+            }
             __syncwarp();
             for (int i = j + 1 + lane; i < k; i += 32) {
                 const double lij = A[i + (size_t)j * k];
@@ -96,8 +102,8 @@ __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* 
         }
         // forward and backward substitution for u and w together
         for (int j = 0; j < k; ++j) {
-            const double ljj = A[j + (size_t)j * k];
-            const double uj = u[j] / ljj, wj = w[j] / ljj;
+            const double rj = dinv[j];
+            const double uj = u[j] * rj, wj = w[j] * rj;
             __syncwarp();
             if (lane == 0) {
                 u[j] = uj;
@@ -111,8 +117,8 @@ __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* 
             __syncwarp();
         }
         for (int j = k - 1; j >= 0; --j) {
-            const double ljj = A[j + (size_t)j * k];
-            const double uj = u[j] / ljj, wj = w[j] / ljj;
+            const double rj = dinv[j];
+            const double uj = u[j] * rj, wj = w[j] * rj;
             __syncwarp();
             if (lane == 0) {
                 u[j] = uj;
@@ -497,7 +503,7 @@ __device__ inline void bundle_append_body(int* __restrict__ slot, int* __restric
 __host__ __device__ inline size_t le_smem_bytes(int k)
 {
     const size_t base = 3 * (size_t)k;
-    if (k <= QP_SMEM_K) return (base + (size_t)k * k + (size_t)k * k + 5 * (size_t)k) * sizeof(double);
+    if (k <= QP_SMEM_K) return (base + (size_t)k * k + (size_t)k * k + 6 * (size_t)k) * sizeof(double);
     return base * sizeof(double);
 }
 
