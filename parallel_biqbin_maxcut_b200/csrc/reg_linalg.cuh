@@ -158,8 +158,9 @@ __device__ __forceinline__ void rm_publish_full(const RegMat& M, int k, double* 
 // A_ik = A_ki = c_i / d, A_kk = -1/d; the result is -inv(A), negated at the
 // end.  The pivots are the Schur complements of A, so a non-positive pivot
 // means "not positive definite" (returned uniformly).  Each thread scales
-// its eight column values by 1/d once and applies A_ij -= c_i (c_j / d) with
-// one FMA per entry; then the lane holding row k (one per warp) and the
+// its eight column values by 1/d (= rsqrt(d)^2) once and applies
+// A_ij -= c_i (c_j / d) with one FMA per entry; then the lane holding row k
+// (one per warp, inside a warp-uniform branch on the row block) and the
 // owner warp of column k overwrite the pivot row and column.  (i,j) and
 // (j,i) round c_i (c_j / d) and c_j (c_i / d): symmetric up to the last bit.
 __device__ __forceinline__ bool rm_spd_inverse(RegMat& M, int n, double* col2)
@@ -171,7 +172,8 @@ __device__ __forceinline__ bool rm_spd_inverse(RegMat& M, int n, double* col2)
         const double* col = col2 + (k & 1) * RM_BUF;
         const double d = col[k];
         if (!(d > 0.0)) return false;
-        const double inv = 1.0 / d;
+        const double rq = rsqrt(d);
+        const double inv = rq * rq;   // 1/d
         double cr[4], sc[8];
 #pragma unroll
         for (int a = 0; a < 4; ++a) cr[a] = col[lane + 32 * a];
@@ -186,11 +188,10 @@ __device__ __forceinline__ bool rm_spd_inverse(RegMat& M, int n, double* col2)
             const bool rowk = lane == (k & 31);
             const int ak = k >> 5;
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const bool hit = rowk && a == ak;
+            for (int a = 0; a < 4; ++a)
+                if (a == ak)
 #pragma unroll
-                for (int b = 0; b < 8; ++b) M.m[a][b] = hit ? sc[b] : M.m[a][b];
-            }
+                    for (int b = 0; b < 8; ++b) M.m[a][b] = rowk ? sc[b] : M.m[a][b];
         }
         // column k (the owner warp): c_i / d, and -1/d on the diagonal
         if (tc == (k & 15)) {
