@@ -14,9 +14,12 @@ namespace bqb {
 // Register-resident variant for n <= 128: the matrices being factored or
 // inverted (Z, Zi.*X and the two line-search trial matrices) live in
 // registers, 4 x 8 entries per thread (reg_linalg.cuh), one barrier per
-// elimination step.  Same arithmetic steps as ipm_body.
+// elimination step.  The steps are ipm_body's, except that the Schur matrix
+// M = Zi.*X is inverted by the Gauss-Jordan sweep (F = M^{-1}) and both of
+// its solves are products with F: n barrier steps on 512 threads replace
+// the Cholesky plus two one-warp triangular solves of 2n steps each.
 // Shared memory: red[64], y, zd, dy, dy1, rhs (nv each), the GEMM stage
-// tile (which also holds the factorisations' 2 x 128 pivot-column buffers:
+// tile (which also holds the factorisations' 2 x 130 pivot-column buffers:
 // the GEMM and the factorisations never run at the same time), F (n^2), and
 // Zi (n^2) when it fits; global scratch: dX, dX1, and Zi otherwise.
 // ---------------------------------------------------------------------------
@@ -24,6 +27,21 @@ __host__ __device__ inline size_t ipm_reg_fixed_smem_doubles(int n)
 {
     const size_t nv = (size_t)((n + 1) & ~1);
     return 64 + 5 * nv + (size_t)CTA_KC * STG_LD;
+}
+
+// out = M^{-1} v (v null: v = -e) with Minv stored full, n x n; one warp per
+// row, reading Minv's column r (contiguous; Minv is symmetric).
+__device__ inline void ipm_minv_apply(const double* Minv, int n, const double* v, double* out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = warp; r < n; r += nw) {
+        const double* col = Minv + (size_t)r * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc = fma(col[c], v ? v[c] : -1.0, acc);
+        acc = warp_sum(acc);
+        if (lane == 0) out[r] = acc;
+    }
+    __syncthreads();
 }
 
 // stats (optional, device): the work counters [iterations n^3, problems,
@@ -98,14 +116,13 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
             }
         }
         __syncthreads();
-        if (!rm_potrf(R, n, cbuf)) { status = IPM_M_NOT_PD; break; }
-        rm_store_lower(R, F, n);
-        for (int i = tid; i < n; i += nt) rhs[i] = -1.0;
+        // M^{-1} by the register Gauss-Jordan sweep (its pivots are M's Schur
+        // complements: a non-positive one is where the reference's dposv
+        // fails), then both solves are products with it
+        if (!rm_spd_inverse(R, n, cbuf)) { status = IPM_M_NOT_PD; break; }
+        rm_store(R, F, n);
         __syncthreads();
-        if (warp == 0) warp_chol_solve(F, n, n, rhs);
-        __syncthreads();
-        for (int i = tid; i < n; i += nt) dy1[i] = rhs[i];
-        __syncthreads();
+        ipm_minv_apply(F, n, nullptr, dy1);
 
         // ---- dX1 = Zi * (-Diag(dy1) X) - X, symmetrised ----
         cta_gemm(
@@ -123,12 +140,11 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
             if (lane == 0) rhs[r] = mu * Zi[r + (size_t)r * n] - acc;
         }
         __syncthreads();
-        if (warp == 0) warp_chol_solve(F, n, n, rhs);
-        __syncthreads();
+        ipm_minv_apply(F, n, rhs, dy);
 
         // ---- dX = Zi * (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1 ----
         {
-            const double* dy2 = rhs;
+            const double* dy2 = dy;
             const double muc = mu;
             const double* Zc = Zi;
             cta_gemm(
@@ -144,7 +160,7 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
                 stage);
             cta_symmetrize(dX, n);
         }
-        for (int i = tid; i < n; i += nt) dy[i] = dy1[i] + rhs[i];
+        for (int i = tid; i < n; i += nt) dy[i] = dy1[i] + dy[i];
         __syncthreads();
 
         // ---- primal line search: chol(X + ap dX) ----
