@@ -115,7 +115,9 @@ __device__ inline void cta_symmetrize(double* A, int n)
 // on the fly by `bfun` and staged through shared memory in k-chunks.  Each
 // thread owns a 4 x 8 register tile of a 128 x 128 supertile.  The k sum is
 // sequential, so results are deterministic.  `epi(r, c, acc)` stores.
+// Called by CTAs of CTA_GEMM_THREADS threads.
 constexpr int STG_LD = CTA_TILE + 1;
+constexpr int CTA_GEMM_THREADS = 512;   // cta_gemm is called by 512-thread CTAs
 
 template <class BF, class EF>
 __device__ inline void cta_gemm(const double* A, int n, int lda, BF bfun, EF epi, double* stage)
@@ -130,13 +132,32 @@ __device__ inline void cta_gemm(const double* A, int n, int lda, BF bfun, EF epi
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+            // The next chunk of B' is formed into registers while the current
+            // one is multiplied, so its global loads overlap the FMAs.
+            constexpr int PRE = CTA_KC * CTA_TILE / CTA_GEMM_THREADS;   // chunk entries per thread
+            double pre[PRE];
+            auto form = [&](int k0) {
+#pragma unroll
+                for (int q = 0; q < PRE; ++q) {
+                    const int e = tid + q * nt;
+                    double v = 0.0;
+                    if (e < CTA_KC * CTA_TILE) {
+                        const int kk = e % CTA_KC, cc = e / CTA_KC;
+                        const int k = k0 + kk, c = c0 + cc;
+                        if (k < n && c < n) v = bfun(k, c);
+                    }
+                    pre[q] = v;
+                }
+            };
+            form(0);
             for (int k0 = 0; k0 < n; k0 += CTA_KC) {
-                for (int e = tid; e < CTA_KC * CTA_TILE; e += nt) {
-                    const int kk = e % CTA_KC, cc = e / CTA_KC;
-                    const int k = k0 + kk, c = c0 + cc;
-                    stage[kk * STG_LD + cc] = (k < n && c < n) ? bfun(k, c) : 0.0;
+#pragma unroll
+                for (int q = 0; q < PRE; ++q) {
+                    const int e = tid + q * nt;
+                    if (e < CTA_KC * CTA_TILE) stage[(e % CTA_KC) * STG_LD + e / CTA_KC] = pre[q];
                 }
                 __syncthreads();
+                if (k0 + CTA_KC < n) form(k0 + CTA_KC);
                 const int kmax = min(CTA_KC, n - k0);
                 for (int kk = 0; kk < kmax; ++kk) {
                     const double* Ak = A + (size_t)(k0 + kk) * lda;
