@@ -221,6 +221,23 @@ int bqb_solve(const double *adj, int num_vertices, const BiqBinParameters *prm, 
 int bqb_solve_parallel(const double *adj, int num_vertices, const BiqBinParameters *prm, int threads,
                        bqb_solve_result *out);
 
+/* Host heuristic plug-in (the reference's Python `set_heuristic`,
+ * src/wrapper.cpp:205-227, reached through runHeuristic,
+ * src/heuristic.c:11-17): a function with runHeuristic_unpacked's contract
+ * (P0_L, P0_N, P_L, P_N, node xfixed, node sol.X, x -> value; x receives
+ * the 0/1 solution of the BabPbSize original variables) that SDPbound on
+ * the library's default engine calls instead of the GPU heuristic; the
+ * global X holds the node's X during the call, as runHeuristic_unpacked
+ * expects.  NULL restores the GPU heuristic.  Engines and the fused kernel
+ * always use their own GPU heuristic. */
+typedef double (*bqb_heuristic_fn)(double *P0_L, int P0_N, double *P_L, int P_N, int *xfixed, int *sol_X,
+                                   int *x);
+void bqb_set_heuristic_hook(bqb_heuristic_fn fn);
+/* Heuristic calls made by SDPbound on the default engine and on engines
+ * since the last reset (reset != 0 resets after reading; the fused kernel's
+ * calls are not counted). */
+long long bqb_heuristic_runs(int reset);
+
 /* The same B&B with the nodes bounded in batches by the fused node kernel
  * (bqb_fused_submit / bqb_fused_collect): after the root (rank 0, library
  * globals), batches of at most `batch` open nodes with the largest parent
@@ -288,6 +305,9 @@ void bqb_fused_stats_reset(void);
  * scan, triangle list update, k-gonal separation, cut upload, B^T, B,
  * lambda_eta, bundle step}. */
 void bqb_fused_profile(double *out);
+/* Calls per phase of the fused kernel since the last reset, the phases of
+ * bqb_fused_profile (out[11]; out[2] = heuristic runs). */
+void bqb_fused_phase_calls(long long *out);
 /* Device milliseconds each node of the last bqb_bound_nodes_fused call took
  * (node order of that call); writes at most `count`, returns how many. */
 int bqb_fused_node_times(double *out, int count);

@@ -119,8 +119,11 @@ SIGNATURES = {
     "bqb_fused_stats": (None, [D]),
     "bqb_fused_stats_reset": (None, []),
     "bqb_fused_profile": (None, [D]),
+    "bqb_fused_phase_calls": (None, [C.POINTER(C.c_longlong)]),
     "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),
+    "bqb_set_heuristic_hook": (None, [C.c_void_p]),
+    "bqb_heuristic_runs": (C.c_longlong, [C.c_int]),
     "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),
@@ -243,20 +246,23 @@ class GlobalArrays:
         dbl = {"X": N * N, "Z": N * N, "X_test": N * N, "X_bundle": N * N * bundle_cap,
                "dual_gamma": mmax, "dgamma": mmax, "gamma_test": mmax, "eta": mmax, "g": mmax,
                "lambda": bundle_cap, "F": bundle_cap, "G": mmax * bundle_cap}
-        self.arr = {}
-        for name, size in dbl.items():
-            a = np.zeros(size)
-            self.arr[name] = a
-            C.c_void_p.in_dll(cdll, name).value = a.ctypes.data
+        self.arr = {name: np.zeros(size) for name, size in dbl.items()}
         self.cuts = (TriIneq * mmax)()
         self.lst = (TriIneq * list_cap)()
         self.pcuts = (PentIneq * mmax)()
         self.plst = (PentIneq * list_cap)()
         self.hcuts = (HeptIneq * mmax)()
         self.hlst = (HeptIneq * list_cap)()
+        self.bind()
+
+    def bind(self) -> None:
+        """Point the library's globals at these buffers (again: a solve in
+        between points them at the library's own)."""
+        for name, a in self.arr.items():
+            C.c_void_p.in_dll(self.cdll, name).value = a.ctypes.data
         for name, obj in (("Cuts", self.cuts), ("List", self.lst), ("Pent_Cuts", self.pcuts),
                           ("Pent_List", self.plst), ("Hepta_Cuts", self.hcuts), ("Hepta_List", self.hlst)):
-            C.c_void_p.in_dll(cdll, name).value = C.addressof(obj)
+            C.c_void_p.in_dll(self.cdll, name).value = C.addressof(obj)
 
     def __getitem__(self, name):
         return self.arr[name]

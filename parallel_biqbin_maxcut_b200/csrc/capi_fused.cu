@@ -164,8 +164,8 @@ void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int ra
         F.P0L_gen = gen;
     }
     if (!F.prof.p) {
-        F.prof.ensure(NKP_COUNT);
-        BQB_CUDA(cudaMemset(F.prof.p, 0, NKP_COUNT * sizeof(unsigned long long)));
+        F.prof.ensure(2 * NKP_COUNT);
+        BQB_CUDA(cudaMemset(F.prof.p, 0, 2 * NKP_COUNT * sizeof(unsigned long long)));
     }
     const size_t cN = (size_t)count * N;
     int* hf = P.hfix.ensure(2 * cN);
@@ -371,7 +371,7 @@ BQB_API void bqb_fused_stats_reset(void)
     FusedState& F = fstate();
     std::lock_guard<std::mutex> lock(F.mu);
     F.st_calls = F.st_nodes = F.st_kernel_ms = F.st_fallback_nodes = F.st_fallback_ms = 0;
-    if (F.prof.p) BQB_CUDA(cudaMemset(F.prof.p, 0, NKP_COUNT * sizeof(unsigned long long)));
+    if (F.prof.p) BQB_CUDA(cudaMemset(F.prof.p, 0, 2 * NKP_COUNT * sizeof(unsigned long long)));
 }
 
 // Time per phase of the fused kernel (seconds, summed over its CTAs) since
@@ -385,4 +385,16 @@ BQB_API void bqb_fused_profile(double* out)
     unsigned long long h[NKP_COUNT] = {};
     if (F.prof.p) BQB_CUDA(cudaMemcpy(h, F.prof.p, sizeof h, cudaMemcpyDeviceToHost));
     for (int i = 0; i < NKP_COUNT; ++i) out[i] = 1e-9 * (double)h[i];
+}
+
+// Calls per phase of the fused kernel since the last reset (out[11], the
+// phases of bqb_fused_profile; out[2] counts the heuristic runs).
+BQB_API void bqb_fused_phase_calls(long long* out)
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    unsigned long long h[NKP_COUNT] = {};
+    if (F.prof.p)
+        BQB_CUDA(cudaMemcpy(h, F.prof.p + NKP_COUNT, sizeof h, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < NKP_COUNT; ++i) out[i] = (long long)h[i];
 }

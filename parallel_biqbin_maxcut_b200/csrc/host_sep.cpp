@@ -49,6 +49,9 @@ using namespace bqb;
 namespace bqb {
 double qap_sa(const int* H, int k, const double* Xm, int n, int* ineq, Rng& rng)
 {
+    // fewer than k vertices: no k-gonal inequality exists (the reference
+    // reads past its permutation there); nothing is drawn or written
+    if (n < k) return BIG_NUMBER;
     const int inner_iter = n;
     const double reduce_temp = 0.6;
     const double increase_iter = 1.1;

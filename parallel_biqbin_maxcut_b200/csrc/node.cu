@@ -29,6 +29,9 @@ extern double diff;
 
 namespace bqb {
 
+std::atomic<bqb_heuristic_fn> g_heuristic_hook{nullptr};
+std::atomic<long long> g_heuristic_runs{0};
+
 void upload_cuts(Engine& E, const HostState& H, const Problem* P)
 {
     std::vector<CutRec> rec = pack_cuts(H.cuts, P->NIneq, H.pcuts, P->NPentIneq, H.hcuts, P->NHeptaIneq);
@@ -135,9 +138,23 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
                 node->fracsol[i] = 0.5 * (col[index++] + 1.0);
         }
     };
+    std::vector<double> hostL;
     auto heuristic = [&]() {
         for (int i = 0; i < NB; ++i) x[i] = node->xfixed[i] ? node->sol.X[i] : 0;
-        heuristic_device(E.heur, E.rng, dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
+        g_heuristic_runs.fetch_add(1);
+        bqb_heuristic_fn hook = g_heuristic_hook.load();
+        if (hook && E.is_default) {
+            // runHeuristic's plug-in point (src/heuristic.c:11-17): the caller's
+            // function gets host P0_L, P_L and the node's arrays, and the
+            // global X holds the node's X (runHeuristic_unpacked reads it)
+            hostL.resize(nn);
+            BQB_CUDA(cudaMemcpyAsync(H.X, dX, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaMemcpyAsync(hostL.data(), dL, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+            hook(SP_->L, N0, hostL.data(), n, node->xfixed, node->sol.X, x.data());
+        } else {
+            heuristic_device(E.heur, E.rng, dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
+        }
         updateSolution(x.data());
     };
 
@@ -165,6 +182,12 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) return bound;
 
     viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
+    // No violated triangle inequality (X is a cut matrix up to the
+    // tolerance): the bundle would start from t = .../0 with no cuts, where
+    // the reference's BLAS calls reject m = 0 (src/bounding.c:122-131,
+    // src/bundle.c:63, 315) and its result is undefined.  The basic bound is
+    // the node's bound, returned as the reference's early exits return it.
+    if (PP_->NIneq == 0) return bound;
     for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
     double t = 0.5 * (bound - Bab_LBGet()) / (PP_->NIneq * viol3 * viol3);
 
@@ -239,7 +262,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         } else {
             tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
         }
-        done = prune || giveup;
+        // no cuts left: the bundle cannot move (the reference's bundle
+        // calls BLAS with m = 0 there, which is undefined); stop here
+        done = prune || giveup || PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq == 0;
         store_fracsol();
 
         if (!done) {
@@ -284,6 +309,16 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
 }  // namespace bqb
 
 using namespace bqb;
+
+// Replace the default engine's GW heuristic by a host function with
+// runHeuristic_unpacked's contract (NULL: back to the GPU heuristic).
+BQB_API void bqb_set_heuristic_hook(bqb_heuristic_fn fn) { g_heuristic_hook.store(fn); }
+
+// Heuristic calls made by SDPbound / sdp_bound since the last reset.
+BQB_API long long bqb_heuristic_runs(int reset)
+{
+    return reset ? g_heuristic_runs.exchange(0) : g_heuristic_runs.load();
+}
 
 // SDPbound (src/bounding.c:24-342) in the default engine: the reference's
 // globals and rand() stream.

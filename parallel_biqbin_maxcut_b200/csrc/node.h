@@ -1,8 +1,17 @@
 // The device-resident bounding driver (SDPbound) and its pieces.
 #pragma once
+#include <atomic>
+
 #include "engine.h"
 
+// A host heuristic with runHeuristic_unpacked's contract
+// (src/heuristic.c:19): P0_L, P0_N, P_L, P_N, node xfixed, node sol.X, x.
+typedef double (*bqb_heuristic_fn)(double*, int, double*, int, int*, int*, int*);
+
 namespace bqb {
+
+extern std::atomic<bqb_heuristic_fn> g_heuristic_hook;
+extern std::atomic<long long> g_heuristic_runs;
 
 // bdl_iter iterations of src/bundle.c:47-235 on the engine's device-resident
 // bundle; t in/out on the host.  Synchronises once at the end; returns f.

@@ -59,7 +59,8 @@ __device__ __forceinline__ unsigned long long nk_now()
     return t;
 }
 
-// Phase timer: thread 0 adds the elapsed time of the enclosing scope.
+// Phase timer: thread 0 adds the elapsed time of the enclosing scope to
+// prof[phase] and counts the scope in prof[NKP_COUNT + phase].
 struct NkTimer {
     unsigned long long* prof;
     int phase;
@@ -70,7 +71,10 @@ struct NkTimer {
     }
     __device__ ~NkTimer()
     {
-        if (threadIdx.x == 0 && prof) atomicAdd(&prof[phase], nk_now() - t0);
+        if (threadIdx.x == 0 && prof) {
+            atomicAdd(&prof[phase], nk_now() - t0);
+            atomicAdd(&prof[NKP_COUNT + phase], 1ULL);
+        }
     }
 };
 __shared__ double nk_sd[8];
@@ -1158,6 +1162,9 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
 
     viol3 = nk_tri_update(c, k, k.gam, smem, &tri_add, &tri_sub);
     if (k.status) return 0.0;
+    // no violated triangle inequality: the basic bound is the node's bound
+    // (the reference's bundle start divides by the cut count)
+    if (k.mt == 0) return bound;
     // dual_gamma = the cuts' y (0 for the new ones)
     for (int i = tid; i < k.mt; i += nt) k.gam[i] = k.triy[i];
     lb = nk_lb(c);
@@ -1235,7 +1242,9 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
         } else {
             tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
         }
-        done = prune || giveup;
+        // no cuts left: the bundle cannot move (the reference's bundle
+        // calls BLAS with m = 0 there, which is undefined); stop here
+        done = prune || giveup || k.mt + k.mp + k.mh == 0;
         nk_fracsol(c, k);
 
         if (!done) {

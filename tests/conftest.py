@@ -31,10 +31,17 @@ def lib():
 
 
 @pytest.fixture(scope="session")
-def lib_globals(lib):
-    """The product library's reference-layout globals, sized for n <= 344."""
+def _global_arrays(lib):
     from parallel_biqbin_maxcut_b200 import _lib
     return _lib.GlobalArrays(lib, 344)
+
+
+@pytest.fixture
+def lib_globals(_global_arrays):
+    """The product library's reference-layout globals, sized for n <= 344,
+    bound for this test (a solve in an earlier test re-points them)."""
+    _global_arrays.bind()
+    return _global_arrays
 
 
 @pytest.fixture(scope="session")

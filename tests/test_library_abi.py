@@ -18,6 +18,7 @@ pytestmark = pytest.mark.skipif(not os.path.exists(_lib.LIB_PATH), reason="libra
 def declared_functions():
     txt = open(HEADER).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    txt = re.sub(r"^typedef\b[^;]*;", "", txt, flags=re.M | re.S)
     names = set()
     for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", txt, flags=re.M):
         name = m.group(1)
