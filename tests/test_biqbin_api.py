@@ -130,6 +130,33 @@ def test_reference_qubo_fixture_conversion():
     assert cut * g == pytest.approx(exp["maxcut"]["computed_val"])
 
 
+@pytest.mark.skipif(not os.path.exists("/root/reference/biqbin_base.py"), reason="reference Python layer not present")
+def test_reference_python_layer_imports_this_module(tmp_path, monkeypatch):
+    """The reference's biqbin_base.py imports its six functions from this
+    module: its solvers install their overrides here, and its default data
+    getter reads a Rudy file through our default_read_data."""
+    import importlib
+    import sys
+    monkeypatch.setattr(sys, "dont_write_bytecode", True)   # nothing is written next to the reference
+    monkeypatch.setitem(sys.modules, "biqbin", biqbin)
+    monkeypatch.syspath_prepend("/root/reference")
+    monkeypatch.delitem(sys.modules, "biqbin_base", raising=False)
+    base = importlib.import_module("biqbin_base")
+    try:
+        A = instances.gnp_int(10, 0.5, 5, seed=2)
+        p = tmp_path / "g.rudy"
+        instances.write_rudy(str(p), A)
+        solver = base.MaxCutSolver(base.DataGetterMaxCutDefault(str(p)), "params")
+        assert biqbin._heuristic is not None and biqbin._read_data is not None
+        assert np.array_equal(biqbin._read_data(), A)
+        assert solver.get_rank() == 0
+        (tmp_path / "a.json").write_text(json.dumps({"adjacency": biqbin.to_sparse(A)}))
+        assert np.array_equal(base.DataGetterAdjacencyJson(str(tmp_path / "a.json")).read_file(), A)
+    finally:
+        biqbin._clean()
+        sys.modules.pop("biqbin_base", None)
+
+
 # ---- GPU: run() end to end ------------------------------------------------
 
 def _golden(kind, nv, seed):
