@@ -17,7 +17,9 @@ namespace bqb {
 // elimination step.  The steps are ipm_body's, except that the Schur matrix
 // M = Zi.*X is inverted by the Gauss-Jordan sweep (F = M^{-1}) and both of
 // its solves are products with F: n barrier steps on 512 threads replace
-// the Cholesky plus two one-warp triangular solves of 2n steps each.
+// the Cholesky plus two one-warp triangular solves of 2n steps each.  The
+// line searches need only "positive definite or not": the pivots of the
+// elimination, without forming the factor.
 // Shared memory: red[64], y, zd, dy, dy1, rhs (nv each), the GEMM stage
 // tile (which also holds the factorisations' 2 x 130 pivot-column buffers:
 // the GEMM and the factorisations never run at the same time), F (n^2), and
@@ -163,7 +165,7 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
         for (int i = tid; i < n; i += nt) dy[i] = dy1[i] + dy[i];
         __syncthreads();
 
-        // ---- primal line search: chol(X + ap dX) ----
+        // ---- primal line search: X + ap dX positive definite (the reference's chol) ----
         double ap = 1.0;
         int trials = 0;
         bool ok = false;
@@ -173,7 +175,7 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
                 const size_t e = r + (size_t)c * n;
                 return fma(al, dX[e], X[e]);
             });
-            if (rm_potrf(R, n, cbuf)) { ok = true; break; }
+            if (rm_posdef(R, n, cbuf)) { ok = true; break; }
             __syncthreads();
             if (++trials >= IPM_MAX_TRIALS) break;
             ap *= 0.8;
@@ -182,7 +184,7 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
         if (!ok) { status = IPM_LINESEARCH; break; }
         if (ap < 1.0) ap *= 0.95;
 
-        // ---- dual line search: chol(Z + ad Diag(dy)) ----
+        // ---- dual line search: Z + ad Diag(dy) positive definite ----
         double ad = 1.0;
         trials = 0;
         ok = false;
@@ -191,7 +193,7 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
             rm_fill(R, n, [&](int r, int c) {
                 return r == c ? fma(al, dy[r], zd[r]) : -L[r + (size_t)c * n];
             });
-            if (rm_potrf(R, n, cbuf)) { ok = true; break; }
+            if (rm_posdef(R, n, cbuf)) { ok = true; break; }
             __syncthreads();
             if (++trials >= IPM_MAX_TRIALS) break;
             ad *= 0.8;

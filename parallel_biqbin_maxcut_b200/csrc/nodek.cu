@@ -59,6 +59,11 @@ __device__ __forceinline__ unsigned long long nk_now()
     return t;
 }
 
+// The kernel's dynamic shared memory.  Most phases below are separate
+// functions (not inlined); they name this array instead of taking a pointer,
+// so the compiler keeps shared-memory addressing across the call boundary.
+extern __shared__ __align__(16) double nk_smem[];
+
 // Phase timer: thread 0 adds the elapsed time of the enclosing scope to
 // prof[phase] and counts the scope in prof[NKP_COUNT + phase].
 struct NkTimer {
@@ -394,12 +399,14 @@ __device__ __noinline__ void nk_subproblem(const FusedCfg& c, Nk& k)
 // IPM (the engine's kernel body)
 // ---------------------------------------------------------------------------
 // Separate (not inlined) so the IPM body keeps the whole register budget.
+// (The IPM body takes the shared memory as a generic pointer: measured
+// faster here than naming nk_smem inside.)
 __device__ __noinline__ void nk_ipm_call(IpmDesc d, double* smem, int zi, double* stats)
 {
     ipm_body_reg(d, smem, zi, stats);
 }
 
-__device__ bool nk_ipm(const FusedCfg& c, Nk& k, const double* Lsrc, double* Xdst, const int* xslot, double* smem)
+__device__ bool nk_ipm(const FusedCfg& c, Nk& k, const double* Lsrc, double* Xdst, const int* xslot)
 {
     const int n = k.n;
     const size_t fixed = ipm_reg_fixed_smem_doubles(n) * sizeof(double);
@@ -408,7 +415,7 @@ __device__ bool nk_ipm(const FusedCfg& c, Nk& k, const double* Lsrc, double* Xds
     IpmDesc d{Lsrc, Xdst, k.ws, k.out, xslot, n, 0};
     {
         NkTimer tm(c.prof, NKP_IPM);
-        nk_ipm_call(d, smem, zi, c.ipm_stats);
+        nk_ipm_call(d, nk_smem, zi, c.ipm_stats);
     }
     __syncthreads();
     if ((int)k.out[2] != IPM_OK) {
@@ -463,8 +470,9 @@ __device__ void nk_report(const FusedCfg& c, Nk& k, double value, const int* x)
 // counter-based random numbers.  Shared: Z (n^2), column buffer, 1-opt
 // buffers.
 // ---------------------------------------------------------------------------
-__device__ __noinline__ double nk_heuristic(const FusedCfg& c, Nk& k, double* smem)
+__device__ __noinline__ double nk_heuristic(const FusedCfg& c, Nk& k)
 {
+    double* const smem = nk_smem;
     NkTimer tm(c.prof, NKP_HEUR);
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const int n = k.n, N = k.N, num = k.N0;
@@ -660,8 +668,9 @@ __device__ void nk_heap_down(double* hv, int* hs, int T, int i)
 }
 
 // Returns the maximum violation; list in k.tslist, its size in *size.
-__device__ __noinline__ double nk_trisep(const FusedCfg& c, Nk& k, const double* X, double* smem, int* size)
+__device__ __noinline__ double nk_trisep(const FusedCfg& c, Nk& k, const double* X, int* size)
 {
+    double* const smem = nk_smem;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const int n = k.n;
     const int T = c.TriIneq;
@@ -812,7 +821,7 @@ __device__ __forceinline__ uint32_t nk_hash(uint32_t x, uint32_t mask)
 
 // purge + separate + append for the triangle list.  y: current duals of
 // the triangle cuts.  Returns the maximum violation (viol3).
-__device__ __noinline__ double nk_tri_update(const FusedCfg& c, Nk& k, const double* y, double* smem, int* added, int* subtracted)
+__device__ __noinline__ double nk_tri_update(const FusedCfg& c, Nk& k, const double* y, int* added, int* subtracted)
 {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int kept = cta_compact<TriEnt>(
@@ -828,7 +837,7 @@ __device__ __noinline__ double nk_tri_update(const FusedCfg& c, Nk& k, const dou
     double mx;
     {
         NkTimer tm(c.prof, NKP_TRISEP);
-        mx = nk_trisep(c, k, k.X, smem, &size);
+        mx = nk_trisep(c, k, k.X, &size);
     }
     NkTimer tm2(c.prof, NKP_TRILIST);
     // membership among the kept cuts
@@ -873,9 +882,10 @@ __device__ __noinline__ double nk_tri_update(const FusedCfg& c, Nk& k, const dou
 
 // purge + separate (annealing chains) + append for the k-gonal list.
 template <int K>
-__device__ __noinline__ double nk_kgon_update(const FusedCfg& c, Nk& k, const double* y, double* smem, int* added,
+__device__ __noinline__ double nk_kgon_update(const FusedCfg& c, Nk& k, const double* y, int* added,
                                  int* subtracted)
 {
+    double* const smem = nk_smem;
     NkTimer tm(c.prof, NKP_KGON);
     const int tid = threadIdx.x, nt = blockDim.x;
     unsigned long long* keys = K == 5 ? k.pentkey : k.heptkey;
@@ -1093,10 +1103,10 @@ __device__ __noinline__ void nk_opB(Nk& k, const int* slots, int ncols)
 // ---------------------------------------------------------------------------
 // Bundle (the engine's bodies)
 // ---------------------------------------------------------------------------
-__device__ __noinline__ void nk_lambda_eta(LeArgs a, double* smem) { lambda_eta_body(a, smem); }
+__device__ __noinline__ void nk_lambda_eta(LeArgs a) { lambda_eta_body(a, nk_smem); }
 __device__ __noinline__ void nk_step(StepArgs a) { bundle_step_body(a); }
 
-__device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter, double* smem)
+__device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter)
 {
     const int m = k.mt + k.mp + k.mh;
     const size_t nn = (size_t)k.n * k.n;
@@ -1105,14 +1115,14 @@ __device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter, dou
                  k.qpws, -1};
         {
             NkTimer tm(c.prof, NKP_LAMBDA);
-            nk_lambda_eta(a, smem);
+            nk_lambda_eta(a);
         }
         __syncthreads();
         {
             NkTimer tm(c.prof, NKP_OPBT);
             nk_opBt(c, k, k.gtest);
         }
-        if (!nk_ipm(c, k, k.L0, k.Xb, k.istate + BI_NEXT, smem)) return;
+        if (!nk_ipm(c, k, k.L0, k.Xb, k.istate + BI_NEXT)) return;
         if (m > 0) {
             NkTimer tm(c.prof, NKP_OPB);
             nk_opB(k, k.istate + BI_NEXT, 1);
@@ -1138,7 +1148,7 @@ __device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter, dou
 // ---------------------------------------------------------------------------
 // One node: SDPbound (src/bounding.c:24-342)
 // ---------------------------------------------------------------------------
-__device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
+__device__ double nk_bound(const FusedCfg& c, Nk& k)
 {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int n = k.n;
@@ -1148,11 +1158,11 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
     int tri_add = 0, tri_sub = 0, pent_add = 0, pent_sub = 0, hept_add = 0, hept_sub = 0;
     double viol3 = 0.0, viol5 = 0.0;
 
-    if (!nk_ipm(c, k, k.L, k.X, nullptr, smem)) return 0.0;
+    if (!nk_ipm(c, k, k.L, k.X, nullptr)) return 0.0;
     double f = k.out[0];
     const double basic_bound = f + k.fixedvalue;
     nk_fracsol(c, k);
-    nk_heuristic(c, k, smem);
+    nk_heuristic(c, k);
     if (k.status) return 0.0;
 
     double bound = f + k.fixedvalue;
@@ -1160,7 +1170,7 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
     if (bound < lb + 1.0) return bound;
     if (c.use_diff && c.rank != 0 && bound > lb + c.diff + 1.0) return bound;
 
-    viol3 = nk_tri_update(c, k, k.gam, smem, &tri_add, &tri_sub);
+    viol3 = nk_tri_update(c, k, k.gam, &tri_add, &tri_sub);
     if (k.status) return 0.0;
     // no violated triangle inequality: the basic bound is the node's bound
     // (the reference's bundle start divides by the cut count)
@@ -1203,7 +1213,7 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
             k.status |= NKS_BUNDLE_CAP;
             return 0.0;
         }
-        nk_bundle_iterations(c, k, bdl_iter, smem);
+        nk_bundle_iterations(c, k, bdl_iter);
         if (k.status) return 0.0;
         f = k.dstate[BD_F];
         t = k.dstate[BD_T];
@@ -1212,7 +1222,7 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
         lb = nk_lb(c);
         prune = bound < lb + 1.0;
         if (!prune) {
-            nk_heuristic(c, k, smem);
+            nk_heuristic(c, k);
             if (k.status) return 0.0;
             lb = nk_lb(c);
             prune = bound < lb + 1.0;
@@ -1227,16 +1237,16 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
         if (!prune && !giveup) {
             const int triag = k.mt;
             const int penta = k.mp;
-            viol3 = nk_tri_update(c, k, k.gam, smem, &tri_add, &tri_sub);
+            viol3 = nk_tri_update(c, k, k.gam, &tri_add, &tri_sub);
             if (k.status) return 0.0;
             const bool do_pent = c.include_Pent && (count > c.triag_iter || viol3 < 0.2);
             if (do_pent) {
-                viol5 = nk_kgon_update<5>(c, k, k.gam + triag, smem, &pent_add, &pent_sub);
+                viol5 = nk_kgon_update<5>(c, k, k.gam + triag, &pent_add, &pent_sub);
                 if (k.status) return 0.0;
             }
             if (c.include_Hepta &&
                 ((count > c.triag_iter + c.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4)))) {
-                nk_kgon_update<7>(c, k, k.gam + triag + penta, smem, &hept_add, &hept_sub);
+                nk_kgon_update<7>(c, k, k.gam + triag + penta, &hept_add, &hept_sub);
                 if (k.status) return 0.0;
             }
         } else {
@@ -1264,7 +1274,7 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
                 NkTimer tm(c.prof, NKP_OPBT);
                 nk_opBt(c, k, k.gam);
             }
-            if (!nk_ipm(c, k, k.L0, k.Xb, k.istate + BI_NEXT, smem)) return 0.0;
+            if (!nk_ipm(c, k, k.L0, k.Xb, k.istate + BI_NEXT)) return 0.0;
             if (m > 0) {
                 nk_opB(k, k.slot, kb);
                 nk_opB(k, k.istate + BI_NEXT, 1);
@@ -1290,7 +1300,6 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k, double* smem)
 
 __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
 {
-    extern __shared__ __align__(16) double smem[];
     Nk k;
     nk_bind(c, k, blockIdx.x);
     k.N0 = c.N0;
@@ -1320,7 +1329,7 @@ __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
         if (k.n > NK_NMAX)
             k.status |= NKS_SIZE;
         else
-            b = nk_bound(c, k, smem);
+            b = nk_bound(c, k);
         __syncthreads();
         if (threadIdx.x == 0) {
             c.bound[node] = b;

@@ -93,17 +93,18 @@ __device__ __forceinline__ void rm_publish_tail(const RegMat& M, int k, double* 
     }
 }
 
-// Cholesky A = L L^T (L in the lower triangle of M; the upper triangle is
-// left with symmetric leftovers).  col2: 2 * RM_BUF doubles of shared
-// memory.  Returns false, uniformly, at the first non-positive pivot.
-// Step k: the owners publish rows r > k of column k (zeros for r <= k, and
-// the padding rows hold zeros, so the update needs no index tests) and the
-// pivot a_kk; every thread applies A_ij -= (a_ik / a_kk) a_jk to its 32
-// entries (a no-op where either factor is zero); the owners turn their
-// column into L_ik = a_ik / sqrt(a_kk).
-__device__ __forceinline__ bool rm_potrf(RegMat& M, int n, double* col2)
+// Is the symmetric matrix in M (lower triangle read) positive definite?
+// The pivots of the symmetric elimination, as a Cholesky factorisation
+// meets them: step k reads the published tail of column k (rows r > k;
+// zeros for r <= k, and the padding rows hold zeros, so the update needs no
+// index tests) and the pivot a_kk, and every thread applies
+// A_ij -= (a_ik / a_kk) a_jk to its 32 entries (a no-op where either factor
+// is zero).  Only the pivots are needed, so the factor itself is not formed
+// (the owner warp has no extra work on the step's critical path).  Returns
+// false, uniformly, at the first non-positive pivot; M is overwritten.
+// col2: 2 * RM_BUF doubles of shared memory.
+__device__ __forceinline__ bool rm_posdef(RegMat& M, int n, double* col2)
 {
-    (void)n;
     rm_publish_tail(M, 0, col2);
     __syncthreads();
     const int lane = threadIdx.x & 31, tc = threadIdx.x >> 5;
@@ -122,18 +123,6 @@ __device__ __forceinline__ bool rm_potrf(RegMat& M, int n, double* col2)
         for (int a = 0; a < 4; ++a)
 #pragma unroll
             for (int b = 0; b < 8; ++b) M.m[a][b] = fma(-cr[a], cc[b], M.m[a][b]);
-        if (tc == (k & 15)) {
-            const int kb = k >> 4;
-#pragma unroll
-            for (int b = 0; b < 8; ++b)
-                if (b == kb)
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int r = lane + 32 * a;
-                        if (r > k) M.m[a][b] = col[r] * rs;
-                        else if (r == k) M.m[a][b] = d * rs;   // sqrt(d)
-                    }
-        }
         if (k + 1 < n) rm_publish_tail(M, k + 1, col2 + ((k + 1) & 1) * RM_BUF);
         __syncthreads();
     }
