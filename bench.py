@@ -415,6 +415,28 @@ def run_gpu(args):
         # restore the bench's problem (the solver set up its own)
         arm.reset_problem()
 
+    # ---- learned warm start: B&B to optimality, plain vs warm-started bundle ----
+    learned = None
+    if args.learned and rank == 0:
+        from parallel_biqbin_maxcut_b200 import warm
+        p_w, _ = warm.load_model(warm.MODEL_C5)
+        A = warm.c5_instance(80, 913)
+        learned = {"instance": "G(80,0.9), integer weights U[-10,10], seed 913 (held out from the model's "
+                               "training instances)", "call": "bqb_solve_parallel, 16 engines"}
+        for mode in ("plain", "warm"):
+            warm.use_model(arm.lib, p_w if mode == "warm" else None)
+            kst = (C.c_longlong * 2)()
+            arm.lib.bqb_warm_stats(kst, 1)
+            t0 = time.perf_counter()
+            r = _lib.solve(A, threads=16, time_limit=300)
+            learned[mode] = {"seconds": time.perf_counter() - t0, "optimum": r["best_value"], "nodes": r["nodes"]}
+            arm.lib.bqb_warm_stats(kst, 1)
+            learned[mode]["proposals_kept"] = int(kst[0])
+            learned[mode]["proposals_rejected"] = int(kst[1])
+        warm.use_model(arm.lib, None)
+        learned["speedup_warm_vs_plain"] = learned["plain"]["seconds"] / learned["warm"]["seconds"]
+        arm.reset_problem()
+
     pk = peaks()
     kernel_ms = fst[2]
     flops = FLOP_PER_ITER_N3 * stats[0]
@@ -463,6 +485,7 @@ def run_gpu(args):
             "engines": eng,
             "dropin_serial": drop,
             "time_to_optimality": tto,
+            "learned_warm_start": learned,
             "gpu_launches": int(launches),
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -633,6 +656,8 @@ def main():
     ap.add_argument("--depth", type=int, default=8, help="fused launches in flight (1..8)")
     ap.add_argument("--no-tto", dest="tto", action="store_false",
                     help="skip the time-to-optimality run")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the learned warm-start comparison (two B&B runs, about 10 s)")
     ap.add_argument("--tto-plain", action="store_true",
                     help="also time the plain drop-in solver to optimality (about 40 s)")
     ap.add_argument("--engine-nodes", type=int, default=128,

@@ -382,6 +382,44 @@ int bqb_ipm_noalloc(const double *L, double *X, int n, double *out, void *stream
 int bqb_ipm_batch(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
                   double *phi, int *iters, int *status);
 
+/* ==== Learned warm start of the bundle multipliers ====================
+ * No reference counterpart.  After a node's first triangle separation the
+ * reference starts its bundle at gamma = 0 (src/bounding.c:121-131).  With
+ * a model loaded and the warm start switched on, SDPbound on every engine
+ * evaluates a network's proposal gamma >= 0 for those cuts once (one IPM on
+ * L - B^T(gamma)) and starts the bundle there when its dual value is below
+ * the plain start's; any gamma >= 0 gives a valid bound, and the bundle then
+ * runs to the reference's stopping rules.  Off by default.  Network: 12 cut
+ * features -> 32 -> 32 (ReLU) -> softplus, in units of the node's objective
+ * scale (mean |L_ij|); FP32 training (Adam) with this library's kernels,
+ * BF16-weight inference.  Parameters: BQB_WARM_NPARAM floats, layout
+ * W1[12][32], b1[32], W2[32][32], b2[32], w3[32], b3. */
+#define BQB_WARM_NPARAM 1505
+/* out[3] = {features per cut, hidden units, parameters}. */
+void bqb_warm_dims(int *out);
+/* Train from params (in/out) on N rows: feats[N x 12], targets[N]; Adam,
+ * `steps` minibatches of `batch` rows (seeded shuffle); losses[steps] may be
+ * NULL.  Returns 0, or -1 on bad arguments. */
+int bqb_warm_train(const float *feats, const float *targets, int N, int steps, int batch, float lr,
+                   unsigned seed, float *params, float *losses);
+/* Full-batch loss and gradient at params (the training kernels). */
+int bqb_warm_grad(const float *params, const float *feats, const float *targets, int N, float *grad,
+                  float *loss);
+/* Inference path (BF16 weights) on N feature rows: out[N]. */
+int bqb_warm_predict(const float *params, const float *feats, int N, double *out);
+/* Load the model SDPbound uses (NULL unloads); call before bounding. */
+int bqb_warm_set_model(const float *params);
+/* Warm start on (a model must be loaded) / off. */
+void bqb_warm_enable(int on);
+/* Record training pairs while bounding (features of each node's first-
+ * separation cuts, the multipliers they end with; off by default). */
+void bqb_warm_record(int on);
+/* Copy min(count, cap) recorded pairs out; returns the count. */
+long long bqb_warm_dataset(float *feats, float *targets, long long cap);
+void bqb_warm_dataset_clear(void);
+/* out[2] = {proposals kept, proposals rejected}; reset != 0 zeroes them. */
+void bqb_warm_stats(long long *out, int reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -122,6 +122,18 @@ SIGNATURES = {
     "bqb_fused_phase_calls": (None, [C.POINTER(C.c_longlong)]),
     "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),
+    "bqb_warm_train": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float,
+                                 C.c_uint, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "bqb_warm_grad": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                                C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "bqb_warm_predict": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, D]),
+    "bqb_warm_set_model": (C.c_int, [C.POINTER(C.c_float)]),
+    "bqb_warm_enable": (None, [C.c_int]),
+    "bqb_warm_record": (None, [C.c_int]),
+    "bqb_warm_dataset": (C.c_longlong, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_longlong]),
+    "bqb_warm_dataset_clear": (None, []),
+    "bqb_warm_stats": (None, [C.POINTER(C.c_longlong), C.c_int]),
+    "bqb_warm_dims": (None, [C.POINTER(C.c_int)]),
     "bqb_set_heuristic_hook": (None, [C.c_void_p]),
     "bqb_heuristic_runs": (C.c_longlong, [C.c_int]),
     "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
@@ -174,6 +186,11 @@ def dptr(a: np.ndarray):
 def iptr(a: np.ndarray):
     assert a.dtype == np.int32 and a.flags.c_contiguous, (a.dtype, a.flags)
     return a.ctypes.data_as(I)
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 def colmajor(A: np.ndarray) -> np.ndarray:

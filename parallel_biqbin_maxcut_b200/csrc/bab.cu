@@ -376,6 +376,15 @@ BQB_API int bqb_read_params(const char* path, BiqBinParameters* p)
 // Allocate the reference globals the bounding path reads on the host
 // (src/allocate_free.c:8-42).  X_bundle and G stay on the device in this
 // driver, so their host copies are not allocated.
+// The solvers keep their incumbent cut in a record of their own: BabSol may
+// point at memory a host program or binding has since released.  Zeroed.
+static BabSolution* solver_solution()
+{
+    static BabSolution sol;
+    memset(&sol, 0, sizeof sol);
+    return &sol;
+}
+
 static void alloc_globals(int N)
 {
     // Only arrays this function allocated earlier are freed: a host program
@@ -429,8 +438,7 @@ BQB_API int bqb_solve(const double* adj, int num_vertices, const BiqBinParameter
     process_adj_matrix(A.data(), num_vertices);
     if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
     srand(2020);
-    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
-    memset(BabSol, 0, sizeof(BabSolution));
+    BabSol = solver_solution();
     g_LB.store(0.0);
     g_num_nodes = 0;
     stopped = 0;
@@ -572,8 +580,7 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
     process_adj_matrix(A.data(), num_vertices);
     if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
     srand(2020);
-    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
-    memset(BabSol, 0, sizeof(BabSolution));
+    BabSol = solver_solution();
     g_LB.store(0.0);
     g_num_nodes = 0;
     stopped = 0;
@@ -690,8 +697,7 @@ BQB_API int bqb_solve_fused(const double* adj, int num_vertices, const BiqBinPar
     process_adj_matrix(A.data(), num_vertices);
     if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
     srand(2020);
-    if (!BabSol) BabSol = (BabSolution*)calloc(1, sizeof(BabSolution));
-    memset(BabSol, 0, sizeof(BabSolution));
+    BabSol = solver_solution();
     g_LB.store(0.0);
     g_num_nodes = 0;
     stopped = 0;

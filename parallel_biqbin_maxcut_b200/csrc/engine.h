@@ -17,6 +17,7 @@
 #include "kgon_sa.cuh"
 #include "rng.h"
 #include "trisep.cuh"
+#include "warm.h"
 
 namespace bqb {
 
@@ -61,6 +62,7 @@ struct Engine {
     uint64_t sa_seed = 0;    // its chains' seed base ...
     uint64_t sa_calls = 0;   // ... and the separation calls made so far
     DevBuf<double> ipm_ws;
+    WarmDev warm;            // learned warm start of the bundle multipliers
     // private host state (extra engines only)
     std::vector<Triangle_Inequality> cuts_v;
     std::vector<Pentagonal_Inequality> pcuts_v, plist_v;

@@ -193,6 +193,46 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
 
     // bundle init: X_bundle(0) = X, G(:,0) = 1 - B(X), F(0) = <L,X>, bundle = 1
     upload_cuts(E, H, PP_);
+
+    // Learned warm start (off unless a model is loaded and switched on):
+    // evaluate the proposed multipliers once (L0 = L - B^T(gamma_w), one
+    // IPM) and start the bundle there when their dual value is below the
+    // plain start's (gamma = 0, where the dual value is the basic bound f).
+    // Any gamma >= 0 gives a valid bound; the bundle then runs to its own
+    // stopping rules.  Recording keeps the first-separation cuts' features
+    // and, at the end, the multipliers they finish with (training pairs).
+    const bool warm_rec = warm_recording();
+    std::vector<float> warm_feats;
+    std::vector<Triangle_Inequality> warm_first;
+    double warm_scale = 1.0;
+    if (warm_rec || warm_active()) {
+        warm_features(E.warm, H.cuts, PP_->NIneq, dX, dL, n, viol3, bound - Bab_LBGet(), s);
+        if (warm_rec) {
+            warm_scale = warm_fetch_features(E.warm, PP_->NIneq, warm_feats, s);
+            warm_first.assign(H.cuts, H.cuts + PP_->NIneq);
+        }
+    }
+    if (warm_active()) {
+        const int mw = PP_->NIneq;
+        warm_infer(E.warm, mw, s);
+        BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        opBt_launch(nd.cuts, nd.L0.p, n, E.warm.gam.p, s);
+        double* Xw = E.warm.X.ensure(nn);
+        ipm_device(E.ipm_ws, nd.L0.p, Xw, n, dout, s);
+        double* hg = E.warm.hgam.ensure(mw);
+        BQB_CUDA(cudaMemcpyAsync(hg, E.warm.gam.p, (size_t)mw * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+        double fw = nd.hs.p[0];
+        for (int i = 0; i < mw; ++i) fw += hg[i];
+        const bool keep = (int)nd.hs.p[2] == IPM_OK && fw < f;
+        warm_count(keep);
+        if (keep) {
+            for (int i = 0; i < mw; ++i) H.dual_gamma[i] = hg[i];
+            BQB_CUDA(cudaMemcpyAsync(dX, Xw, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            f = fw;
+        }
+    }
     BundleDev& b = nd.b;
     b.ensure_cap(1 + bdl_iter + 2, n, s);
     const int m0 = nd.cuts.m;
@@ -300,6 +340,16 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         }
         bdl_iter += count % 2;
         bdl_iter = (bdl_iter < params.max_bundle_iter) ? bdl_iter : params.max_bundle_iter;
+    }
+    if (warm_rec && !warm_first.empty()) {
+        std::vector<double> fg(PP_->NIneq > 0 ? PP_->NIneq : 1);
+        if (PP_->NIneq > 0) {
+            BQB_CUDA(cudaMemcpyAsync(fg.data(), b.gam.p, (size_t)PP_->NIneq * sizeof(double), cudaMemcpyDeviceToHost,
+                                     s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+        }
+        warm_record(warm_feats, warm_scale, warm_first.data(), (int)warm_first.size(), H.cuts, fg.data(),
+                    PP_->NIneq);
     }
     bound = f + fixedvalue;
     if (rank == 0) diff = basic_bound - bound;

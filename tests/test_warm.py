@@ -1,0 +1,160 @@
+"""Learned warm start of the bundle multipliers.
+
+CPU: the network oracle's analytic gradient against central differences.
+GPU: the library's training kernels (loss and gradient) and its BF16
+inference kernel against the oracle; training lowers the loss; the
+recorder yields training pairs; warm-started bounds are valid upper bounds
+(checked by enumeration) and the warm start is off by default."""
+import ctypes as C
+import itertools
+
+import numpy as np
+import pytest
+
+from oracle import warm_oracle as W
+from parallel_biqbin_maxcut_b200 import _lib, warm
+
+
+def _data(N, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((N, W.F)).astype(np.float32)
+    y = np.abs(rng.standard_normal(N)).astype(np.float32)
+    return X, y
+
+
+def test_oracle_gradient_matches_central_differences():
+    X, y = _data(40, 1)
+    p = warm.init_params(3, lib=_FakeDims()).astype(np.float64)
+    p[-1] = 0.3
+    loss, g = W.loss_and_grad(p, X, y)
+    idx = list(range(0, W.NPARAM, 37)) + [W.NPARAM - 1]
+    num = W.numeric_grad(p, X, y, idx)
+    np.testing.assert_allclose(g[idx], num, rtol=1e-5, atol=1e-8)
+    assert loss > 0
+
+
+def test_bf16_rounding():
+    v = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 0.0], np.float32)
+    r = W.bf16(v)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == np.float32(1.0078125)
+    assert abs(r[3] + 3.140625) < 1e-6 and r[4] == 0.0
+
+
+class _FakeDims:
+    """Stands in for the library in warm.init_params on CPU (the network's
+    sizes come from the oracle)."""
+
+    def bqb_warm_dims(self, d):
+        d[0], d[1], d[2] = W.F, W.H, W.NPARAM
+
+
+@pytest.mark.gpu
+def test_dims_match_oracle(lib):
+    assert warm.dims(lib) == (W.F, W.H, W.NPARAM)
+
+
+@pytest.mark.gpu
+def test_gpu_gradient_matches_oracle(lib):
+    X, y = _data(700, 2)
+    p = warm.init_params(5, lib)
+    p[-1] = 0.2
+    g = np.zeros(W.NPARAM, np.float32)
+    loss = C.c_float()
+    assert lib.bqb_warm_grad(_lib.fptr(p), _lib.fptr(X), _lib.fptr(y), len(y), _lib.fptr(g), C.byref(loss)) == 0
+    l_ref, g_ref = W.loss_and_grad(p, X, y)
+    assert abs(loss.value - l_ref) <= 1e-5 * l_ref
+    # float32 sums over 700 rows: relative to the gradient's scale
+    np.testing.assert_allclose(g, g_ref, rtol=0, atol=2e-5 * np.abs(g_ref).max())
+
+
+@pytest.mark.gpu
+def test_bf16_inference_matches_oracle(lib):
+    X, _ = _data(333, 4)
+    p = warm.init_params(6, lib)
+    out = np.zeros(len(X))
+    assert lib.bqb_warm_predict(_lib.fptr(p), _lib.fptr(X), len(X), _lib.dptr(out)) == 0
+    ref, _ = W.forward(W.bf16(p), X)
+    np.testing.assert_allclose(out, ref, rtol=1e-4, atol=1e-5)
+    assert np.all(out >= 0)
+
+
+@pytest.mark.gpu
+def test_training_lowers_loss(lib):
+    X, _ = _data(6000, 7)
+    teacher = warm.init_params(11, lib)
+    y, _ = W.forward(teacher, X)
+    y = y.astype(np.float32)
+    p0 = warm.init_params(12, lib)
+    l0, _ = W.loss_and_grad(p0, X, y)
+    p, losses = warm.train(lib, X, y, steps=600, batch=512, lr=3e-3, seed=1, params=p0, standardize=False)
+    l1, _ = W.loss_and_grad(p, X, y)
+    assert l1 < 0.2 * l0, (l0, l1)
+    assert losses[-20:].mean() < losses[:20].mean()
+
+
+def _best_completion(A, xf, sol):
+    nv = A.shape[0]
+    free = np.flatnonzero(xf == 0)
+    best = -np.inf
+    for bits in itertools.product((0, 1), repeat=len(free)):
+        x = np.zeros(nv, dtype=int)
+        x[:-1] = np.where(xf == 1, sol, 0)
+        x[free] = bits
+        best = max(best, float(np.sum(np.triu(A, 1) * (x[:, None] != x[None, :]))))
+    return best
+
+
+@pytest.mark.gpu
+def test_record_train_and_warm_bounds_are_valid(lib):
+    """End to end on a small instance of the warm-start family: record
+    pairs, train, bound held-out nodes with and without the warm start.
+    Every bound must be an upper bound of the node's best cut."""
+    feats, targets = warm.record_pairs(lib, [(40, 101), (40, 102)], nodes_per_instance=24, kmax=20, threads=8)
+    assert len(targets) > 0 and feats.shape == (len(targets), W.F)
+    assert np.all(targets >= 0) and np.all(np.isfinite(feats))
+    p, _ = warm.train(lib, feats, targets, steps=300, batch=256, lr=3e-3, seed=2)
+    A = warm.c5_instance(40, 103)
+    inst = warm.Instance(lib, A)
+    rng = np.random.default_rng(9)
+    nodes = (_lib.BabNode * 8)()
+    for q in range(8):
+        xf = np.ones(39, dtype=int)
+        xf[rng.choice(39, 8 + q % 3, replace=False)] = 0   # 8..10 free vertices
+        sol = rng.integers(0, 2, 39) * xf
+        nodes[q].xfixed[:39] = [int(v) for v in xf]
+        nodes[q].sol[:39] = [int(v) for v in sol]
+    res = warm.compare(lib, inst, nodes, p, threads=4)
+    for q in range(8):
+        xf, sol = np.array(nodes[q].xfixed[:39]), np.array(nodes[q].sol[:39])
+        best = _best_completion(A, xf, sol)
+        assert res["bounds_plain"][q] >= best - 1e-6
+        assert res["bounds_warm"][q] >= best - 1e-6
+    # off by default again, and the counters saw every node that reached the bundle
+    st = (C.c_longlong * 2)()
+    lib.bqb_warm_stats(st, 0)
+    assert res["warm"]["kept"] + res["warm"]["rejected"] <= 8
+
+
+@pytest.mark.gpu
+def test_shipped_model_against_plain_bundle(lib):
+    """What the trained network gains: full B&B on a held-out instance of
+    its family, plain bundle and warm-started bundle.  The optimum must be
+    identical and proposals must be used; the times, node counts and IPM
+    calls of both runs are printed (run with -s) for the record."""
+    p, meta = warm.load_model(warm.MODEL_C5)
+    assert len(p) == W.NPARAM
+    A = warm.c5_instance(60, 911)
+    out = {}
+    for mode in ("plain", "warm"):
+        warm.use_model(lib, p if mode == "warm" else None)
+        st = (C.c_longlong * 2)()
+        lib.bqb_warm_stats(st, 1)
+        r = _lib.solve(A, threads=16, time_limit=120)
+        lib.bqb_warm_stats(st, 1)
+        out[mode] = dict(opt=r["best_value"], nodes=r["nodes"], seconds=round(r["seconds"], 3), kept=int(st[0]),
+                         rejected=int(st[1]), stopped=r["stopped"])
+    warm.use_model(lib, None)
+    print(out)
+    assert not out["plain"]["stopped"] and not out["warm"]["stopped"]
+    assert out["warm"]["opt"] == out["plain"]["opt"]
+    assert out["plain"]["kept"] == 0 and out["warm"]["kept"] >= 1
