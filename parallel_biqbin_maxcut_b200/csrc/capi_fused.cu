@@ -216,6 +216,8 @@ void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int ra
     c.lb = P.lb.p;
     c.ipm_stats = ipm_stats_device();
     c.prof = F.prof.p;
+    c.warm_p = warm_device_params();
+    c.warm_stats = c.warm_p ? warm_device_stats() : nullptr;
     c.arena = P.arena.p;
     BQB_CUDA(cudaEventRecord(P.ev0, s));
     nk_launch(c, slots, s);

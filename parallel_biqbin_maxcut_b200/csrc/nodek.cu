@@ -39,6 +39,7 @@
 #include "kgon_sa.cuh"
 #include "nodek.h"
 #include "trisep.cuh"
+#include "warm_body.cuh"
 
 namespace bqb {
 
@@ -1146,6 +1147,57 @@ __device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter)
 }
 
 // ---------------------------------------------------------------------------
+// Learned warm start (warm.h): the network's proposal for the first-
+// separation cuts, evaluated once (L0 = L - B^T(gamma_w), one IPM into
+// bundle slot 0); kept, as the bundle's starting multipliers and X, when its
+// dual value is below f (the plain start's).  Returns the starting f.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ double nk_warm(const FusedCfg& c, Nk& k, double viol3, double gap, double f)
+{
+    const __nv_bfloat16* P = (const __nv_bfloat16*)c.warm_p;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = k.n, m = k.mt;
+    const size_t nn = (size_t)n * n;
+    // the objective's scale: mean |L_ij| over i != j
+    double a = 0.0;
+    for (size_t e = tid; e < nn; e += nt)
+        if (e % n != e / n) a += fabs(k.L[e]);
+    a = block_sum(a, nk_red);
+    const double sc = (n > 1 && a > 0.0) ? a / ((double)n * (n - 1)) : 1.0;
+    double sg = 0.0;
+    for (int q = tid; q < m; q += nt) {
+        int type, i, j, kk;
+        tri_decode(k.tricode[q], &type, &i, &j, &kk);
+        const double xij = k.X[i + (size_t)j * n], xik = k.X[i + (size_t)kk * n], xjk = k.X[j + (size_t)kk * n];
+        // the cut's violation as src/cutting_planes.c:20-39 evaluates it
+        const double v = type == 1   ? -xij - xik - xjk - 1.0
+                         : type == 2 ? -xij + xik + xjk - 1.0
+                         : type == 3 ? xij - xik + xjk - 1.0
+                                     : xij + xik - xjk - 1.0;
+        float xf[WARM_F];
+        warm_cut_features(type, i, j, kk, v, k.X, k.L, n, m, viol3, gap, sc, xf);
+        const double g = sc * (double)warm_mlp_bf16(xf, P);
+        k.gtest[q] = g;
+        sg += g;
+    }
+    sg = block_sum(sg, nk_red);
+    nk_opBt(c, k, k.gtest);
+    const int st0 = k.status;
+    const bool ok = nk_ipm(c, k, k.L0, k.Xb, nullptr);
+    const double fw = ok ? k.out[0] + sg : 0.0;
+    __syncthreads();
+    k.status = st0;   // a failed proposal is only rejected
+    const bool keep = ok && fw < f;
+    if (keep) {
+        for (int q = tid; q < m; q += nt) k.gam[q] = k.gtest[q];
+        for (size_t e = tid; e < nn; e += nt) k.X[e] = k.Xb[e];
+    }
+    __syncthreads();
+    if (tid == 0 && c.warm_stats) atomicAdd(&c.warm_stats[keep ? 0 : 1], 1ull);
+    return keep ? fw : f;
+}
+
+// ---------------------------------------------------------------------------
 // One node: SDPbound (src/bounding.c:24-342)
 // ---------------------------------------------------------------------------
 __device__ double nk_bound(const FusedCfg& c, Nk& k)
@@ -1186,6 +1238,7 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k)
         k.status |= NKS_BUNDLE_CAP;
         return 0.0;
     }
+    if (c.warm_p) f = nk_warm(c, k, viol3, bound - lb, f);
     for (size_t e = tid; e < nn; e += nt) k.Xb[e] = k.X[e];
     if (tid < BI_WORDS) k.istate[tid] = 0;
     __syncthreads();

@@ -71,6 +71,10 @@ struct FusedCfg {
     unsigned long long* lb;   // incumbent, order-preserving bits of a double
     double* ipm_stats;
     unsigned long long* prof;   // NKP_COUNT phase times (ns, summed over CTAs)
+    // learned warm start (warm.h): BF16 weights (null: off) and the
+    // {kept, rejected} proposal counters
+    const void* warm_p;
+    unsigned long long* warm_stats;
     // slot arena
     unsigned char* arena;
     size_t slot_bytes;

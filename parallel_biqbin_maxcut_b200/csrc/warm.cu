@@ -15,6 +15,7 @@
 
 #include "internal.h"
 #include "warm.h"
+#include "warm_body.cuh"
 
 namespace bqb {
 
@@ -22,7 +23,6 @@ namespace {
 
 constexpr int WT = 128;   // threads per block of the warm-start kernels
 
-__device__ __forceinline__ float warm_softplus(float z) { return z > 20.f ? z : log1pf(expf(z)); }
 __device__ __forceinline__ float warm_sigmoid(float z) { return 1.f / (1.f + expf(-z)); }
 
 // Scale of the node's objective: the mean |L_ij| over i != j (1 when
@@ -46,12 +46,7 @@ __global__ void warm_scale_kernel(const double* __restrict__ L, int n, double* _
     }
 }
 
-// Features of cut c (type, i, j, k), whose inequality is
-// s_ij X_ij + s_ik X_ik + s_jk X_jk <= 1 with the type's signs
-// (src/cutting_planes.c:20-39): its violation, the violation relative to
-// the largest, the largest, the three signed X entries (sorted), the
-// signed objective entries s L / scale (sorted), n / 128, log(1 + m) / 10
-// and log(1 + gap / scale).
+// Features of each cut (warm_cut_features), one thread per cut.
 __global__ void warm_feat_kernel(const int4* __restrict__ cut, const double* __restrict__ val, int m,
                                  const double* __restrict__ X, const double* __restrict__ L, int n, double viol3,
                                  double gap, const double* __restrict__ scale, float* __restrict__ F)
@@ -59,36 +54,7 @@ __global__ void warm_feat_kernel(const int4* __restrict__ cut, const double* __r
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m) return;
     const int4 q = cut[c];
-    // signs of (ij, ik, jk) for types 1..4
-    const double sij = (q.x == 3 || q.x == 4) ? 1.0 : -1.0;
-    const double sik = (q.x == 2 || q.x == 4) ? 1.0 : -1.0;
-    const double sjk = (q.x == 2 || q.x == 3) ? 1.0 : -1.0;
-    const size_t eij = q.y + (size_t)q.z * n, eik = q.y + (size_t)q.w * n, ejk = q.z + (size_t)q.w * n;
-    const double sc = *scale;
-    double x0 = sij * X[eij], x1 = sik * X[eik], x2 = sjk * X[ejk];
-    double l0 = sij * L[eij] / sc, l1 = sik * L[eik] / sc, l2 = sjk * L[ejk] / sc;
-    auto sort3 = [](double& a, double& b, double& d) {
-        double t;
-        if (a > b) t = a, a = b, b = t;
-        if (b > d) t = b, b = d, d = t;
-        if (a > b) t = a, a = b, b = t;
-    };
-    sort3(x0, x1, x2);
-    sort3(l0, l1, l2);
-    const double v = val[c];
-    float* f = F + (size_t)c * WARM_F;
-    f[0] = (float)v;
-    f[1] = (float)(viol3 > 1e-12 ? v / viol3 : 0.0);
-    f[2] = (float)viol3;
-    f[3] = (float)x0;
-    f[4] = (float)x1;
-    f[5] = (float)x2;
-    f[6] = (float)l0;
-    f[7] = (float)l1;
-    f[8] = (float)l2;
-    f[9] = (float)(n / 128.0);
-    f[10] = (float)(log1p((double)m) / 10.0);
-    f[11] = (float)log1p(fmax(gap, 0.0) / sc);
+    warm_cut_features(q.x, q.y, q.z, q.w, val[c], X, L, n, m, viol3, gap, *scale, F + (size_t)c * WARM_F);
 }
 
 // Inference with BF16 weights, FP32 arithmetic; one thread per cut.  The
@@ -98,26 +64,10 @@ __global__ void warm_infer_kernel(const float* __restrict__ F, int m, const __nv
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m) return;
-    const float* x = F + (size_t)c * WARM_F;
     float xf[WARM_F];
 #pragma unroll
-    for (int i = 0; i < WARM_F; ++i) xf[i] = x[i];
-    float h1[WARM_H];
-#pragma unroll
-    for (int h = 0; h < WARM_H; ++h) {
-        float a = __bfloat162float(P[WARM_OFF_B1 + h]);
-#pragma unroll
-        for (int i = 0; i < WARM_F; ++i) a = fmaf(xf[i], __bfloat162float(P[WARM_OFF_W1 + i * WARM_H + h]), a);
-        h1[h] = fmaxf(a, 0.f);
-    }
-    float z = __bfloat162float(P[WARM_OFF_B3]);
-    for (int h2 = 0; h2 < WARM_H; ++h2) {
-        float a = __bfloat162float(P[WARM_OFF_B2 + h2]);
-#pragma unroll
-        for (int h = 0; h < WARM_H; ++h) a = fmaf(h1[h], __bfloat162float(P[WARM_OFF_W2 + h * WARM_H + h2]), a);
-        z = fmaf(fmaxf(a, 0.f), __bfloat162float(P[WARM_OFF_W3 + h2]), z);
-    }
-    gam[c] = (scale ? *scale : 1.0) * (double)warm_softplus(z);
+    for (int i = 0; i < WARM_F; ++i) xf[i] = F[(size_t)c * WARM_F + i];
+    gam[c] = (scale ? *scale : 1.0) * (double)warm_mlp_bf16(xf, P);
 }
 
 __global__ void warm_to_bf16_kernel(const float* __restrict__ P, __nv_bfloat16* __restrict__ Q, int count)
@@ -239,6 +189,7 @@ struct WarmGlobal {
     std::atomic<bool> recording{false};
     std::vector<float> feats, targets;  // recorded training pairs
     std::atomic<long long> kept{0}, rejected{0};
+    DevBuf<unsigned long long> dstats;  // the fused kernel's {kept, rejected}
     // training buffers
     DevBuf<float> X, Y, P, G, M1, M2, H1, H2, dz, dH1, dH2, lossb, pf;
     DevBuf<int> idx;
@@ -358,6 +309,19 @@ void warm_record(const std::vector<float>& feats, double scale, const Triangle_I
 }
 
 void warm_count(bool kept) { (kept ? wg().kept : wg().rejected).fetch_add(1); }
+
+const void* warm_device_params() { return warm_active() ? (const void*)wg().pb.p : nullptr; }
+
+unsigned long long* warm_device_stats()
+{
+    WarmGlobal& g = wg();
+    std::lock_guard<std::mutex> lock(g.mu);
+    if (!g.dstats.p) {
+        g.dstats.ensure(2);
+        BQB_CUDA(cudaMemset(g.dstats.p, 0, 2 * sizeof(unsigned long long)));
+    }
+    return g.dstats.p;
+}
 
 }  // namespace bqb
 
@@ -502,12 +466,22 @@ BQB_API void bqb_warm_dataset_clear(void)
     g.targets.clear();
 }
 
-// out[2] = {proposals kept, proposals rejected} since the last reset.
+// out[2] = {proposals kept, proposals rejected} since the last reset (the
+// engines' and the fused kernel's).
 BQB_API void bqb_warm_stats(long long* out, int reset)
 {
     WarmGlobal& g = wg();
     out[0] = reset ? g.kept.exchange(0) : g.kept.load();
     out[1] = reset ? g.rejected.exchange(0) : g.rejected.load();
+    std::lock_guard<std::mutex> lock(g.mu);
+    if (g.dstats.p) {
+        unsigned long long d[2];
+        BQB_CUDA(cudaDeviceSynchronize());
+        BQB_CUDA(cudaMemcpy(d, g.dstats.p, sizeof d, cudaMemcpyDeviceToHost));
+        out[0] += (long long)d[0];
+        out[1] += (long long)d[1];
+        if (reset) BQB_CUDA(cudaMemset(g.dstats.p, 0, sizeof d));
+    }
 }
 
 // Sizes of the network: out[3] = {features, hidden units, parameters}.

@@ -77,5 +77,9 @@ void warm_record(const std::vector<float>& feats, double scale, const Triangle_I
                  const Triangle_Inequality* final_cuts, const double* final_gamma, int m_final);
 // Counters: proposals kept and proposals rejected (worse than the plain start).
 void warm_count(bool kept);
+// For the fused node kernel: the loaded model's device weights (BF16) when
+// the warm start is on, else null; device counters {kept, rejected}.
+const void* warm_device_params();
+unsigned long long* warm_device_stats();
 
 }  // namespace bqb

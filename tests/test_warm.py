@@ -158,3 +158,38 @@ def test_shipped_model_against_plain_bundle(lib):
     assert not out["plain"]["stopped"] and not out["warm"]["stopped"]
     assert out["warm"]["opt"] == out["plain"]["opt"]
     assert out["plain"]["kept"] == 0 and out["warm"]["kept"] >= 1
+
+
+@pytest.mark.gpu
+def test_fused_kernel_warm_start(lib):
+    """The fused node kernel runs the same proposal (features, BF16
+    network, one IPM, fallback): B&B optimum unchanged, proposals counted,
+    and its bounds on enumerable nodes are valid upper bounds."""
+    p, _ = warm.load_model(warm.MODEL_C5)
+    A = warm.c5_instance(60, 911)
+    plain = _lib.solve(A, fused_batch=64, fused_depth=2)
+    st = (C.c_longlong * 2)()
+    warm.use_model(lib, p)
+    try:
+        lib.bqb_warm_stats(st, 1)
+        r = _lib.solve(A, fused_batch=64, fused_depth=2)
+        lib.bqb_warm_stats(st, 1)
+        assert r["best_value"] == plain["best_value"]
+        assert st[0] + st[1] >= 1
+        B = warm.c5_instance(40, 104)
+        inst = warm.Instance(lib, B)
+        rng = np.random.default_rng(10)
+        nodes = (_lib.BabNode * 8)()
+        for q in range(8):
+            xf = np.ones(39, dtype=int)
+            xf[rng.choice(39, 8 + q % 3, replace=False)] = 0
+            nodes[q].xfixed[:39] = [int(v) for v in xf]
+            nodes[q].sol[:39] = [int(v) for v in rng.integers(0, 2, 39) * xf]
+        lib.bqb_reset_incumbent(C.c_double(-1e9))   # every node runs its bundle
+        b = np.zeros(8)
+        assert lib.bqb_bound_nodes_fused(nodes, 8, 1, _lib.dptr(b)) == 0, lib.bqb_last_error()
+        for q in range(8):
+            xf, sol = np.array(nodes[q].xfixed[:39]), np.array(nodes[q].sol[:39])
+            assert b[q] >= _best_completion(B, xf, sol) - 1e-6
+    finally:
+        warm.use_model(lib, None)
