@@ -66,7 +66,7 @@ WORKLOAD = "G(100,0.5) ±1 weights; 512 subproblems, k~U[0,40] fixed (n=60..100)
 FLOP_PER_ITER_N3 = 6.0
 # DRAM traffic of the fused kernel per node, measured with ncu on a small case
 # (16 nodes of a G(60, 0.5) +-1 instance: 1.39 MB in one launch).
-NODEK_DRAM_BYTES_PER_NODE = 1.39e6 / 16
+NODEK_DRAM_BYTES_PER_NODE = 1.95e6 / 16
 
 
 # Time-to-optimality instance: the batched configuration's graph itself,
@@ -422,19 +422,25 @@ def run_gpu(args):
         p_w, _ = warm.load_model(warm.MODEL_C5)
         A = warm.c5_instance(80, 913)
         learned = {"instance": "G(80,0.9), integer weights U[-10,10], seed 913 (held out from the model's "
-                               "training instances)", "call": "bqb_solve_parallel, 16 engines"}
-        for mode in ("plain", "warm"):
-            warm.use_model(arm.lib, p_w if mode == "warm" else None)
+                               "training instances)"}
+        runs = (("engines_plain", None, dict(threads=16)), ("engines_warm", p_w, dict(threads=16)),
+                ("fused_plain", None, dict(fused_batch=2 * arm.lib_sms(), fused_depth=4)),
+                ("fused_warm", p_w, dict(fused_batch=2 * arm.lib_sms(), fused_depth=4)))
+        for name, model, kw in runs:
+            warm.use_model(arm.lib, model)
             kst = (C.c_longlong * 2)()
             arm.lib.bqb_warm_stats(kst, 1)
             t0 = time.perf_counter()
-            r = _lib.solve(A, threads=16, time_limit=300)
-            learned[mode] = {"seconds": time.perf_counter() - t0, "optimum": r["best_value"], "nodes": r["nodes"]}
+            r = _lib.solve(A, time_limit=300, **kw)
+            learned[name] = {"seconds": time.perf_counter() - t0, "optimum": r["best_value"], "nodes": r["nodes"]}
             arm.lib.bqb_warm_stats(kst, 1)
-            learned[mode]["proposals_kept"] = int(kst[0])
-            learned[mode]["proposals_rejected"] = int(kst[1])
+            learned[name]["proposals_kept"] = int(kst[0])
+            learned[name]["proposals_rejected"] = int(kst[1])
         warm.use_model(arm.lib, None)
-        learned["speedup_warm_vs_plain"] = learned["plain"]["seconds"] / learned["warm"]["seconds"]
+        learned["call"] = "bqb_solve_parallel (16 engines) and bqb_solve_fused (batches of 2 x SMs, 4 in flight)"
+        learned["speedup_warm_vs_plain_engines"] = (learned["engines_plain"]["seconds"] /
+                                                    learned["engines_warm"]["seconds"])
+        learned["speedup_warm_vs_plain_fused"] = learned["fused_plain"]["seconds"] / learned["fused_warm"]["seconds"]
         arm.reset_problem()
 
     pk = peaks()
@@ -444,7 +450,7 @@ def run_gpu(args):
     peak = pk["bf16_tflops_sustained"]
     roof = {"kernel": "nodek_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": NODEK_DRAM_BYTES_PER_NODE * B,
-            "traffic_note": "DRAM bytes per launch: 87 KB per node from the ncu capture of a small case "
+            "traffic_note": "DRAM bytes per launch: 122 KB per node from the ncu capture of a small case "
                             "(profiles/nodek_kernel_G60_16nodes.md, n = 60) times the nodes of a launch",
             "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
                            f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
