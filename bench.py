@@ -245,6 +245,43 @@ def _dist():
     return ws, rank, local
 
 
+def rank_batches(rank: int, B: int, nsteps: int, n_sub: int):
+    """The subproblem indices rank `rank` bounds, as `nsteps` batches of B
+    (weak scaling: every rank has its own share, per-rank work fixed)."""
+    order = [(i * 7919 + rank * 131) % n_sub for i in range(B * nsteps)]
+    return [order[s * B:(s + 1) * B] for s in range(nsteps)]
+
+
+def make_collectives(pg, device: str, sync=None):
+    """barrier() and max_over_ranks(x) over the process group `pg` (None:
+    one process).  `sync` (e.g. torch.cuda.synchronize) runs on both sides
+    of the barrier; the tensors live on `device`."""
+    import torch
+
+    def barrier():
+        if sync:
+            sync()
+        if pg:
+            pg.barrier()
+        if sync:
+            sync()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
+def aggregate_rate(units_per_rank: int, world_size: int, ms_max: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time."""
+    return units_per_rank * world_size / (ms_max / 1e3)
+
+
 def run_gpu(args):
     import torch
     ws, rank, local = _dist()
@@ -261,22 +298,9 @@ def run_gpu(args):
     T = args.threads
     # rank r bounds its own share of the subproblems (weak scaling: per-GPU
     # work fixed); each step is a batch of B subproblems
-    order = [(i * 7919 + rank * 131) % N_SUB for i in range(B * (args.warmup + args.steps))]
-    batches = [order[s * B:(s + 1) * B] for s in range(args.warmup + args.steps)]
+    batches = rank_batches(rank, B, args.warmup + args.steps, N_SUB)
     timed = range(args.warmup, args.warmup + args.steps)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = make_collectives(pg, "cuda", torch.cuda.synchronize)
 
     def fused(arr):
         lib.bqb_reset_incumbent(arm.lb)   # every batch starts from the root's incumbent
@@ -341,8 +365,7 @@ def run_gpu(args):
     tot_cta_s = max(sum(prof), 1e-30)
     ms = span_ms
     ms_max = max_over_ranks(ms)
-    total_nodes = B * args.steps * ws
-    value = total_nodes / (ms_max / 1e3)
+    value = aggregate_rate(B * args.steps, ws, ms_max)
 
     # ---- e2e: the same C-ABI call from host node structs, every copy in
     # the timed region (events on the idle current stream around the call) ----
@@ -358,7 +381,7 @@ def run_gpu(args):
     ms_e2e = t0.elapsed_time(t1)
     barrier()
     ms_e2e = max_over_ranks(ms_e2e)
-    e2e = total_nodes / (ms_e2e / 1e3)
+    e2e = aggregate_rate(B * args.steps, ws, ms_e2e)
     b0 = batches[args.warmup]
     N = NV - 1
     h2d = B * 2 * N * 4 + 8
