@@ -176,11 +176,17 @@ def main():
     # 8. end-to-end optimal values of the reference's serial B&B
     e2e = []
     with tempfile.TemporaryDirectory() as td:
-        for kind, nv, seed in (("unit", 40, 1), ("unit", 60, 2), ("pm1", 40, 3), ("qubo", 30, 4)):
+        # the last four: the QUBO configuration at n = 100 (Max-Cut on 101
+        # vertices) and two held-out instances of the learned warm start's
+        # family, G(n, 0.9) with integer weights in [-10, 10]
+        for kind, nv, seed in (("unit", 40, 1), ("unit", 60, 2), ("pm1", 40, 3), ("qubo", 30, 4),
+                               ("qubo", 100, 1), ("qubo", 100, 2), ("int10", 60, 911), ("int10", 80, 913)):
             if kind == "unit":
                 A = instances.gnp_unit(nv, 0.5, seed)
             elif kind == "pm1":
                 A = instances.gnp_pm1(nv, 0.5, seed)
+            elif kind == "int10":
+                A = instances.gnp_int(nv, 0.9, 10, seed)
             else:
                 A = instances.qubo_to_maxcut(instances.qubo_dense(nv, 0.1, seed))
             inst, prm = os.path.join(td, "g.rudy"), os.path.join(td, "params")

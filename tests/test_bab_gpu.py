@@ -63,3 +63,32 @@ def test_bab_root_only_and_time_limit(lib):
     r = _lib.solve(A, root=1)
     assert r["nodes"] == 1
     assert r["root_bound"] >= r["best_value"]
+
+
+def _golden_optima():
+    import json
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bab_optima.json")) as fh:
+        return json.load(fh)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [c for c in _golden_optima() if c["nv"] >= 60 and c["kind"] in ("qubo", "int10")],
+                         ids=lambda c: f"{c['kind']}{c['nv']}-{c['seed']}")
+def test_fused_optimum_matches_reference_fixture(lib, case):
+    """The QUBO configuration at n = 100 and the learned family's held-out
+    instances: the fused-batch B&B (and, for the learned family, the fused
+    B&B with the shipped warm-start model) reaches the optimum the
+    reference's serial B&B printed (tests/golden/bab_optima.json)."""
+    from parallel_biqbin_maxcut_b200 import warm
+    A = _adj(case["kind"], case["nv"], case["seed"])
+    r = _lib.solve(A, fused_batch=296, fused_depth=4)
+    assert r["best_value"] == case["max_value"]
+    assert O.evaluateSolution(O.build_SP_L(A), r["x"]) == r["best_value"]
+    if case["kind"] == "int10":
+        p, _ = warm.load_model(warm.MODEL_C5)
+        warm.use_model(lib, p)
+        try:
+            rw = _lib.solve(A, fused_batch=296, fused_depth=4)
+        finally:
+            warm.use_model(lib, None)
+        assert rw["best_value"] == case["max_value"]
