@@ -299,6 +299,11 @@ void bqb_reset_incumbent(double value);
  * nodes, fused-kernel milliseconds (CUDA events), nodes bounded again by
  * engines, milliseconds of that}. */
 void bqb_fused_stats(double *out);
+/* Fused-kernel launches since the last bqb_fused_stats_reset: submissions
+ * made while a launch runs wait on the host and start together, as one
+ * launch with a heaviest-first order over all their nodes, at the next
+ * collect (or the next submission that finds the GPU idle). */
+long long bqb_fused_launches(void);
 void bqb_fused_stats_reset(void);
 /* Seconds spent per phase inside the fused kernel since the last reset,
  * summed over its CTAs: out[11] = {subproblem, IPM, heuristic, triangle

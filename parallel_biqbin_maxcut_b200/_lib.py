@@ -119,6 +119,7 @@ SIGNATURES = {
     "bqb_fused_stats": (None, [D]),
     "bqb_fused_stats_reset": (None, []),
     "bqb_fused_profile": (None, [D]),
+    "bqb_fused_launches": (C.c_longlong, []),
     "bqb_fused_phase_calls": (None, [C.POINTER(C.c_longlong)]),
     "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),

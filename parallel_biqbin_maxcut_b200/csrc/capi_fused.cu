@@ -13,7 +13,13 @@
 // Submissions go to a ring of NK_PIPES pipes, each with its own stream,
 // arena and buffers, so several launches are in flight at once: when the
 // last, heaviest nodes of one batch hold a few SMs, the next batch's CTAs
-// take the rest.  bqb_bound_nodes_fused is a submission collected at once.
+// take the rest.  A submission made while a launch is running waits on the
+// host; the next collect (or the next submission that finds the GPU idle)
+// launches every waiting submission as one kernel, whose node order is
+// heaviest-first over all of them, so the heavy nodes of later batches
+// start early instead of forming the tail of the last launch.  Each
+// submission is still collected on its own, in any order.
+// bqb_bound_nodes_fused is a submission collected at once.
 #include <string.h>
 
 #include <algorithm>
@@ -38,9 +44,15 @@ namespace {
 constexpr int NK_PIPES = 8;
 
 struct FusedPipe {
-    bool busy = false;
+    bool busy = false;       // holds an uncollected submission
+    bool launched = false;   // its nodes are in a launch (its own or a leader's)
+    int leader = -1;         // the pipe whose launch carries its nodes
+    int offset = 0;          // its first node in the leader's arrays
+    int refs = 0;            // (leader) uncollected submissions its launch carries
+    bool counted = false;    // (leader) launch time added to the statistics
     int count = 0, rank = 0, N = 0;
     unsigned long long ticket = 0;
+    HostBuf<int> gfix;       // (leader) the launch's fixings, all submissions
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf<unsigned char> arena;
@@ -65,6 +77,7 @@ struct FusedState {
     long long fallbacks = 0;
     std::vector<double> last_node_ms;
     double st_calls = 0, st_nodes = 0, st_kernel_ms = 0, st_fallback_nodes = 0, st_fallback_ms = 0;
+    long long st_launches = 0;
 };
 
 FusedState& fstate()
@@ -134,20 +147,46 @@ bool fused_supported(int N0, size_t smem_optin)
     return c.smem_bytes <= smem_optin;
 }
 
-// Launch a batch on pipe P (the caller holds F.mu).
-void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int rank)
+// Stage a submission on pipe P: its fixings go to P's pinned buffer (the
+// caller holds F.mu).
+void stage(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int rank)
 {
-    Runtime& R = rt();
-    const int N0 = SP->n;
-    const int N = N0 - 1;
+    const int N = SP->n - 1;
     if (!P.stream) {
         BQB_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
         BQB_CUDA(cudaEventCreate(&P.ev0));
         BQB_CUDA(cudaEventCreate(&P.ev1));
     }
+    const size_t cN = (size_t)count * N;
+    int* hf = P.hfix.ensure(2 * cN);
+    for (int i = 0; i < count; ++i) {
+        memcpy(hf + (size_t)i * N, nodes[i].xfixed, N * sizeof(int));
+        memcpy(hf + cN + (size_t)i * N, nodes[i].sol.X, N * sizeof(int));
+    }
+    P.busy = true;
+    P.launched = false;
+    P.leader = -1;
+    P.offset = 0;
+    P.count = count;
+    P.rank = rank;
+    P.N = N;
+    P.ticket = F.next_ticket++;
+}
+
+// One launch for the staged submissions `members` (pipe indices in ticket
+// order, same rank), carried by the first one's pipe (the caller holds F.mu).
+void launch(FusedState& F, const std::vector<int>& members)
+{
+    Runtime& R = rt();
+    const int N0 = SP->n;
+    const int N = N0 - 1;
+    FusedPipe& P = F.pipe[members[0]];
+    const int rank = P.rank;
+    int count = 0;
+    for (int q : members) count += F.pipe[q].count;
     cudaStream_t s = P.stream;
     FusedCfg c;
-    fill_cfg(c, N0, count, rank, F.seed + 0x9E3779B97F4A7C15ull * (F.next_ticket + 1), R.smem_optin);
+    fill_cfg(c, N0, count, rank, F.seed + 0x9E3779B97F4A7C15ull * (P.ticket + 1), R.smem_optin);
     const size_t slot_bytes = nk_layout(c);
     int slots = R.num_sms;
     if (slots > count) slots = count;
@@ -156,7 +195,7 @@ void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int ra
     if (F.P0L_src != SP->L || F.P0N != N0 || F.P0L_gen != gen) {
         // every pipe reads P0L: let the launches in flight finish first
         for (int q = 0; q < NK_PIPES; ++q)
-            if (F.pipe[q].busy) BQB_CUDA(cudaStreamSynchronize(F.pipe[q].stream));
+            if (F.pipe[q].refs > 0) BQB_CUDA(cudaStreamSynchronize(F.pipe[q].stream));
         F.P0L.ensure((size_t)N0 * N0);
         BQB_CUDA(cudaMemcpy(F.P0L.p, SP->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice));
         F.P0L_src = SP->L;
@@ -168,13 +207,22 @@ void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int ra
         BQB_CUDA(cudaMemset(F.prof.p, 0, 2 * NKP_COUNT * sizeof(unsigned long long)));
     }
     const size_t cN = (size_t)count * N;
-    int* hf = P.hfix.ensure(2 * cN);
+    int* hf = P.gfix.ensure(2 * cN);
+    int off = 0;
+    for (int q : members) {
+        FusedPipe& M = F.pipe[q];
+        const size_t mN = (size_t)M.count * N;
+        memcpy(hf + (size_t)off * N, M.hfix.p, mN * sizeof(int));
+        memcpy(hf + cN + (size_t)off * N, M.hfix.p + mN, mN * sizeof(int));
+        M.launched = true;
+        M.leader = members[0];
+        M.offset = off;
+        off += M.count;
+    }
     std::vector<int> ord(count), nfree(count);
     for (int i = 0; i < count; ++i) {
-        memcpy(hf + (size_t)i * N, nodes[i].xfixed, N * sizeof(int));
-        memcpy(hf + cN + (size_t)i * N, nodes[i].sol.X, N * sizeof(int));
         int nf = 0;
-        for (int j = 0; j < N; ++j) nf += nodes[i].xfixed[j] ? 0 : 1;
+        for (int j = 0; j < N; ++j) nf += hf[(size_t)i * N + j] ? 0 : 1;
         nfree[i] = nf;
         ord[i] = i;
     }
@@ -229,45 +277,82 @@ void submit(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int ra
     BQB_CUDA(cudaMemcpyAsync(P.hst.ensure(count), P.status.p, count * sizeof(int), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaMemcpyAsync(P.hns.ensure(count), P.node_ns.p, count * sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost, s));
-    P.busy = true;
-    P.count = count;
-    P.rank = rank;
-    P.N = N;
-    P.ticket = F.next_ticket++;
+    P.refs = (int)members.size();
+    P.counted = false;
+    ++F.st_launches;
+}
+
+// Launch the staged submissions: one launch per run of equal rank, in
+// ticket order (the caller holds F.mu).
+void launch_staged(FusedState& F)
+{
+    std::vector<int> st;
+    for (int q = 0; q < NK_PIPES; ++q)
+        if (F.pipe[q].busy && !F.pipe[q].launched) st.push_back(q);
+    std::sort(st.begin(), st.end(), [&](int a, int b) { return F.pipe[a].ticket < F.pipe[b].ticket; });
+    size_t i = 0;
+    while (i < st.size()) {
+        std::vector<int> group{st[i]};
+        size_t j = i + 1;
+        while (j < st.size() && F.pipe[st[j]].rank == F.pipe[st[i]].rank) group.push_back(st[j++]);
+        launch(F, group);
+        i = j;
+    }
+}
+
+// Is a launch still running on the GPU?
+bool any_running(FusedState& F)
+{
+    for (int q = 0; q < NK_PIPES; ++q) {
+        FusedPipe& L = F.pipe[q];
+        if (L.refs <= 0) continue;
+        const cudaError_t e = cudaEventQuery(L.ev1);
+        if (e == cudaErrorNotReady) return true;
+        if (e != cudaSuccess) BQB_CUDA(e);
+    }
+    return false;
 }
 
 // Wait for pipe P and hand its results to the caller's nodes (the caller
 // holds F.mu).
 int collect(FusedState& F, FusedPipe& P, BabNode* nodes, double* bounds)
 {
+    // submissions still waiting on the host start now, behind the launches
+    // in flight, so they run while this one is waited for
+    launch_staged(F);
+    FusedPipe& L = F.pipe[P.leader];
     cudaStream_t s = P.stream;
-    BQB_CUDA(cudaStreamSynchronize(s));
+    BQB_CUDA(cudaStreamSynchronize(L.stream));
     P.busy = false;
-    const int count = P.count, N = P.N;
-    float kms = 0.f;
-    BQB_CUDA(cudaEventElapsedTime(&kms, P.ev0, P.ev1));
+    --L.refs;
+    const int count = P.count, N = P.N, o = P.offset;
+    if (!L.counted) {
+        float kms = 0.f;
+        BQB_CUDA(cudaEventElapsedTime(&kms, L.ev0, L.ev1));
+        F.st_kernel_ms += kms;
+        L.counted = true;
+    }
     F.st_calls += 1;
     F.st_nodes += count;
-    F.st_kernel_ms += kms;
     F.last_node_ms.assign(count, 0.0);
-    for (int i = 0; i < count; ++i) F.last_node_ms[i] = 1e-6 * (double)P.hns.p[i];
+    for (int i = 0; i < count; ++i) F.last_node_ms[i] = 1e-6 * (double)L.hns.p[o + i];
 
     std::vector<int> redo;
     for (int i = 0; i < count; ++i) {
-        if (P.hst.p[i]) {
+        if (L.hst.p[o + i]) {
             redo.push_back(i);
             continue;
         }
-        bounds[i] = P.hb.p[i];
-        memcpy(nodes[i].fracsol, P.hfs.p + (size_t)i * N, N * sizeof(double));
+        bounds[i] = L.hb.p[o + i];
+        memcpy(nodes[i].fracsol, L.hfs.p + (size_t)(o + i) * N, N * sizeof(double));
     }
     // incumbent updates in node order (updateSolution's test and update)
     for (int i = 0; i < count; ++i) {
-        if (!(P.hhv.p[i] > Bab_LBGet())) continue;
+        if (!(L.hhv.p[o + i] > Bab_LBGet())) continue;
         BabSolution bs;
         memset(&bs, 0, sizeof bs);
-        memcpy(bs.X, P.hhs.p + (size_t)i * N, N * sizeof(int));
-        Bab_LBUpd(P.hhv.p[i], &bs);
+        memcpy(bs.X, L.hhs.p + (size_t)(o + i) * N, N * sizeof(int));
+        Bab_LBUpd(L.hhv.p[o + i], &bs);
     }
     if (!redo.empty()) {
         F.fallbacks += (long long)redo.size();
@@ -308,8 +393,11 @@ BQB_API long long bqb_fused_submit(const BabNode* nodes, int count, int rank)
     std::lock_guard<std::mutex> lock(F.mu);
     for (int q = 0; q < NK_PIPES; ++q) {
         FusedPipe& P = F.pipe[(F.next_ticket + q) % NK_PIPES];
-        if (P.busy) continue;
-        submit(F, P, nodes, count, rank);
+        if (P.busy || P.refs > 0) continue;   // free: collected and not carrying others' nodes
+        stage(F, P, nodes, count, rank);
+        // an idle GPU starts at once; otherwise the submission waits to be
+        // launched together with the others submitted meanwhile
+        if (!any_running(F)) launch_staged(F);
         return (long long)P.ticket;
     }
     set_error("bqb_fused_submit", "every pipe holds an uncollected submission");
@@ -357,6 +445,15 @@ BQB_API void bqb_fused_stats(double* out)
     out[4] = F.st_fallback_ms;
 }
 
+// Fused-kernel launches since the last bqb_fused_stats_reset (a launch
+// carries one submission or several that waited for it).
+BQB_API long long bqb_fused_launches(void)
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    return F.st_launches;
+}
+
 // Device milliseconds of every node of the last collected submission (as
 // many as it had, at most `count`); returns how many were written.
 BQB_API int bqb_fused_node_times(double* out, int count)
@@ -373,6 +470,7 @@ BQB_API void bqb_fused_stats_reset(void)
     FusedState& F = fstate();
     std::lock_guard<std::mutex> lock(F.mu);
     F.st_calls = F.st_nodes = F.st_kernel_ms = F.st_fallback_nodes = F.st_fallback_ms = 0;
+    F.st_launches = 0;
     if (F.prof.p) BQB_CUDA(cudaMemset(F.prof.p, 0, 2 * NKP_COUNT * sizeof(unsigned long long)));
 }
 

@@ -54,6 +54,9 @@ class Instance:
         SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
         PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
         C.CDLL("libc.so.6").srand(2020)
+        # a fresh incumbent (a cut of value 0 always exists), so the root's
+        # heuristic records its cut in babsol
+        lib.bqb_reset_incumbent(C.c_double(0.0))
         root = _lib.BabNode()
         self.root_bound = lib.Evaluate(C.byref(root), SP, PP, 0)
         self.lb = lib.Bab_LBGet()
