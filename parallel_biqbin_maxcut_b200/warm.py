@@ -171,11 +171,19 @@ def train(lib, feats, targets, steps=3000, batch=2048, lr=1e-3, seed=0, params=N
                             _lib.fptr(p), _lib.fptr(losses))
     assert rc == 0
     if standardize:
-        W1 = p[:F * H].reshape(F, H).astype(np.float64)
-        b1 = p[F * H:F * H + H].astype(np.float64)
-        p[F * H:F * H + H] = (b1 - (mu / sd) @ W1).astype(np.float32)
-        p[:F * H] = (W1 / sd[:, None]).astype(np.float32).ravel()
+        p = fold_standardization(p, mu, sd, F, H)
     return p, losses
+
+
+def fold_standardization(p, mu, sd, F, H):
+    """Parameters that take raw features x from parameters trained on
+    (x - mu) / sd: W1' = W1 / sd (by row), b1' = b1 - (mu / sd) W1."""
+    p = np.array(p, np.float32)
+    W1 = p[:F * H].reshape(F, H).astype(np.float64)
+    b1 = p[F * H:F * H + H].astype(np.float64)
+    p[F * H:F * H + H] = (b1 - (np.asarray(mu) / np.asarray(sd)) @ W1).astype(np.float32)
+    p[:F * H] = (W1 / np.asarray(sd)[:, None]).astype(np.float32).ravel()
+    return p
 
 
 def save_model(path, params, meta=None):

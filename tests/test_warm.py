@@ -193,3 +193,22 @@ def test_fused_kernel_warm_start(lib):
             assert b[q] >= _best_completion(B, xf, sol) - 1e-6
     finally:
         warm.use_model(lib, None)
+
+
+def test_standardization_folds_into_the_first_layer():
+    rng = np.random.default_rng(4)
+    X = (rng.standard_normal((50, W.F)) * 3 + 2).astype(np.float32)
+    mu, sd = X.mean(axis=0, dtype=np.float64), X.std(axis=0, dtype=np.float64)
+    p = warm.init_params(8, lib=_FakeDims())
+    q = warm.fold_standardization(p, mu, sd, W.F, W.H)
+    a, _ = W.forward(p, (X - mu) / sd)
+    b, _ = W.forward(q, X)
+    np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-6)
+
+
+def test_shipped_model_file():
+    p, meta = warm.load_model(warm.MODEL_C5)
+    assert p.dtype == np.float32 and len(p) == W.NPARAM and np.all(np.isfinite(p))
+    assert meta["train_instances"] and "command" in meta
+    g, _ = W.forward(p, np.zeros((3, W.F), np.float32))
+    assert np.all(g >= 0)
