@@ -250,6 +250,8 @@ BQB_API double Evaluate(BabNode* node, Problem* SP_, Problem* PP_, int rank)
 // ---- src/process_input.c:259-344 --------------------------------------------
 BQB_API int process_adj_matrix(double* Adj, int num_vertices)
 {
+    // fused submissions waiting on the host were made for the current problem
+    bqb::fused_launch_pending();
     BabPbSize = num_vertices - 1;
     ++bqb::g_sp_generation;
     if (!SP) SP = (Problem*)calloc(1, sizeof(Problem));

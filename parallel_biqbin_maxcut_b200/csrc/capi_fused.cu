@@ -378,6 +378,16 @@ int collect(FusedState& F, FusedPipe& P, BabNode* nodes, double* bounds)
 }
 
 }  // namespace
+
+// Launch every submission still waiting on the host: process_adj_matrix
+// calls this before it replaces the problem they were made for.
+void fused_launch_pending()
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    launch_staged(F);
+}
+
 }  // namespace bqb
 
 using namespace bqb;

@@ -87,4 +87,7 @@ void engine_destroy(Engine* e);
 // SDPbound (src/bounding.c:24-342) in engine E.
 double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank);
 
+// Launch the fused submissions still waiting on the host (capi_fused.cu).
+void fused_launch_pending();
+
 }  // namespace bqb

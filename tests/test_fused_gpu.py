@@ -115,6 +115,33 @@ def test_fused_submit_collect_pipelined(lib, solved):
 
 
 @pytest.mark.gpu
+def test_pending_submissions_survive_a_problem_change(lib, solved):
+    """Submissions made while a launch runs wait on the host; replacing the
+    problem (process_adj_matrix) first launches them for the problem they
+    were made for."""
+    A, r = solved
+    batches = [_nodes(24, 30, 60 + q) for q in range(3)]
+    singles = []
+    for b in batches:
+        c = _copy(b)
+        out = np.zeros(len(c))
+        assert lib.bqb_bound_nodes_fused(c, len(c), 1, _lib.dptr(out)) == 0
+        singles.append(out)
+    tickets = [lib.bqb_fused_submit(b, len(b), 1) for b in batches]
+    assert all(t >= 0 for t in tickets)
+    B = instances.gnp_unit(NV, 0.5, 77)
+    keep = np.ascontiguousarray(B, dtype=np.float64).copy()
+    lib.process_adj_matrix(_lib.dptr(keep), NV)      # a different problem, same size
+    outs = [np.zeros(len(b)) for b in batches]
+    for t, b, o in zip(tickets, batches, outs):
+        assert lib.bqb_fused_collect(t, b, _lib.dptr(o)) == 0
+    for o, s in zip(outs, singles):
+        np.testing.assert_array_equal(o, s)
+    # the module's problem back for the tests that follow
+    lib.process_adj_matrix(_lib.dptr(np.ascontiguousarray(A, dtype=np.float64).copy()), NV)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("kind,nv,seed", [("unit", 60, 2), ("pm1", 50, 4), ("qubo", 40, 6)])
 def test_fused_solve_optimum(lib, kind, nv, seed):
     """B&B with fused batches reaches the serial solver's optimum."""
