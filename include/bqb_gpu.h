@@ -424,6 +424,12 @@ long long bqb_warm_dataset(float *feats, float *targets, long long cap);
 void bqb_warm_dataset_clear(void);
 /* out[2] = {proposals kept, proposals rejected}; reset != 0 zeroes them. */
 void bqb_warm_stats(long long *out, int reset);
+/* The features of m triangle cuts (cuts: m x {type, i, j, k}, values: their
+ * violations) at X and the objective L (host, n x n column-major) into
+ * out[m x 12]; for checking against the oracle.  Returns 0, or -1 on bad
+ * arguments (an index outside 0..n-1, a type outside 1..4). */
+int bqb_warm_features(const double *X, const double *L, int n, const int *cuts, const double *values, int m,
+                      double viol3, double gap, float *out);
 
 #ifdef __cplusplus
 }

@@ -88,3 +88,28 @@ def bf16(a):
     u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
     r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
     return r.astype(np.uint32).view(np.float32)
+
+
+def features(X, L, cuts, values, viol3, gap):
+    """The per-cut features the GPU computes (csrc/warm_body.cuh), float64:
+    the violation v, v / viol3, viol3, the signed X entries of the cut's
+    inequality s_ij X_ij + s_ik X_ik + s_jk X_jk <= 1 (sorted), the signed
+    objective entries s L / scale (sorted; scale = mean |L_ij|, i != j),
+    n / 128, log(1 + m) / 10 and log(1 + gap / scale).  cuts: m x 4
+    (type, i, j, k)."""
+    X = np.asarray(X, dtype=np.float64)
+    L = np.asarray(L, dtype=np.float64)
+    n = X.shape[0]
+    m = len(cuts)
+    off = np.abs(L).sum() - np.abs(np.diag(L)).sum()
+    sc = off / (n * (n - 1)) if n > 1 and off > 0 else 1.0
+    signs = {1: (-1, -1, -1), 2: (-1, 1, 1), 3: (1, -1, 1), 4: (1, 1, -1)}
+    out = np.zeros((m, F))
+    for c, (t, i, j, k) in enumerate(cuts):
+        s = signs[int(t)]
+        xs = sorted([s[0] * X[i, j], s[1] * X[i, k], s[2] * X[j, k]])
+        ls = sorted([s[0] * L[i, j] / sc, s[1] * L[i, k] / sc, s[2] * L[j, k] / sc])
+        v = values[c]
+        out[c] = [v, v / viol3 if viol3 > 1e-12 else 0.0, viol3, *xs, *ls, n / 128.0, np.log1p(m) / 10.0,
+                  np.log1p(max(gap, 0.0) / sc)]
+    return out

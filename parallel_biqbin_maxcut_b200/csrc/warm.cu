@@ -491,3 +491,37 @@ BQB_API void bqb_warm_dims(int* out)
     out[1] = WARM_H;
     out[2] = WARM_NPARAM;
 }
+
+// The warm start's features of m triangle cuts (cuts: m x {type, i, j, k};
+// values: their violations) at X and the objective L (n x n, column-major,
+// host); out: m x 12 floats.  For tests against the oracle.
+BQB_API int bqb_warm_features(const double* Xh, const double* Lh, int n, const int* cuts, const double* values,
+                              int m, double viol3, double gap, float* out)
+{
+    if (!Xh || !Lh || !cuts || !values || !out || n <= 0 || m <= 0) return -1;
+    static WarmDev w;
+    static DevBuf<double> dX, dL;
+    WarmGlobal& g = wg();
+    std::lock_guard<std::mutex> lock(g.mu);
+    cudaStream_t s = rt().stream;
+    const size_t nn = (size_t)n * n;
+    BQB_CUDA(cudaMemcpyAsync(dX.ensure(nn), Xh, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaMemcpyAsync(dL.ensure(nn), Lh, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+    std::vector<Triangle_Inequality> t(m);
+    for (int c = 0; c < m; ++c) {
+        t[c].type = cuts[4 * c];
+        t[c].i = cuts[4 * c + 1];
+        t[c].j = cuts[4 * c + 2];
+        t[c].k = cuts[4 * c + 3];
+        t[c].value = values[c];
+        t[c].y = 0.0;
+        if (t[c].type < 1 || t[c].type > 4 || t[c].i < 0 || t[c].i >= n || t[c].j < 0 || t[c].j >= n || t[c].k < 0 ||
+            t[c].k >= n)
+            return -1;
+    }
+    warm_features(w, t.data(), m, dX.p, dL.p, n, viol3, gap, s);
+    std::vector<float> f;
+    warm_fetch_features(w, m, f, s);
+    memcpy(out, f.data(), f.size() * sizeof(float));
+    return 0;
+}

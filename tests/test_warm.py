@@ -212,3 +212,30 @@ def test_shipped_model_file():
     assert meta["train_instances"] and "command" in meta
     g, _ = W.forward(p, np.zeros((3, W.F), np.float32))
     assert np.all(g >= 0)
+
+
+@pytest.mark.gpu
+def test_gpu_features_match_oracle(lib):
+    from helpers import O, instances
+    A = instances.gnp_int(30, 0.9, 10, 5)
+    L = O.create_subproblem(O.build_SP_L(A), np.zeros(29, int), np.zeros(29, int))
+    n = L.shape[0]
+    rng = np.random.default_rng(3)
+    Xm = rng.uniform(-1, 1, (n, n))
+    Xm = 0.5 * (Xm + Xm.T)
+    np.fill_diagonal(Xm, 1.0)
+    cuts = []
+    for _ in range(40):
+        i, j, k = sorted(rng.choice(n, 3, replace=False), reverse=True)
+        cuts.append((int(rng.integers(1, 5)), int(i), int(j), int(k)))
+    values = rng.uniform(0.05, 0.9, len(cuts))
+    out = np.zeros((len(cuts), W.F), np.float32)
+    ci = np.ascontiguousarray(np.array(cuts, dtype=np.int32).ravel())
+    assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(ci),
+                                 _lib.dptr(values), len(cuts), 0.9, 12.5, _lib.fptr(out)) == 0
+    ref = W.features(Xm, L, cuts, values, 0.9, 12.5)
+    np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-6)
+    bad = ci.copy()
+    bad[1] = n   # index out of range: rejected before any device work
+    assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(bad),
+                                 _lib.dptr(values), len(cuts), 0.9, 12.5, _lib.fptr(out)) == -1
