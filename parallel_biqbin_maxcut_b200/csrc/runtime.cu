@@ -113,7 +113,7 @@ static void init_device(int dev)
     BQB_CUDA(cudaGetDeviceProperties(&prop, dev));
     if (prop.major < 10) {
         char buf[128];
-        snprintf(buf, sizeof buf, "device %s is sm_%d%d; this build targets sm_100a", prop.name,
+        snprintf(buf, sizeof buf, "device %s is sm_%d%d; libbqb_gpu is compiled for sm_100a", prop.name,
                  prop.major, prop.minor);
         fatal("bqb_init", buf);
         return;
