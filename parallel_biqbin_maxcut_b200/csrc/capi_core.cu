@@ -64,6 +64,10 @@ void check_ipm_status_host(const double* out)
 void ipm_device(DevBuf<double>& wsbuf, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
                 const int* xslot)
 {
+    if (n > IPM_REG_NMAX) {
+        ipm_large(wsbuf, dL, dX, n, dout, s, xslot);
+        return;
+    }
     size_t bytes = 0;
     const int place = ipm_place(n, rt().smem_optin, &bytes);
     double* ws = wsbuf.ensure(ipm_ws_doubles(n, place));

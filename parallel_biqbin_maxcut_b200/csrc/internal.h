@@ -18,6 +18,15 @@ namespace bqb {
 void ipm_device(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
                 const int* xslot = nullptr);
 
+// Largest n of the register-resident IPM body (RM_NMAX in reg_linalg.cuh);
+// ipm_device hands larger problems to ipm_large.
+constexpr int IPM_REG_NMAX = 128;
+
+// ipm_mc_pk for n > IPM_REG_NMAX as host-orchestrated multi-CTA kernels
+// (csrc/ipm_large.cu); same arguments and results as ipm_device.
+void ipm_large(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
+               const int* xslot);
+
 // Raise the reference's fatal error for a non-zero IPM status word.
 void check_ipm_status_host(const double* out);
 
