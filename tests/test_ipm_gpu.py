@@ -77,6 +77,34 @@ def test_ipm_large_torus(lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind,nv,seed", [("pm1", 129, 21), ("unit", 160, 22), ("int10", 200, 23)])
+def test_ipm_multi_cta_panel_edges(lib, kind, nv, seed):
+    """n > 128 runs as 32-column panels: a last panel of one column (129),
+    whole panels only (160), a ragged last panel (200)."""
+    L = root_L(_adj(kind, nv, seed))
+    X, phi = gpu_ipm(lib, L)
+    r = O.ipm_mc_pk(L)
+    assert abs(phi - r.phi) <= RTOL_PHI * abs(r.phi), (phi, r.phi)
+    assert np.max(np.abs(X - r.X)) <= ATOL_X
+    assert np.allclose(np.diag(X), 1.0, atol=1e-9)
+    assert np.array_equal(X, X.T)
+
+
+@pytest.mark.gpu
+def test_ipm_torus_subproblems_match_oracle(lib):
+    """Subproblems of the n = 343 torus (couplings ~1e5) after fixing up to
+    40 vertices."""
+    A = instances.torus3d(7, 1)
+    SPL = O.build_SP_L(A)
+    for xf, sol in instances.random_fixings(343, 2, 40, seed=24):
+        L = O.create_subproblem(SPL, xf, sol)
+        X, phi = gpu_ipm(lib, L)
+        r = O.ipm_mc_pk(L)
+        assert abs(phi - r.phi) <= RTOL_PHI * abs(r.phi)
+        assert np.max(np.abs(X - r.X)) <= 1e-5
+
+
+@pytest.mark.gpu
 @pytest.mark.skipif(not refbind.available(), reason="reference build absent")
 def test_ipm_matches_reference_build(lib):
     ref = refbind.RefLib()
