@@ -366,7 +366,8 @@ __global__ void wl_scale(const double* __restrict__ a, double alpha, int n, doub
     if (i < n) out[i] = alpha * a[i];
 }
 
-__global__ void wl_vadd(const double* __restrict__ a, const double* __restrict__ b, int n, double* __restrict__ c)
+// c = a + b elementwise; c may be a (no __restrict__ on a and c)
+__global__ void wl_vadd(const double* a, const double* __restrict__ b, int n, double* c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) c[i] = a[i] + b[i];
