@@ -15,7 +15,8 @@ import pytest
 from parallel_biqbin_maxcut_b200 import _lib, biqbin, instances
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_QUBO = "/root/reference/tests/qubos/40/kcluster40_025_10_1.json"
+REF_QUBOS = ["/root/reference/tests/qubos/40/kcluster40_025_10_1.json",
+             "/root/reference/tests/qubos/80/kcluster80_025_20_1.json"]
 
 
 def brute_maxcut(A):
@@ -111,13 +112,15 @@ def test_default_read_data_rudy(tmp_path):
         biqbin.default_read_data(str(tmp_path / "missing"))
 
 
-@pytest.mark.skipif(not os.path.exists(REF_QUBO), reason="reference test fixtures not present")
-def test_reference_qubo_fixture_conversion():
-    """The reference's shipped QUBO test (tests/qubos/40) read by our JSON
-    reader: its expected Max-Cut solution converts to its expected QUBO x,
-    whose value x'Qx is its expected QUBO value."""
-    Q = biqbin.read_json_qubo(REF_QUBO)
-    with open(REF_QUBO + "-expected_output.json") as fh:
+@pytest.mark.parametrize("path", REF_QUBOS)
+def test_reference_qubo_fixture_conversion(path):
+    """The reference's shipped QUBO tests (tests/qubos/40 and 80) read by our
+    JSON reader: the expected Max-Cut solution converts to the expected QUBO
+    x, whose value x'Qx is the expected QUBO value."""
+    if not os.path.exists(path):
+        pytest.skip("reference test fixtures not present")
+    Q = biqbin.read_json_qubo(path)
+    with open(path + "-expected_output.json") as fh:
         exp = json.load(fh)
     n = Q.shape[0]
     qsol, qx, mcx = biqbin.maxcut_to_qubo_solution(exp["maxcut"]["solution"], n)
@@ -128,6 +131,30 @@ def test_reference_qubo_fixture_conversion():
     x = np.array(mcx)
     cut = float(sum(A[i, j] for i in range(n + 1) for j in range(i + 1, n + 1) if x[i] != x[j]))
     assert cut * g == pytest.approx(exp["maxcut"]["computed_val"])
+
+
+def test_reference_qubo_fixture_through_reference_bab(tmp_path):
+    """tests/qubos/40 converted by our QUBO -> Max-Cut conversion and solved
+    by the reference build's own B&B: the expected Max-Cut value (its
+    tests/test.sh compares this line)."""
+    import re
+    import subprocess
+    from oracle import refbind
+    path = REF_QUBOS[0]
+    if not (os.path.exists(path) and refbind.available()):
+        pytest.skip("reference fixtures or build absent")
+    Q = biqbin.read_json_qubo(path)
+    with open(path + "-expected_output.json") as fh:
+        exp = json.load(fh)
+    A, g = biqbin.qubo_to_maxcut(Q)
+    inst, prm = tmp_path / "q.rudy", tmp_path / "params"
+    instances.write_rudy(str(inst), A)
+    with open("/root/reference/params") as fi:
+        prm.write_text(fi.read())
+    out = subprocess.run([refbind.REF_BAB, str(inst), str(prm)], capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, OPENBLAS_NUM_THREADS="1")).stdout
+    best = float(re.search(r"Maximum value = (\S+)", out).group(1))
+    assert best * g == pytest.approx(exp["maxcut"]["computed_val"])
 
 
 @pytest.mark.skipif(not os.path.exists("/root/reference/biqbin_base.py"), reason="reference Python layer not present")

@@ -106,7 +106,7 @@ def test_reference_build_reproduces_reference_fixtures():
         params = os.path.join(td, "params")
         with open("/root/reference/params") as fi, open(params, "w") as fo:
             fo.write(fi.read())
-        for name in ("g05_60.0",):
+        for name in ("g05_60.0", "g05_80.0", "g05_100.4"):
             inst = os.path.join(td, name)
             with open(os.path.join(src, name)) as fi, open(inst, "w") as fo:
                 fo.write(fi.read())
