@@ -7,6 +7,9 @@
         selected counters from `ncu -i report.ncu-rep --page raw --csv`
     python -m parallel_biqbin_maxcut_b200.profiling ipm <n> <repeats>
         bound the root of a G(n, 0.5) +-1 instance (IPM kernel case)
+    python -m parallel_biqbin_maxcut_b200.profiling ipm_torus <side> <repeats>
+        the same for the side^3-vertex 3D torus (side 7: n = 343, the
+        multi-CTA IPM case)
     python -m parallel_biqbin_maxcut_b200.profiling fused <n> <count> <kmax>
         bound `count` subproblems with the fused node kernel (nodek case)
 """
@@ -68,9 +71,11 @@ def summarize_raw(path: str) -> str:
     return "\n".join(out)
 
 
-def run_ipm(n_vertices: int, repeats: int) -> None:
-    """Bound the root of a seeded G(n, 0.5) +-1 instance `repeats` times
-    through ipm_mc_pk (a small, self-contained case for kernel profiling)."""
+def run_ipm(n_vertices: int, repeats: int, torus: bool = False) -> None:
+    """Bound the root of a seeded G(n, 0.5) +-1 instance (torus: of the
+    n x n x n 3D torus with Gaussian couplings x 1e5, seed 1) `repeats` times
+    through ipm_mc_pk (a small, self-contained case for kernel profiling;
+    above 128 vertices it runs the multi-CTA IPM)."""
     import ctypes as C
     import time
 
@@ -80,7 +85,7 @@ def run_ipm(n_vertices: int, repeats: int) -> None:
 
     lib = _lib.load()
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
-    A = instances.gnp_pm1(n_vertices, 0.5, seed=1)
+    A = instances.torus3d(n_vertices, 1) if torus else instances.gnp_pm1(n_vertices, 0.5, seed=1)
     nv = A.shape[0]
     lap = np.diag(A.sum(axis=1)) - A
     L = np.zeros((nv, nv))
@@ -137,6 +142,8 @@ if __name__ == "__main__":
     mode = sys.argv[1]
     if mode == "ipm":
         run_ipm(int(sys.argv[2]), int(sys.argv[3]))
+    elif mode == "ipm_torus":
+        run_ipm(int(sys.argv[2]), int(sys.argv[3]), torus=True)
     elif mode == "fused":
         run_fused(int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]))
     else:
