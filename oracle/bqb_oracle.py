@@ -517,6 +517,79 @@ def lambda_eta(zeta, G, gamma, t):
             return dgamma, lam, eta, t
 
 
+MAX_BUNDLE = 400   # MaxBundle, src/biqbin.h:42
+
+
+def bundle_inner(L: np.ndarray, X: np.ndarray) -> float:
+    """<L, X> over the upper triangle, off-diagonal terms doubled, column by
+    column (src/bundle.c:150-160, src/bounding.c:143-152)."""
+    n = L.shape[0]
+    temp = 0.0
+    for i in range(n):
+        temp += L[i, i] * X[i, i] + float(np.sum(2.0 * L[i + 1:, i] * X[i + 1:, i]))
+    return temp
+
+
+@dataclass
+class Bundle:
+    """The bundle: F[k] = <L, X_i>, G (m x k) subgradients, Xb the k primal
+    matrices, in the reference's slot order (src/bundle.c:14-17)."""
+    F: np.ndarray
+    G: np.ndarray
+    Xb: list
+
+    @property
+    def k(self) -> int:
+        return len(self.F)
+
+
+def bundle_method(L: np.ndarray, cuts: Cuts, gamma: np.ndarray, f: float, X: np.ndarray, bundle: Bundle,
+                  t: float, bdl_iter: int):
+    """bdl_iter proximal bundle iterations (src/bundle.c:9-239).  Returns
+    (gamma, f, X, bundle, t); the inputs are not modified.
+
+    Per iteration: zeta = -F - G'gamma; (dgamma, lambda) from lambda_eta;
+    f_test = fct_eval(gamma + dgamma); del = f - (F + G'gamma_test)'lambda;
+    a serious step (f - f_test > 0.05 del) moves gamma, sets X = Xb lambda,
+    t *= 1.01, drops the elements with lambda < 0.01 max(lambda) and appends
+    the new one; a null step keeps gamma and X, t /= 1.01, purges the first
+    k - 1 elements the same way and keeps the last one after the new one."""
+    gamma = np.array(gamma, dtype=np.float64, copy=True)
+    X = np.array(X, dtype=np.float64, copy=True)
+    F = np.array(bundle.F, dtype=np.float64, copy=True)
+    G = np.array(bundle.G, dtype=np.float64, copy=True)
+    Xb = [np.array(x, dtype=np.float64, copy=True) for x in bundle.Xb]
+    for _ in range(bdl_iter):
+        k = len(F)
+        zeta = -F - G.T @ gamma                                  # :54-61
+        dgamma, lam, _eta, t = lambda_eta(zeta, G, gamma, t)     # :64
+        gamma_test = gamma + dgamma                              # :67-68
+        f_test, X_test, g = fct_eval(L, cuts, gamma_test)        # :71
+        dl = f - float((F + G.T @ gamma_test) @ lam)             # :74-81
+        lmax = float(np.max(lam))                                # :84-86
+        F_new = bundle_inner(L, X_test)
+        if f - f_test > 0.05 * dl:                               # :91 serious step
+            gamma = gamma_test
+            f = f_test
+            X = sum(lam[i] * Xb[i] for i in range(k))            # :106-108
+            t *= 1.01
+            keep = [i for i in range(k) if not lam[i] < 0.01 * lmax]
+            if len(keep) == MAX_BUNDLE:
+                raise RuntimeError("Bundle size too large")
+            F = np.concatenate([F[keep], [F_new]])
+            G = np.concatenate([G[:, keep], g[:, None]], axis=1)
+            Xb = [Xb[i] for i in keep] + [X_test]
+        else:                                                    # :169 null step
+            t /= 1.01
+            keep = [i for i in range(k - 1) if not lam[i] < 0.01 * lmax]
+            if len(keep) + 1 == MAX_BUNDLE:
+                raise RuntimeError("Bundle size too large")
+            F = np.concatenate([F[keep], [F_new, F[k - 1]]])
+            G = np.concatenate([G[:, keep], g[:, None], G[:, k - 1:k]], axis=1)
+            Xb = [Xb[i] for i in keep] + [X_test, Xb[k - 1]]
+    return gamma, f, X, Bundle(F, G, Xb), t
+
+
 # --------------------------------------------------------------------------
 # Instance construction (src/process_input.c:259-344, src/evaluate.c:38-138)
 # --------------------------------------------------------------------------

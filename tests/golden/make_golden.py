@@ -173,6 +173,9 @@ def main():
 
     np.savez_compressed(os.path.join(HERE, "components.npz"), **out)
 
+    # 9. bundle_method on the root of SP
+    bundle_golden(ref, SPL)
+
     # 8. end-to-end optimal values of the reference's serial B&B
     e2e = []
     with tempfile.TemporaryDirectory() as td:
@@ -200,7 +203,65 @@ def main():
                         "root_bound": float(re.search(r"Root node bound = (\S+)", txt).group(1))})
     with open(os.path.join(HERE, "bab_optima.json"), "w") as fh:
         json.dump(e2e, fh, indent=1)
-    print("wrote", os.path.join(HERE, "components.npz"), "and bab_optima.json")
+    print("wrote components.npz, bundle.npz and bab_optima.json in", HERE)
+
+
+def bundle_golden(ref, SPL):
+    """The root of SP after the first triangle separation, the bundle set up
+    as SDPbound does (src/bounding.c:120-157), then three calls of
+    bundle_method with 4 iterations each, the third with t x 200 (null
+    steps); the state after each call goes to bundle.npz."""
+    N0 = SPL.shape[0]
+    L = O.create_subproblem(SPL, np.zeros(N0 - 1, np.int32), np.zeros(N0 - 1, np.int32))
+    n = L.shape[0]
+    ref.set_param("TriIneq", 3 * n)
+    ref.set_param("violated_TriIneq", 0.05)
+    PP = C.POINTER(refbind.Problem).in_dll(ref.lib, "PP")
+    pp = PP.contents
+    Lc = colmajor(L)
+    for q in range(n * n):
+        pp.L[q] = Lc[q]
+    pp.n, pp.NIneq, pp.NPentIneq, pp.NHeptaIneq = n, 0, 0, 0
+    Xr, phi = ref.ipm(L)
+    gX = ref.gptr("X", C.c_double)
+    Xc = colmajor(Xr)
+    for q in range(n * n):
+        gX[q] = Xc[q]
+    gamma = ref.gptr("dual_gamma", C.c_double)
+    added, subtracted = C.c_int(), C.c_int()
+    viol3 = ref.lib.updateTriangleInequalities(PP, gamma, C.byref(added), C.byref(subtracted))
+    m = pp.NIneq
+    cuts = ref.gptr("Cuts", refbind.TriIneq)
+    tri = np.array([(cuts[c].i, cuts[c].j, cuts[c].k) for c in range(m)], np.int32).reshape(-1, 3)
+    tri_type = np.array([cuts[c].type for c in range(m)], np.int32)
+    for c in range(m):
+        gamma[c] = cuts[c].y
+    g = np.ones(m)
+    ref.lib.op_B(PP, refbind.dptr(g), refbind.dptr(Xc))
+    F0 = O.bundle_inner(L, Xr)
+    gF, gG, gXb = ref.gptr("F", C.c_double), ref.gptr("G", C.c_double), ref.gptr("X_bundle", C.c_double)
+    gF[0] = F0
+    for c in range(m):
+        gG[c] = g[c]
+    for q in range(n * n):
+        gXb[q] = Xc[q]
+    pp.bundle = 1
+    C.c_double.in_dll(ref.lib, "f").value = phi
+    t = C.c_double(0.5 * 2.0 / (m * viol3 * viol3))   # a gap of 2 to the incumbent
+    out = dict(L=L, tri=tri, tri_type=tri_type, gamma0=np.array([gamma[c] for c in range(m)]), f0=np.array([phi]),
+               X0=Xr, F0=np.array([F0]), G0=g[:, None].copy(), t0=np.array([t.value]))
+    for call in (1, 2, 3):
+        if call == 3:
+            t.value *= 200.0   # steps far too long: null steps
+        ref.lib.bundle_method(PP, C.byref(t), 4)
+        k = pp.bundle
+        out[f"b{call}_f"] = np.array([C.c_double.in_dll(ref.lib, "f").value])
+        out[f"b{call}_gamma"] = np.array([gamma[c] for c in range(m)])
+        out[f"b{call}_X"] = from_col([gX[q] for q in range(n * n)], n)
+        out[f"b{call}_F"] = np.array([gF[i] for i in range(k)])
+        out[f"b{call}_G"] = np.array([gG[q] for q in range(m * k)]).reshape(k, m).T.copy()
+        out[f"b{call}_t"] = np.array([t.value])
+    np.savez_compressed(os.path.join(HERE, "bundle.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -69,6 +69,30 @@ def test_bundle_qp_matches_golden():
     assert t == G["le_tout"][0]
 
 
+def test_bundle_method_matches_golden():
+    """Three calls of 4 bundle iterations from the state SDPbound sets up at
+    the root (src/bounding.c:120-157): serious steps, then, with t x 200,
+    null steps and a lambda_eta that runs into its 50-round limit.  The QP
+    inside agrees to ~1e-8, the IPM to ~1e-12; the tolerances cover that,
+    and every discrete decision (serious or null step, purge) must agree for
+    F to have the reference's length."""
+    B = np.load(os.path.join(HERE, "golden", "bundle.npz"))
+    cuts = O.Cuts(tri=B["tri"], tri_type=B["tri_type"])
+    bundle = O.Bundle(F=B["F0"], G=B["G0"], Xb=[B["X0"]])
+    gamma, f, X, t = B["gamma0"], float(B["f0"][0]), B["X0"], float(B["t0"][0])
+    for call in (1, 2, 3):
+        if call == 3:
+            t *= 200.0
+        gamma, f, X, bundle, t = O.bundle_method(B["L"], cuts, gamma, f, X, bundle, t, 4)
+        assert bundle.k == len(B[f"b{call}_F"])
+        assert abs(f - B[f"b{call}_f"][0]) <= 1e-7 * abs(f)
+        assert t == pytest.approx(B[f"b{call}_t"][0], rel=1e-12)
+        np.testing.assert_allclose(gamma, B[f"b{call}_gamma"], rtol=0, atol=1e-6)
+        np.testing.assert_allclose(X, B[f"b{call}_X"], rtol=0, atol=1e-6)
+        np.testing.assert_allclose(bundle.F, B[f"b{call}_F"], rtol=1e-7, atol=1e-7)
+        np.testing.assert_allclose(bundle.G, B[f"b{call}_G"], rtol=0, atol=1e-6)
+
+
 def test_subproblem_construction_consistent():
     """createSubproblem / getFixedValue restated: the subproblem objective
     plus the fixed value equals the full objective for every completion."""
