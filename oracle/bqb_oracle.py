@@ -590,6 +590,132 @@ def bundle_method(L: np.ndarray, cuts: Cuts, gamma: np.ndarray, f: float, X: np.
     return gamma, f, X, Bundle(F, G, Xb), t
 
 
+@dataclass
+class BoundResult:
+    """What SDPbound leaves behind: the bound it returns, the incumbent
+    value and cut (Bab_LBGet / BabSol after its updateSolution calls), the
+    node's fracsol, and diff (set at the root, rank 0)."""
+    bound: float
+    lb: float
+    best_x: np.ndarray
+    fracsol: np.ndarray
+    diff: float
+    outer_iterations: int
+    prune: bool
+    giveup: bool
+
+
+def _fracsol(X, xfixed, sol, N):
+    """Fixed variables keep their value, free ones 0.5 (X[n-1, i] + 1)
+    (src/bounding.c:76-87, 246-257)."""
+    n = X.shape[0]
+    out = np.zeros(N)
+    idx = 0
+    for i in range(N):
+        if xfixed[i]:
+            out[i] = float(sol[i])
+        else:
+            out[i] = 0.5 * (X[n - 1, idx] + 1.0)
+            idx += 1
+    return out
+
+
+def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: int = 1,
+             diff: float = 0.0) -> BoundResult:
+    """The node bound (src/bounding.c:24-342) with triangle cuts only: the
+    pentagonal and heptagonal separations are not restated here, so
+    prm["include_Pent"] and prm["include_Hepta"] must be 0.
+
+    prm holds the reference's parameters (init_bundle_iter, max_bundle_iter,
+    triag_iter, pent_iter, hept_iter, max_outer_iter, extra_iter,
+    violated_TriIneq, TriIneq after adjust_TriIneq, use_diff).  lb / best_x:
+    the incumbent (Bab_LBGet / BabSol) before the call; diff: the global
+    diff.  The heuristic draws from rand() in the reference's order, so call
+    srand() first to reproduce a run."""
+    if prm.get("include_Pent", 0) or prm.get("include_Hepta", 0):
+        raise ValueError("the oracle's SDPbound covers triangle cuts only")
+    N = SP_L.shape[0] - 1
+    xfixed = np.asarray(xfixed[:N])
+    sol = np.asarray(sol[:N])
+    best_x = np.array(best_x[:N], dtype=np.int64, copy=True)
+    L = create_subproblem(SP_L, xfixed, sol)
+    fixedvalue = fixed_value(SP_L, xfixed, sol)                  # :60
+    cuts = Cuts()
+    r = ipm_mc_pk(L)                                             # :73
+    X, f = r.X, r.phi
+    basic_bound = f + fixedvalue
+    fracsol = _fracsol(X, xfixed, sol, N)
+
+    def heuristic(Xcur, lb, best_x):                             # :90-103, :182-195
+        x = np.where(xfixed != 0, sol, 0).astype(np.int64)
+        runHeuristic_unpacked(SP_L, L, xfixed, sol, x, Xcur)
+        val = evaluateSolution(SP_L, x)
+        if val > lb:                                             # Bab_LBUpd, src/heap.c:185-193
+            return val, x.copy()
+        return lb, best_x
+
+    lb, best_x = heuristic(X, lb, best_x)
+    bound = f + fixedvalue
+    if bound < lb + 1.0:                                         # :109
+        return BoundResult(bound, lb, best_x, fracsol, diff, 0, True, False)
+    if prm["use_diff"] and rank != 0 and bound > lb + diff + 1.0:   # :115
+        return BoundResult(bound, lb, best_x, fracsol, diff, 0, False, True)
+
+    tri, ttype, gamma, _, _, viol3 = updateTriangleInequalities(cuts, np.zeros(0), X, int(prm["TriIneq"]),
+                                                                 float(prm["violated_TriIneq"]))   # :120
+    cuts = Cuts(tri=tri, tri_type=ttype)
+    m = cuts.m
+    t = 0.5 * (bound - lb) / (m * viol3 * viol3)                 # :133
+    g = op_B(cuts, np.ones(m), X)                                # :138-139
+    bundle = Bundle(F=np.array([bundle_inner(L, X)]), G=g[:, None].copy(), Xb=[X.copy()])
+
+    bdl_iter = int(prm["init_bundle_iter"])
+    count = 0
+    prune = giveup = False
+    while True:
+        count += 1                                               # :168-172
+        oldf = f
+        gamma, f, X, bundle, t = bundle_method(L, cuts, gamma, f, X, bundle, t, bdl_iter)
+        bound = f + fixedvalue
+        prune = bound < lb + 1.0
+        if not prune:
+            lb, best_x = heuristic(X, lb, best_x)
+            prune = bound < lb + 1.0
+        gap = bound - lb
+        if count == prm["triag_iter"] + prm["pent_iter"] + prm["hept_iter"]:     # :201-205
+            if gap - 1.0 > (oldf - f) * (prm["max_outer_iter"] - count):
+                giveup = True
+        if count == prm["max_outer_iter"]:                       # :208-211
+            if gap - 1.0 > (oldf - f) * prm["extra_iter"]:
+                giveup = True
+        if count == prm["max_outer_iter"] + prm["extra_iter"]:   # :214-215
+            giveup = True
+        if not prune and not giveup:                             # :219-230
+            tri, ttype, gamma, _, _, viol3 = updateTriangleInequalities(cuts, gamma, X, int(prm["TriIneq"]),
+                                                                         float(prm["violated_TriIneq"]))
+            cuts = Cuts(tri=tri, tri_type=ttype)
+        done = prune or giveup
+        fracsol = _fracsol(X, xfixed, sol, N)                    # :246-257
+        if not done:                                             # :260-315
+            m = cuts.m
+            _, X_test, g = fct_eval(L, cuts, gamma)
+            k = bundle.k
+            G = np.column_stack([op_B(cuts, np.ones(m), bundle.Xb[i]) for i in range(k)] + [g])
+            if k == MAX_BUNDLE:
+                raise RuntimeError("Bundle size too large")
+            bundle = Bundle(F=np.concatenate([bundle.F, [bundle_inner(L, X_test)]]), G=G,
+                            Xb=bundle.Xb + [X_test])
+            t *= 1.05
+        bdl_iter += count % 2                                    # :320-321
+        bdl_iter = min(bdl_iter, int(prm["max_bundle_iter"]))
+        if done:
+            break
+    bound = f + fixedvalue
+    if rank == 0:
+        diff = basic_bound - bound                               # :328-329
+    return BoundResult(bound, lb, best_x, fracsol, diff, count, prune, giveup)
+
+
 # --------------------------------------------------------------------------
 # Instance construction (src/process_input.c:259-344, src/evaluate.c:38-138)
 # --------------------------------------------------------------------------

@@ -173,8 +173,10 @@ def main():
 
     np.savez_compressed(os.path.join(HERE, "components.npz"), **out)
 
-    # 9. bundle_method on the root of SP
+    # 9. bundle_method on the root of SP; 10. SDPbound (its own process: the
+    #    reference's globals are sized once per process)
     bundle_golden(ref, SPL)
+    subprocess.run([sys.executable, os.path.abspath(__file__), "--sdpbound"], check=True)
 
     # 8. end-to-end optimal values of the reference's serial B&B
     e2e = []
@@ -203,7 +205,7 @@ def main():
                         "root_bound": float(re.search(r"Root node bound = (\S+)", txt).group(1))})
     with open(os.path.join(HERE, "bab_optima.json"), "w") as fh:
         json.dump(e2e, fh, indent=1)
-    print("wrote components.npz, bundle.npz and bab_optima.json in", HERE)
+    print("wrote components.npz, bundle.npz, sdpbound.npz and bab_optima.json in", HERE)
 
 
 def bundle_golden(ref, SPL):
@@ -264,5 +266,64 @@ def bundle_golden(ref, SPL):
     np.savez_compressed(os.path.join(HERE, "bundle.npz"), **out)
 
 
+SDP_PARAMS = {"init_bundle_iter": 5, "max_bundle_iter": 15, "triag_iter": 5, "pent_iter": 5, "hept_iter": 5,
+              "max_outer_iter": 20, "extra_iter": 10, "violated_TriIneq": 0.05, "use_diff": 1,
+              "include_Pent": 0, "include_Hepta": 0}
+
+
+def sdpbound_golden():
+    """SDPbound (src/bounding.c:24-342) with triangle cuts only, as Evaluate
+    runs it, on G(50, 0.9) with integer weights in [-10, 10] (seed 4): the
+    root at rank 0 with max_outer_iter = 7 and extra_iter = 0 (it gives up
+    after 7 outer iterations), the root with the default limits (it gives up
+    at outer iteration 15 and sets diff), then four subproblems at rank 1
+    from the incumbent the calls before left, the last with diff forced to
+    0.5 (the use_diff give-up), each from a fixed rand() state.  Inputs and
+    results go to sdpbound.npz."""
+    ref = refbind.RefLib()
+    prm = dict(SDP_PARAMS)
+    ref.setup(instances.gnp_int(50, 0.9, 10, 4), prm)
+    SPL = ref.SP_L()
+    N0 = SPL.shape[0]
+    N = N0 - 1
+    prm["TriIneq"] = ref.param("TriIneq")   # adjust_TriIneq: 10 SP->n
+    PP = C.POINTER(refbind.Problem).in_dll(ref.lib, "PP")
+    SP = C.POINTER(refbind.Problem).in_dll(ref.lib, "SP")
+    babsol = C.POINTER(C.c_int).in_dll(ref.lib, "BabSol")
+    root = (np.zeros(N, np.int32), np.zeros(N, np.int32))
+    cases = [root + (0, 7, 0), root + (0, prm["max_outer_iter"], prm["extra_iter"])]
+    cases += [(xf, sol, 1, prm["max_outer_iter"], prm["extra_iter"])
+              for xf, sol in instances.random_fixings(N0, 4, 6, seed=31)]
+    out = {"SPL": SPL, "params": np.array([prm[k] for k in sorted(prm)]),
+           "param_names": np.array(sorted(prm))}
+    for q, (xf, sol, rank, max_outer, extra) in enumerate(cases):
+        ref.set_param("max_outer_iter", max_outer)
+        ref.set_param("extra_iter", extra)
+        out[f"c{q}_limits"] = np.array([max_outer, extra])
+        node = refbind.BabNode()
+        node.xfixed[:N] = [int(v) for v in xf]
+        node.sol[:N] = [int(v) for v in sol]
+        out[f"c{q}_xfixed"], out[f"c{q}_sol"], out[f"c{q}_rank"] = xf, sol, np.array([rank])
+        if q == len(cases) - 1:
+            ref.lib.bqbref_set_diff(0.5)
+        out[f"c{q}_lb_in"] = np.array([ref.lib.Bab_LBGet()])
+        out[f"c{q}_best_in"] = np.array([babsol[i] for i in range(N)], np.int32)
+        out[f"c{q}_diff_in"] = np.array([ref.lib.bqbref_get_diff()])
+        libc.srand(500 + q)
+        ref.lib.createSubproblem(C.byref(node), SP, PP)
+        bound = ref.lib.SDPbound(C.byref(node), SP, PP, rank)
+        out[f"c{q}_bound"] = np.array([bound])
+        out[f"c{q}_lb_out"] = np.array([ref.lib.Bab_LBGet()])
+        out[f"c{q}_best_out"] = np.array([babsol[i] for i in range(N)], np.int32)
+        out[f"c{q}_fracsol"] = np.array(node.fracsol[:N])
+        out[f"c{q}_diff_out"] = np.array([ref.lib.bqbref_get_diff()])
+        out[f"c{q}_rand_after"] = np.array([libc.rand()])
+    out["ncases"] = np.array([len(cases)])
+    np.savez_compressed(os.path.join(HERE, "sdpbound.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["--sdpbound"]:
+        sdpbound_golden()
+    else:
+        main()
