@@ -590,6 +590,76 @@ def bundle_method(L: np.ndarray, cuts: Cuts, gamma: np.ndarray, f: float, X: np.
     return gamma, f, X, Bundle(F, G, Xb), t
 
 
+MAX_KGON_ADDED = 50000   # MaxPentIneqAdded, MaxHeptaIneqAdded, src/biqbin.h:38-39
+
+
+def getViolated_KgonalInequalities(X: np.ndarray, k: int, trials: int, cap: int):
+    """Pentagonal (k = 5, types 1-3) or heptagonal (k = 7, types 1-4)
+    separation (src/cutting_planes.c:223-301 and its heptagonal twin): for
+    each trial and type one annealing chain (the C restatement in
+    oracle/kgon_sa_chain.c, drawing from rand() with the reference's flags);
+    values below 1 fill a list of at most `cap`, beyond which a more violated
+    one replaces the tracked least violated entry.  Returns (list of
+    (type, permutation, value), the smallest chain value).
+
+    The reference's re-scan after a replacement starts from BIG_NUMBER and
+    looks for a larger value, so it never moves the tracked entry again;
+    this is kept."""
+    from . import portbind
+    types = 3 if k == 5 else 4
+    n = X.shape[0]
+    Xc = np.ascontiguousarray(np.asarray(X, dtype=np.float64).T).reshape(-1)
+    lst = []
+    least_idx, least_val, min_all = 0, -BIG_NUMBER, BIG_NUMBER
+    for _ in range(trials):
+        for typ in range(1, types + 1):
+            v, perm = portbind.qap_sa_glibc(Xc, n, k, typ)
+            min_all = v if v < min_all else min_all
+            if v < 1.0:
+                if len(lst) < cap:
+                    lst.append((typ, tuple(int(a) for a in perm), v))
+                    if len(lst) == 1 or v > least_val:
+                        least_val, least_idx = v, len(lst) - 1
+                elif v < least_val:
+                    lst[least_idx] = (typ, tuple(int(a) for a in perm), v)
+                    least_val = BIG_NUMBER
+                    for q, entry in enumerate(lst):
+                        if entry[2] > least_val:
+                            least_val, least_idx = entry[2], q
+    return lst, min_all
+
+
+def updateKgonalInequalities(perm: np.ndarray, types: np.ndarray, y: np.ndarray, X: np.ndarray, k: int,
+                             trials: int, cap: int):
+    """Purge the k-gonal cuts whose multiplier is below 1e-5 (keeping
+    order), separate, append the separated cuts that are not among the kept
+    ones (src/cutting_planes.c:307-404 and its heptagonal twin).  Returns
+    (perm, types, y of the new list, added, subtracted, smallest value)."""
+    m_old = len(types)
+    keep = [i for i in range(m_old) if not y[i] < 1e-5]
+    perm = np.asarray(perm, dtype=np.int32).reshape(-1, k)[keep]
+    types = np.asarray(types, dtype=np.int32)[keep]
+    ykept = np.asarray(y[:m_old], dtype=np.float64)[keep]
+    lst, min_all = getViolated_KgonalInequalities(X, k, trials, cap)
+    existing = {(int(t), tuple(int(a) for a in p)) for t, p in zip(types, perm)}
+    new_perm, new_types = [], []
+    count = len(keep)
+    for t, p, _v in lst:
+        if count == MAX_KGON_ADDED:
+            break
+        if (t, p) in existing:
+            continue
+        new_perm.append(p)
+        new_types.append(t)
+        count += 1
+    added = len(new_types)
+    if added:
+        perm = np.concatenate([perm, np.array(new_perm, np.int32)])
+        types = np.concatenate([types, np.array(new_types, np.int32)])
+        ykept = np.concatenate([ykept, np.zeros(added)])
+    return perm, types, ykept, added, m_old - len(keep), min_all
+
+
 @dataclass
 class BoundResult:
     """What SDPbound leaves behind: the bound it returns, the incumbent
@@ -603,6 +673,7 @@ class BoundResult:
     outer_iterations: int
     prune: bool
     giveup: bool
+    kgon_rounds: int = 0   # pentagonal / heptagonal separation calls
 
 
 def _fracsol(X, xfixed, sol, N):
@@ -622,18 +693,21 @@ def _fracsol(X, xfixed, sol, N):
 
 def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: int = 1,
              diff: float = 0.0) -> BoundResult:
-    """The node bound (src/bounding.c:24-342) with triangle cuts only: the
-    pentagonal and heptagonal separations are not restated here, so
-    prm["include_Pent"] and prm["include_Hepta"] must be 0.
+    """The node bound (src/bounding.c:24-342).
 
     prm holds the reference's parameters (init_bundle_iter, max_bundle_iter,
     triag_iter, pent_iter, hept_iter, max_outer_iter, extra_iter,
-    violated_TriIneq, TriIneq after adjust_TriIneq, use_diff).  lb / best_x:
-    the incumbent (Bab_LBGet / BabSol) before the call; diff: the global
-    diff.  The heuristic draws from rand() in the reference's order, so call
-    srand() first to reproduce a run."""
-    if prm.get("include_Pent", 0) or prm.get("include_Hepta", 0):
-        raise ValueError("the oracle's SDPbound covers triangle cuts only")
+    violated_TriIneq, TriIneq after adjust_TriIneq, use_diff, include_Pent,
+    include_Hepta, PentIneq, HeptaIneq, Pent_Trials, Hepta_Trials).  lb /
+    best_x: the incumbent (Bab_LBGet / BabSol) before the call; diff: the
+    global diff.  The heuristic and the k-gonal annealing draw from rand()
+    in the reference's order, so call srand() first to reproduce a run.
+
+    The cut lists keep the multipliers their last update stored (the
+    reference's Cuts[i].y, Pent_Cuts[i].y, Hepta_Cuts[i].y); after each
+    separation round the dual vector is rebuilt from them, so a k-gonal kind
+    that was not separated in a round gets back the multipliers of its last
+    separation (src/bounding.c:261-271)."""
     N = SP_L.shape[0] - 1
     xfixed = np.asarray(xfixed[:N])
     sol = np.asarray(sol[:N])
@@ -661,9 +735,12 @@ def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: 
     if prm["use_diff"] and rank != 0 and bound > lb + diff + 1.0:   # :115
         return BoundResult(bound, lb, best_x, fracsol, diff, 0, False, True)
 
-    tri, ttype, gamma, _, _, viol3 = updateTriangleInequalities(cuts, np.zeros(0), X, int(prm["TriIneq"]),
-                                                                 float(prm["violated_TriIneq"]))   # :120
+    tri, ttype, ytri, _, _, viol3 = updateTriangleInequalities(cuts, np.zeros(0), X, int(prm["TriIneq"]),
+                                                                float(prm["violated_TriIneq"]))   # :120
     cuts = Cuts(tri=tri, tri_type=ttype)
+    ypent, yhept = np.zeros(0), np.zeros(0)
+    gamma = ytri.copy()
+    viol5 = 0.0
     m = cuts.m
     t = 0.5 * (bound - lb) / (m * viol3 * viol3)                 # :133
     g = op_B(cuts, np.ones(m), X)                                # :138-139
@@ -671,6 +748,7 @@ def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: 
 
     bdl_iter = int(prm["init_bundle_iter"])
     count = 0
+    kgon_rounds = 0
     prune = giveup = False
     while True:
         count += 1                                               # :168-172
@@ -691,12 +769,26 @@ def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: 
         if count == prm["max_outer_iter"] + prm["extra_iter"]:   # :214-215
             giveup = True
         if not prune and not giveup:                             # :219-230
-            tri, ttype, gamma, _, _, viol3 = updateTriangleInequalities(cuts, gamma, X, int(prm["TriIneq"]),
-                                                                         float(prm["violated_TriIneq"]))
-            cuts = Cuts(tri=tri, tri_type=ttype)
+            triag, penta = len(cuts.tri_type), len(cuts.pent_type)
+            tri, ttype, ytri, _, _, viol3 = updateTriangleInequalities(cuts, gamma, X, int(prm["TriIneq"]),
+                                                                        float(prm["violated_TriIneq"]))
+            pent, ptype, hept, htype = cuts.pent, cuts.pent_type, cuts.hept, cuts.hept_type
+            if prm.get("include_Pent", 0) and (count > prm["triag_iter"] or viol3 < 0.2):
+                pent, ptype, ypent, _, _, viol5 = updateKgonalInequalities(
+                    pent, ptype, gamma[triag:], X, 5, int(prm["Pent_Trials"]), int(prm["PentIneq"]))
+                kgon_rounds += 1
+            if prm.get("include_Hepta", 0) and ((count > prm["triag_iter"] + prm["pent_iter"])
+                                                or (viol3 < 0.2 and (1 - viol5 < 0.4))):
+                hept, htype, yhept, _, _, _ = updateKgonalInequalities(
+                    hept, htype, gamma[triag + penta:], X, 7, int(prm["Hepta_Trials"]), int(prm["HeptaIneq"]))
+                kgon_rounds += 1
+            cuts = Cuts(tri=tri, tri_type=ttype, pent=np.asarray(pent, np.int32).reshape(-1, 5),
+                        pent_type=np.asarray(ptype, np.int32), hept=np.asarray(hept, np.int32).reshape(-1, 7),
+                        hept_type=np.asarray(htype, np.int32))
         done = prune or giveup
         fracsol = _fracsol(X, xfixed, sol, N)                    # :246-257
         if not done:                                             # :260-315
+            gamma = np.concatenate([ytri, ypent, yhept])
             m = cuts.m
             _, X_test, g = fct_eval(L, cuts, gamma)
             k = bundle.k
@@ -713,7 +805,7 @@ def SDPbound(SP_L: np.ndarray, xfixed, sol, lb: float, best_x, prm: dict, rank: 
     bound = f + fixedvalue
     if rank == 0:
         diff = basic_bound - bound                               # :328-329
-    return BoundResult(bound, lb, best_x, fracsol, diff, count, prune, giveup)
+    return BoundResult(bound, lb, best_x, fracsol, diff, count, prune, giveup, kgon_rounds)
 
 
 # --------------------------------------------------------------------------

@@ -268,18 +268,22 @@ def bundle_golden(ref, SPL):
 
 SDP_PARAMS = {"init_bundle_iter": 5, "max_bundle_iter": 15, "triag_iter": 5, "pent_iter": 5, "hept_iter": 5,
               "max_outer_iter": 20, "extra_iter": 10, "violated_TriIneq": 0.05, "use_diff": 1,
-              "include_Pent": 0, "include_Hepta": 0}
+              "include_Pent": 0, "include_Hepta": 0, "PentIneq": 5000, "HeptaIneq": 5000,
+              "Pent_Trials": 60, "Hepta_Trials": 50}
 
 
 def sdpbound_golden():
-    """SDPbound (src/bounding.c:24-342) with triangle cuts only, as Evaluate
-    runs it, on G(50, 0.9) with integer weights in [-10, 10] (seed 4): the
-    root at rank 0 with max_outer_iter = 7 and extra_iter = 0 (it gives up
-    after 7 outer iterations), the root with the default limits (it gives up
-    at outer iteration 15 and sets diff), then four subproblems at rank 1
-    from the incumbent the calls before left, the last with diff forced to
-    0.5 (the use_diff give-up), each from a fixed rand() state.  Inputs and
-    results go to sdpbound.npz."""
+    """SDPbound (src/bounding.c:24-342) as Evaluate runs it, on G(50, 0.9)
+    with integer weights in [-10, 10] (seed 4), each call from a fixed
+    rand() state and from the incumbent the calls before left.  Triangle
+    cuts only: the root at rank 0 with max_outer_iter = 7 and extra_iter = 0
+    (it gives up after 7 outer iterations), the root with the default limits
+    (it gives up at outer iteration 15 and sets diff), four subproblems at
+    rank 1, the last with diff forced to 0.5 (the use_diff give-up).  With
+    pentagonal and heptagonal cuts: the root capped at 7 and at 12 outer
+    iterations (heptagonal separation starts after 10), two subproblems.
+    Then the pentagonal and heptagonal updates alone on the root's X, three
+    rounds each.  Inputs and results go to sdpbound.npz."""
     ref = refbind.RefLib()
     prm = dict(SDP_PARAMS)
     ref.setup(instances.gnp_int(50, 0.9, 10, 4), prm)
@@ -291,21 +295,29 @@ def sdpbound_golden():
     SP = C.POINTER(refbind.Problem).in_dll(ref.lib, "SP")
     babsol = C.POINTER(C.c_int).in_dll(ref.lib, "BabSol")
     root = (np.zeros(N, np.int32), np.zeros(N, np.int32))
-    cases = [root + (0, 7, 0), root + (0, prm["max_outer_iter"], prm["extra_iter"])]
-    cases += [(xf, sol, 1, prm["max_outer_iter"], prm["extra_iter"])
-              for xf, sol in instances.random_fixings(N0, 4, 6, seed=31)]
+    mo, ex = prm["max_outer_iter"], prm["extra_iter"]
+    # (xfixed, sol, rank, max_outer_iter, extra_iter, k-gonal cuts, diff forced before the call)
+    cases = [root + (0, 7, 0, 0, None), root + (0, mo, ex, 0, None)]
+    fix = instances.random_fixings(N0, 6, 6, seed=31)
+    cases += [(xf, sol, 1, mo, ex, 0, None) for xf, sol in fix[:3]]
+    cases += [fix[3] + (1, mo, ex, 0, 0.5)]
+    # pentagonal and heptagonal cuts on (the reference's defaults)
+    cases += [root + (0, 7, 0, 1, None), root + (0, 12, 0, 1, None)]
+    cases += [(xf, sol, 1, mo, ex, 1, None) for xf, sol in fix[4:]]
     out = {"SPL": SPL, "params": np.array([prm[k] for k in sorted(prm)]),
            "param_names": np.array(sorted(prm))}
-    for q, (xf, sol, rank, max_outer, extra) in enumerate(cases):
+    for q, (xf, sol, rank, max_outer, extra, kgon, force_diff) in enumerate(cases):
         ref.set_param("max_outer_iter", max_outer)
         ref.set_param("extra_iter", extra)
-        out[f"c{q}_limits"] = np.array([max_outer, extra])
+        ref.set_param("include_Pent", kgon)
+        ref.set_param("include_Hepta", kgon)
+        out[f"c{q}_limits"] = np.array([max_outer, extra, kgon])
         node = refbind.BabNode()
         node.xfixed[:N] = [int(v) for v in xf]
         node.sol[:N] = [int(v) for v in sol]
         out[f"c{q}_xfixed"], out[f"c{q}_sol"], out[f"c{q}_rank"] = xf, sol, np.array([rank])
-        if q == len(cases) - 1:
-            ref.lib.bqbref_set_diff(0.5)
+        if force_diff is not None:
+            ref.lib.bqbref_set_diff(force_diff)
         out[f"c{q}_lb_in"] = np.array([ref.lib.Bab_LBGet()])
         out[f"c{q}_best_in"] = np.array([babsol[i] for i in range(N)], np.int32)
         out[f"c{q}_diff_in"] = np.array([ref.lib.bqbref_get_diff()])
@@ -319,6 +331,38 @@ def sdpbound_golden():
         out[f"c{q}_diff_out"] = np.array([ref.lib.bqbref_get_diff()])
         out[f"c{q}_rand_after"] = np.array([libc.rand()])
     out["ncases"] = np.array([len(cases)])
+
+    # the k-gonal updates alone (src/cutting_planes.c:223-602) on one X:
+    # three rounds per kind, each purging every third cut first
+    L = O.create_subproblem(SPL, np.zeros(N, np.int32), np.zeros(N, np.int32))
+    n = L.shape[0]
+    X = O.ipm_mc_pk(L).X
+    pp = PP.contents
+    pp.n, pp.NIneq, pp.NPentIneq, pp.NHeptaIneq = n, 0, 0, 0
+    gX = ref.gptr("X", C.c_double)
+    Xc = colmajor(X)
+    for q in range(n * n):
+        gX[q] = Xc[q]
+    out["kg_X"] = X
+    for k, fn, name, cls in ((5, "updatePentagonalInequalities", "Pent_Cuts", refbind.PentIneq),
+                             (7, "updateHeptagonalInequalities", "Hepta_Cuts", refbind.HeptIneq)):
+        for rnd in range(3):
+            m = pp.NPentIneq if k == 5 else pp.NHeptaIneq
+            y = np.where(np.arange(m) % 3 == 0, 0.0, 0.5)
+            added, subtracted = C.c_int(), C.c_int()
+            libc.srand(900 + rnd)
+            v = getattr(ref.lib, fn)(PP, refbind.dptr(y.copy()), C.byref(added), C.byref(subtracted), 0)
+            cuts = ref.gptr(name, cls)
+            m2 = pp.NPentIneq if k == 5 else pp.NHeptaIneq
+            tag = f"kg{k}_{rnd}"
+            out[f"{tag}_y"] = y
+            out[f"{tag}_perm"] = np.array([[cuts[c].permutation[j] for j in range(k)] for c in range(m2)],
+                                          np.int32).reshape(-1, k)
+            out[f"{tag}_type"] = np.array([cuts[c].type for c in range(m2)], np.int32)
+            out[f"{tag}_yout"] = np.array([cuts[c].y for c in range(m2)])
+            out[f"{tag}_counts"] = np.array([added.value, subtracted.value])
+            out[f"{tag}_value"] = np.array([v])
+            out[f"{tag}_rand_after"] = np.array([libc.rand()])
     np.savez_compressed(os.path.join(HERE, "sdpbound.npz"), **out)
 
 

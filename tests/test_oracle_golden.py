@@ -93,34 +93,63 @@ def test_bundle_method_matches_golden():
         np.testing.assert_allclose(bundle.G, B[f"b{call}_G"], rtol=0, atol=1e-6)
 
 
+_PORT = pytest.mark.skipif(not __import__("oracle.portbind").portbind.available(),
+                           reason="oracle C restatement not built (make -C oracle port)")
+
+
+@_PORT
+def test_kgonal_updates_match_golden_bit_exact():
+    """updatePentagonalInequalities / updateHeptagonalInequalities
+    (src/cutting_planes.c:223-602) on the same X and rand() state: purge,
+    annealing chains, list, duplicate check and the rand() state after are
+    the reference's exactly, three rounds per kind."""
+    B = np.load(os.path.join(HERE, "golden", "sdpbound.npz"))
+    X = B["kg_X"]
+    for k, trials in ((5, 60), (7, 50)):
+        perm, types = np.zeros((0, k), np.int32), np.zeros(0, np.int32)
+        for rnd in range(3):
+            tag = f"kg{k}_{rnd}"
+            O.srand(900 + rnd)
+            perm, types, y, added, subtracted, value = O.updateKgonalInequalities(perm, types, B[f"{tag}_y"], X, k,
+                                                                                  trials, 5000)
+            assert np.array_equal(perm, B[f"{tag}_perm"]) and np.array_equal(types, B[f"{tag}_type"])
+            assert np.array_equal(y, B[f"{tag}_yout"])
+            assert [added, subtracted] == B[f"{tag}_counts"].tolist()
+            assert value == B[f"{tag}_value"][0]
+            assert O.rand() == int(B[f"{tag}_rand_after"][0])
+
+
+@_PORT
 def test_sdpbound_matches_golden():
-    """SDPbound with triangle cuts (src/bounding.c:24-342) against the
-    reference build, case by case, each from the incumbent, diff and rand()
-    state the reference had.  Up to 7 outer iterations the bound agrees to
-    1e-9; the difference of the two builds' arithmetic (the reference runs
-    with -ffast-math and OpenBLAS) then grows by a factor of 30-100 per outer
-    iteration through the bundle's discrete decisions, so the one case with
-    15 outer iterations (the root with the default limits) is held to the
-    same outcome and 1e-3.  Incumbent value and cut, diff and the rand()
-    state after the call are exact or to 1e-9 in every case."""
+    """SDPbound (src/bounding.c:24-342) against the reference build, case by
+    case, each from the incumbent, diff and rand() state the reference had.
+    Up to 7 outer iterations without k-gonal separation the bound agrees to
+    1e-9.  Beyond that the two builds' arithmetic (the reference runs with
+    -ffast-math and OpenBLAS) drifts apart by a factor of 30-100 per outer
+    iteration through the bundle's discrete decisions, and the annealing
+    chains, whose move tests compare costs that are zero up to the last bits
+    of X, take other paths once X differs at all (on the same X they are
+    bit-identical: test_kgonal_updates_match_golden_bit_exact); those cases
+    are held to the same outcome and 2e-3.  Incumbent value and cut are
+    exact in every case."""
     B = np.load(os.path.join(HERE, "golden", "sdpbound.npz"))
     prm = {str(k): float(v) for k, v in zip(B["param_names"], B["params"])}
     SPL = B["SPL"]
     for q in range(int(B["ncases"][0])):
-        max_outer, extra = (int(v) for v in B[f"c{q}_limits"])
-        p = dict(prm, max_outer_iter=max_outer, extra_iter=extra)
+        max_outer, extra, kgon = (int(v) for v in B[f"c{q}_limits"])
+        p = dict(prm, max_outer_iter=max_outer, extra_iter=extra, include_Pent=kgon, include_Hepta=kgon)
         O.srand(500 + q)
         r = O.SDPbound(SPL, B[f"c{q}_xfixed"], B[f"c{q}_sol"], float(B[f"c{q}_lb_in"][0]), B[f"c{q}_best_in"], p,
                        rank=int(B[f"c{q}_rank"][0]), diff=float(B[f"c{q}_diff_in"][0]))
         want = float(B[f"c{q}_bound"][0])
-        tight = r.outer_iterations <= 7
-        assert abs(r.bound - want) <= (1e-9 if tight else 1e-3) * abs(want), (q, r.bound, want)
+        tight = r.outer_iterations <= 7 and r.kgon_rounds == 0
+        assert abs(r.bound - want) <= (1e-9 if tight else 2e-3) * abs(want), (q, r.bound, want)
         if tight:
             np.testing.assert_allclose(r.fracsol, B[f"c{q}_fracsol"], rtol=0, atol=1e-6)
             assert r.diff == pytest.approx(float(B[f"c{q}_diff_out"][0]), rel=1e-9, abs=1e-9)
+            assert O.rand() == int(B[f"c{q}_rand_after"][0])
         assert r.lb == float(B[f"c{q}_lb_out"][0])
         assert np.array_equal(r.best_x, B[f"c{q}_best_out"])
-        assert O.rand() == int(B[f"c{q}_rand_after"][0])
 
 
 def test_subproblem_construction_consistent():
