@@ -340,7 +340,6 @@ struct StepArgs {
 __device__ inline void bundle_step_body(const StepArgs& a)
 {
     __shared__ double red[64];
-    __shared__ double zlam[1];
     __shared__ int s_serious;
     __shared__ unsigned char used[BQB_MAX_BUNDLE + 8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
@@ -357,7 +356,6 @@ __device__ inline void bundle_step_body(const StepArgs& a)
     for (int i = tid; i < a.m; i += blockDim.x) sg += a.gtest[i];
     const double ftest = phi + block_sum(sg, red);
     // del = f - (F + G'gamma_test)'lambda
-    if (tid == 0) zlam[0] = 0.0;
     __syncthreads();
     double dl = 0.0;
     for (int b = warp; b < k; b += nw) {

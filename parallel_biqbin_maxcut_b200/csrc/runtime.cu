@@ -112,7 +112,7 @@ static void init_device(int dev)
     cudaDeviceProp prop;
     BQB_CUDA(cudaGetDeviceProperties(&prop, dev));
     if (prop.major < 10) {
-        char buf[128];
+        char buf[384];
         snprintf(buf, sizeof buf, "device %s is sm_%d%d; libbqb_gpu is compiled for sm_100a", prop.name,
                  prop.major, prop.minor);
         fatal("bqb_init", buf);
