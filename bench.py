@@ -489,6 +489,23 @@ def run_gpu(args):
                                                                   learned["fused_warm"]["seconds"])
         arm.reset_problem()
 
+    # ---- the torus configuration's IPM (n = 343: the multi-CTA IPM above n = 128) ----
+    ipm343 = None
+    if args.ipm_large and rank == 0:
+        L343 = instances.root_matrix(instances.torus3d(7, 1))
+        n343 = L343.shape[0]
+        Lc = _lib.colmajor(L343)
+        Xc = np.zeros(n343 * n343)
+        phi = C.c_double()
+        times = []
+        for _ in range(4):
+            t0 = time.perf_counter()
+            arm.lib.ipm_mc_pk(_lib.dptr(Lc), n343, _lib.dptr(Xc), C.byref(phi), 0)
+            times.append(time.perf_counter() - t0)
+        ipm343 = {"instance": "3D torus 7x7x7 (n = 343), couplings N(0,1) x 1e5 rounded, seed 1, root node",
+                  "call": "ipm_mc_pk with host buffers (copies inside the time)",
+                  "ms_per_call": 1e3 * min(times[1:]), "ms_first_call": 1e3 * times[0], "phi": phi.value}
+
     pk = peaks()
     kernel_ms = fst[2]
     flops = FLOP_PER_ITER_N3 * stats[0]
@@ -538,6 +555,7 @@ def run_gpu(args):
             "dropin_serial": drop,
             "time_to_optimality": tto,
             "learned_warm_start": learned,
+            "ipm_n343": ipm343,
             "gpu_launches": int(launches),
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -710,6 +728,8 @@ def main():
                     help="skip the time-to-optimality run")
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the learned warm-start comparison (two B&B runs, about 10 s)")
+    ap.add_argument("--no-ipm-large", dest="ipm_large", action="store_false",
+                    help="skip timing the n = 343 torus IPM (four calls, about 2 s with the first)")
     ap.add_argument("--tto-plain", action="store_true",
                     help="also time the plain drop-in solver to optimality (about 40 s on the n = 100 "
                          "instance, and on the learned leg's instance)")

@@ -97,6 +97,22 @@ def qubo_to_maxcut(Q: np.ndarray) -> np.ndarray:
     return A
 
 
+def root_matrix(A: np.ndarray) -> np.ndarray:
+    """The root node's matrix PP->L of an adjacency matrix A (nv x nv): the
+    Laplacian over the first nv - 1 vertices bordered by its row sums, the
+    last vertex fixed to 0, scaled by 1/4 (src/process_input.c:289-333,
+    src/evaluate.c:38-115 with nothing fixed).  nv x nv, row-major."""
+    nv = A.shape[0]
+    lap = np.diag(A.sum(axis=1)) - A
+    L = np.zeros((nv, nv))
+    L[:nv - 1, :nv - 1] = lap[:nv - 1, :nv - 1]
+    rs = L[:nv - 1, :nv - 1].sum(axis=1)
+    L[:nv - 1, nv - 1] = rs
+    L[nv - 1, :nv - 1] = rs
+    L[nv - 1, nv - 1] = rs.sum()
+    return 0.25 * L
+
+
 def random_fixings(nv: int, count: int, kmax: int, seed: int):
     """``count`` (xfixed, sol) pairs over the nv-1 branchable vertices: k
     uniform in [0, kmax] vertices fixed, values uniform in {0, 1}."""

@@ -87,15 +87,7 @@ def run_ipm(n_vertices: int, repeats: int, torus: bool = False) -> None:
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
     A = instances.torus3d(n_vertices, 1) if torus else instances.gnp_pm1(n_vertices, 0.5, seed=1)
     nv = A.shape[0]
-    lap = np.diag(A.sum(axis=1)) - A
-    L = np.zeros((nv, nv))
-    L[:nv - 1, :nv - 1] = lap[:nv - 1, :nv - 1]
-    rs = L[:nv - 1, :nv - 1].sum(axis=1)
-    L[:nv - 1, nv - 1] = rs
-    L[nv - 1, :nv - 1] = rs
-    L[nv - 1, nv - 1] = rs.sum()
-    L *= 0.25
-    Lc = _lib.colmajor(L)
+    Lc = _lib.colmajor(instances.root_matrix(A))
     X = np.zeros(nv * nv)
     phi = C.c_double()
     for _ in range(repeats):
