@@ -702,10 +702,23 @@ def run_reference(args):
         tto = {"instance": TTO_NAME, "reference_serial": {
             "seconds": t_r, "optimum": float(mv.group(1)) if mv else None, "nodes": int(mn.group(1)) if mn else None,
             "call": "the reference's serial best-first B&B (oracle/_ref/bqb_ref_bab), 1 core, OpenBLAS 1 thread"}}
+    ipm343 = None
+    if args.ipm_large:   # the GPU arm's ipm_n343 case through the reference's own ipm_mc_pk
+        os.environ["OPENBLAS_NUM_THREADS"] = "1"
+        ref = refbind.RefLib()
+        L343 = instances.root_matrix(instances.torus3d(7, 1))
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            _, phi = ref.ipm(L343)
+            times.append(time.perf_counter() - t0)
+        ipm343 = {"instance": "3D torus 7x7x7 (n = 343), couplings N(0,1) x 1e5 rounded, seed 1, root node",
+                  "call": "the reference's ipm_mc_pk (oracle/_ref), 1 core, OpenBLAS 1 thread",
+                  "ms_per_call": 1e3 * min(times), "phi": phi}
     line = {"metric": METRIC, "value": v, "unit": "nodes/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "time_to_optimality": tto,
+            "time_to_optimality": tto, "ipm_n343": ipm343,
             "config": {"workload": WORKLOAD, "nodes_per_step": B, "processes": P,
                        "dispatch": "dynamic: one node at a time to the next idle process, steps back to back"},
             "cpu_baseline": {"value": v, "unit": "nodes/s", "cores": P, "kind": "reference",

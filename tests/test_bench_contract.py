@@ -27,3 +27,4 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["unit"] == "nodes/s" and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
+    assert d["ipm_n343"]["ms_per_call"] > 0 and abs(d["ipm_n343"]["phi"] - 28282941.94) < 1e-2
