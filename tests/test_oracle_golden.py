@@ -168,6 +168,23 @@ def test_subproblem_construction_consistent():
         assert abs(xpm @ L @ xpm + fv - O.evaluateSolution(SPL, s)) < 1e-9
 
 
+def test_root_matrix_helper_matches_oracle():
+    """instances.root_matrix (used by bench.py and the profiling cases) is
+    the oracle's root subproblem, and its objective is the cut value."""
+    from parallel_biqbin_maxcut_b200 import instances
+    for A in (instances.torus3d(4, 2), instances.gnp_pm1(30, 0.5, 5),
+              instances.qubo_to_maxcut(instances.qubo_dense(20, 0.2, 6))):
+        N = A.shape[0] - 1
+        SPL = O.build_SP_L(A)
+        L = instances.root_matrix(A)
+        assert np.array_equal(L, O.create_subproblem(SPL, np.zeros(N, int), np.zeros(N, int)))
+        x = np.random.default_rng(1).integers(0, 2, N + 1)
+        x[-1] = 0
+        xpm = 2.0 * x[:N] - 1.0   # the convention of createSubproblem (src/evaluate.c:38-115)
+        cut = sum(A[i, j] for i in range(N + 1) for j in range(i + 1, N + 1) if x[i] != x[j])
+        assert abs(np.concatenate([xpm, [1.0]]) @ L @ np.concatenate([xpm, [1.0]]) - cut) < 1e-9
+
+
 def test_bab_optima_fixture_present():
     with open(os.path.join(HERE, "golden", "bab_optima.json")) as fh:
         rows = json.load(fh)
