@@ -10,19 +10,27 @@
 // capacities, numerical failures) are bounded again by engines
 // (bqb_bound_nodes), which follow the reference's code path exactly.
 //
-// Submissions go to a ring of NK_PIPES pipes, each with its own stream,
-// arena and buffers, so several launches are in flight at once: when the
-// last, heaviest nodes of one batch hold a few SMs, the next batch's CTAs
-// take the rest.  A submission made while a launch is running waits on the
-// host; the next collect (or the next submission that finds the GPU idle)
-// launches every waiting submission as one kernel, whose node order is
-// heaviest-first over all of them, so the heavy nodes of later batches
+// A submission takes one of NK_SUBS submission slots (its fixings, its
+// ticket) until it is collected; a launch takes one of NK_LAUNCHES launch
+// records (stream, events, device arena, node buffers, pinned result
+// buffers) until every submission it carries has been collected.  The two
+// are separate so that a launch carrying several submissions never holds a
+// submission slot: a slot frees when its own submission is collected.
+// Every busy launch record carries at least one uncollected submission, so
+// with NK_LAUNCHES >= NK_SUBS a launch record is free whenever staged
+// submissions are launched.  Several launches are in flight at once: when
+// the last, heaviest nodes of one batch hold a few SMs, the next batch's
+// CTAs take the rest.  A submission made while a launch is running waits
+// on the host; the next collect (or the next submission that finds the GPU
+// idle) launches every waiting submission as one kernel, whose node order
+// is heaviest-first over all of them, so the heavy nodes of later batches
 // start early instead of forming the tail of the last launch.  Each
 // submission is still collected on its own, in any order.
 // bqb_bound_nodes_fused is a submission collected at once.
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <mutex>
 #include <vector>
 
@@ -41,32 +49,40 @@ extern double diff;
 namespace bqb {
 namespace {
 
-constexpr int NK_PIPES = 8;
+constexpr int NK_SUBS = 8;
+constexpr int NK_LAUNCHES = NK_SUBS;
+static_assert(NK_LAUNCHES >= NK_SUBS, "a staged submission must always find a free launch record");
 
-struct FusedPipe {
+// One uncollected submission.
+struct FusedSub {
     bool busy = false;       // holds an uncollected submission
-    bool launched = false;   // its nodes are in a launch (its own or a leader's)
-    int leader = -1;         // the pipe whose launch carries its nodes
-    int offset = 0;          // its first node in the leader's arrays
-    int refs = 0;            // (leader) uncollected submissions its launch carries
-    bool counted = false;    // (leader) launch time added to the statistics
+    bool launched = false;   // its nodes are in a launch
+    int launch = -1;         // the launch record carrying its nodes
+    int offset = 0;          // its first node in that launch's arrays
     int count = 0, rank = 0, N = 0;
     unsigned long long ticket = 0;
-    HostBuf<int> gfix;       // (leader) the launch's fixings, all submissions
+    HostBuf<int> hfix;       // xfixed rows then sol.X rows, count x N each
+};
+
+// One launch of the fused kernel and its buffers.
+struct FusedLaunch {
+    int refs = 0;            // uncollected submissions it carries (0: free)
+    bool counted = false;    // launch time added to the statistics
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf<unsigned char> arena;
     DevBuf<double> bound, fracsol, hval;
     DevBuf<int> xf, sx, hsol, status, next, order;
     DevBuf<unsigned long long> lb, node_ns;
-    HostBuf<int> hfix, hhs, hst, hord;
+    HostBuf<int> gfix, hhs, hst, hord;
     HostBuf<double> hb, hfs, hhv;
     HostBuf<unsigned long long> hns, hlb;
 };
 
 struct FusedState {
     std::mutex mu;
-    FusedPipe pipe[NK_PIPES];
+    FusedSub sub[NK_SUBS];
+    FusedLaunch run[NK_LAUNCHES];
     unsigned long long next_ticket = 0;
     DevBuf<double> P0L;
     DevBuf<unsigned long long> prof;
@@ -147,55 +163,72 @@ bool fused_supported(int N0, size_t smem_optin)
     return c.smem_bytes <= smem_optin;
 }
 
-// Stage a submission on pipe P: its fixings go to P's pinned buffer (the
+// Stage a submission in slot S: its fixings go to S's pinned buffer (the
 // caller holds F.mu).
-void stage(FusedState& F, FusedPipe& P, const BabNode* nodes, int count, int rank)
+void stage(FusedState& F, FusedSub& S, const BabNode* nodes, int count, int rank)
 {
     const int N = SP->n - 1;
-    if (!P.stream) {
-        BQB_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
-        BQB_CUDA(cudaEventCreate(&P.ev0));
-        BQB_CUDA(cudaEventCreate(&P.ev1));
-    }
     const size_t cN = (size_t)count * N;
-    int* hf = P.hfix.ensure(2 * cN);
+    int* hf = S.hfix.ensure(2 * cN);
     for (int i = 0; i < count; ++i) {
         memcpy(hf + (size_t)i * N, nodes[i].xfixed, N * sizeof(int));
         memcpy(hf + cN + (size_t)i * N, nodes[i].sol.X, N * sizeof(int));
     }
-    P.busy = true;
-    P.launched = false;
-    P.leader = -1;
-    P.offset = 0;
-    P.count = count;
-    P.rank = rank;
-    P.N = N;
-    P.ticket = F.next_ticket++;
+    S.busy = true;
+    S.launched = false;
+    S.launch = -1;
+    S.offset = 0;
+    S.count = count;
+    S.rank = rank;
+    S.N = N;
+    S.ticket = F.next_ticket++;
 }
 
-// One launch for the staged submissions `members` (pipe indices in ticket
-// order, same rank), carried by the first one's pipe (the caller holds F.mu).
-void launch(FusedState& F, const std::vector<int>& members)
+// A free launch record, its stream and events created on first use; -1 when
+// every record still carries an uncollected submission (the caller holds
+// F.mu).
+int free_launch(FusedState& F)
+{
+    for (int q = 0; q < NK_LAUNCHES; ++q) {
+        FusedLaunch& L = F.run[q];
+        if (L.refs > 0) continue;
+        if (!L.stream) {
+            BQB_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+            BQB_CUDA(cudaEventCreate(&L.ev0));
+            BQB_CUDA(cudaEventCreate(&L.ev1));
+        }
+        return q;
+    }
+    return -1;
+}
+
+// One launch for the staged submissions `members` (slot indices in ticket
+// order, same rank) on a free launch record (the caller holds F.mu).
+// Returns false when no launch record is free.
+bool launch(FusedState& F, const std::vector<int>& members)
 {
     Runtime& R = rt();
+    const int li = free_launch(F);
+    if (li < 0) return false;
+    FusedLaunch& P = F.run[li];
     const int N0 = SP->n;
     const int N = N0 - 1;
-    FusedPipe& P = F.pipe[members[0]];
-    const int rank = P.rank;
+    const FusedSub& S0 = F.sub[members[0]];
+    const int rank = S0.rank;
     int count = 0;
-    for (int q : members) count += F.pipe[q].count;
+    for (int q : members) count += F.sub[q].count;
     cudaStream_t s = P.stream;
     FusedCfg c;
-    fill_cfg(c, N0, count, rank, F.seed + 0x9E3779B97F4A7C15ull * (P.ticket + 1), R.smem_optin);
+    fill_cfg(c, N0, count, rank, F.seed + 0x9E3779B97F4A7C15ull * (S0.ticket + 1), R.smem_optin);
     const size_t slot_bytes = nk_layout(c);
     int slots = R.num_sms;
     if (slots > count) slots = count;
 
     const unsigned gen = g_sp_generation.load();
     if (F.P0L_src != SP->L || F.P0N != N0 || F.P0L_gen != gen) {
-        // every pipe reads P0L: let the launches in flight finish first
-        for (int q = 0; q < NK_PIPES; ++q)
-            if (F.pipe[q].refs > 0) BQB_CUDA(cudaStreamSynchronize(F.pipe[q].stream));
+        // every launch reads P0L: let the launches in flight finish first
+        for (int q = 0; q < NK_LAUNCHES; ++q)
+            if (F.run[q].refs > 0) BQB_CUDA(cudaStreamSynchronize(F.run[q].stream));
         F.P0L.ensure((size_t)N0 * N0);
         BQB_CUDA(cudaMemcpy(F.P0L.p, SP->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice));
         F.P0L_src = SP->L;
@@ -210,12 +243,12 @@ void launch(FusedState& F, const std::vector<int>& members)
     int* hf = P.gfix.ensure(2 * cN);
     int off = 0;
     for (int q : members) {
-        FusedPipe& M = F.pipe[q];
+        FusedSub& M = F.sub[q];
         const size_t mN = (size_t)M.count * N;
         memcpy(hf + (size_t)off * N, M.hfix.p, mN * sizeof(int));
         memcpy(hf + cN + (size_t)off * N, M.hfix.p + mN, mN * sizeof(int));
         M.launched = true;
-        M.leader = members[0];
+        M.launch = li;
         M.offset = off;
         off += M.count;
     }
@@ -280,31 +313,35 @@ void launch(FusedState& F, const std::vector<int>& members)
     P.refs = (int)members.size();
     P.counted = false;
     ++F.st_launches;
+    return true;
 }
 
 // Launch the staged submissions: one launch per run of equal rank, in
-// ticket order (the caller holds F.mu).
-void launch_staged(FusedState& F)
+// ticket order (the caller holds F.mu).  Returns false when a launch found
+// no free record (which the slot count rules out; the submissions stay
+// staged and the caller reports the error).
+bool launch_staged(FusedState& F)
 {
     std::vector<int> st;
-    for (int q = 0; q < NK_PIPES; ++q)
-        if (F.pipe[q].busy && !F.pipe[q].launched) st.push_back(q);
-    std::sort(st.begin(), st.end(), [&](int a, int b) { return F.pipe[a].ticket < F.pipe[b].ticket; });
+    for (int q = 0; q < NK_SUBS; ++q)
+        if (F.sub[q].busy && !F.sub[q].launched) st.push_back(q);
+    std::sort(st.begin(), st.end(), [&](int a, int b) { return F.sub[a].ticket < F.sub[b].ticket; });
     size_t i = 0;
     while (i < st.size()) {
         std::vector<int> group{st[i]};
         size_t j = i + 1;
-        while (j < st.size() && F.pipe[st[j]].rank == F.pipe[st[i]].rank) group.push_back(st[j++]);
-        launch(F, group);
+        while (j < st.size() && F.sub[st[j]].rank == F.sub[st[i]].rank) group.push_back(st[j++]);
+        if (!launch(F, group)) return false;
         i = j;
     }
+    return true;
 }
 
 // Is a launch still running on the GPU?
 bool any_running(FusedState& F)
 {
-    for (int q = 0; q < NK_PIPES; ++q) {
-        FusedPipe& L = F.pipe[q];
+    for (int q = 0; q < NK_LAUNCHES; ++q) {
+        FusedLaunch& L = F.run[q];
         if (L.refs <= 0) continue;
         const cudaError_t e = cudaEventQuery(L.ev1);
         if (e == cudaErrorNotReady) return true;
@@ -313,19 +350,23 @@ bool any_running(FusedState& F)
     return false;
 }
 
-// Wait for pipe P and hand its results to the caller's nodes (the caller
-// holds F.mu).
-int collect(FusedState& F, FusedPipe& P, BabNode* nodes, double* bounds)
+// Wait for submission S and hand its results to the caller's nodes (the
+// caller holds F.mu).  S's slot is free when this returns; its launch record
+// frees when the last submission it carries has been collected.
+int collect(FusedState& F, FusedSub& S, BabNode* nodes, double* bounds)
 {
     // submissions still waiting on the host start now, behind the launches
     // in flight, so they run while this one is waited for
-    launch_staged(F);
-    FusedPipe& L = F.pipe[P.leader];
-    cudaStream_t s = P.stream;
+    if (!launch_staged(F)) {
+        set_error("bqb_fused_collect", "no free launch record");
+        return 1;
+    }
+    FusedLaunch& L = F.run[S.launch];
     BQB_CUDA(cudaStreamSynchronize(L.stream));
-    P.busy = false;
-    --L.refs;
-    const int count = P.count, N = P.N, o = P.offset;
+    const int count = S.count, N = S.N, o = S.offset, rank = S.rank;
+    S.busy = false;
+    S.launched = false;
+    S.launch = -1;
     if (!L.counted) {
         float kms = 0.f;
         BQB_CUDA(cudaEventElapsedTime(&kms, L.ev0, L.ev1));
@@ -354,20 +395,19 @@ int collect(FusedState& F, FusedPipe& P, BabNode* nodes, double* bounds)
         memcpy(bs.X, L.hhs.p + (size_t)(o + i) * N, N * sizeof(int));
         Bab_LBUpd(L.hhv.p[o + i], &bs);
     }
+    // every result of this submission has been read from L's host buffers
+    --L.refs;
     if (!redo.empty()) {
         F.fallbacks += (long long)redo.size();
         std::vector<BabNode> sub(redo.size());
         std::vector<double> sb(redo.size());
         for (size_t q = 0; q < redo.size(); ++q) sub[q] = nodes[redo[q]];
         const int th = redo.size() < 16 ? (int)redo.size() : 16;
-        BQB_CUDA(cudaEventRecord(P.ev0, s));
-        const int rc = bqb_bound_nodes(sub.data(), (int)sub.size(), P.rank, th, nullptr, sb.data());
-        BQB_CUDA(cudaEventRecord(P.ev1, s));
-        BQB_CUDA(cudaEventSynchronize(P.ev1));
-        float fms = 0.f;
-        BQB_CUDA(cudaEventElapsedTime(&fms, P.ev0, P.ev1));
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = bqb_bound_nodes(sub.data(), (int)sub.size(), rank, th, nullptr, sb.data());
+        const auto t1 = std::chrono::steady_clock::now();
         F.st_fallback_nodes += (double)redo.size();
-        F.st_fallback_ms += fms;
+        F.st_fallback_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
         if (rc) return rc;
         for (size_t q = 0; q < redo.size(); ++q) {
             nodes[redo[q]] = sub[q];
@@ -385,7 +425,7 @@ void fused_launch_pending()
 {
     FusedState& F = fstate();
     std::lock_guard<std::mutex> lock(F.mu);
-    launch_staged(F);
+    if (!launch_staged(F)) fatal("fused_launch_pending", "no free launch record");
 }
 
 }  // namespace bqb
@@ -401,16 +441,20 @@ BQB_API long long bqb_fused_submit(const BabNode* nodes, int count, int rank)
     if (!fused_supported(SP->n, R.smem_optin)) return -3;
     FusedState& F = fstate();
     std::lock_guard<std::mutex> lock(F.mu);
-    for (int q = 0; q < NK_PIPES; ++q) {
-        FusedPipe& P = F.pipe[(F.next_ticket + q) % NK_PIPES];
-        if (P.busy || P.refs > 0) continue;   // free: collected and not carrying others' nodes
-        stage(F, P, nodes, count, rank);
+    for (int q = 0; q < NK_SUBS; ++q) {
+        FusedSub& S = F.sub[(F.next_ticket + q) % NK_SUBS];
+        if (S.busy) continue;
+        stage(F, S, nodes, count, rank);
         // an idle GPU starts at once; otherwise the submission waits to be
         // launched together with the others submitted meanwhile
-        if (!any_running(F)) launch_staged(F);
-        return (long long)P.ticket;
+        if (!any_running(F) && !launch_staged(F)) {
+            set_error("bqb_fused_submit", "no free launch record");
+            S.busy = false;
+            return -1;
+        }
+        return (long long)S.ticket;
     }
-    set_error("bqb_fused_submit", "every pipe holds an uncollected submission");
+    set_error("bqb_fused_submit", "eight submissions are uncollected");
     return -1;
 }
 
@@ -419,9 +463,9 @@ BQB_API int bqb_fused_collect(long long ticket, BabNode* nodes, double* bounds)
 {
     FusedState& F = fstate();
     std::lock_guard<std::mutex> lock(F.mu);
-    for (int q = 0; q < NK_PIPES; ++q) {
-        FusedPipe& P = F.pipe[q];
-        if (P.busy && (long long)P.ticket == ticket) return collect(F, P, nodes, bounds);
+    for (int q = 0; q < NK_SUBS; ++q) {
+        FusedSub& S = F.sub[q];
+        if (S.busy && (long long)S.ticket == ticket) return collect(F, S, nodes, bounds);
     }
     set_error("bqb_fused_collect", "unknown or already collected ticket");
     return 1;

@@ -115,6 +115,47 @@ def test_fused_submit_collect_pipelined(lib, solved):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("depth", [8, 5])
+def test_fused_rolling_window_fifo(lib, solved, depth):
+    """A rolling window of `depth` submissions in flight, collected oldest
+    first, for three times as many submissions as there are slots (the
+    pattern of a benchmark that keeps the window full).  Submissions made
+    while a launch runs are grouped into one launch; the launch record must
+    not keep a submission slot once its own submission is collected, so no
+    submission is ever refused.  Bounds equal one batch at a time."""
+    nsub = 24
+    batches = [_nodes(12, 30, seed=400 + q) for q in range(nsub)]
+    singles = []
+    for b in batches:
+        c = _copy(b)
+        out = np.zeros(len(c))
+        assert lib.bqb_bound_nodes_fused(c, len(c), 1, _lib.dptr(out)) == 0
+        singles.append(out)
+    outs = [np.zeros(len(b)) for b in batches]
+    lib.bqb_fused_stats_reset()
+    window = []
+    for q, b in enumerate(batches):
+        if len(window) == depth:
+            t, j = window.pop(0)
+            assert lib.bqb_fused_collect(t, batches[j], _lib.dptr(outs[j])) == 0, lib.bqb_last_error()
+        t = lib.bqb_fused_submit(b, len(b), 1)
+        assert t >= 0, (q, lib.bqb_last_error())
+        window.append((t, q))
+    for t, j in window:
+        assert lib.bqb_fused_collect(t, batches[j], _lib.dptr(outs[j])) == 0, lib.bqb_last_error()
+    launches = lib.bqb_fused_launches()
+    assert 1 <= launches < nsub        # submissions made during a launch were grouped
+    for o, s in zip(outs, singles):
+        np.testing.assert_array_equal(o, s)
+    # nine uncollected submissions are refused, eight are accepted
+    tickets = [lib.bqb_fused_submit(batches[q], len(batches[q]), 1) for q in range(8)]
+    assert all(t >= 0 for t in tickets)
+    assert lib.bqb_fused_submit(batches[8], len(batches[8]), 1) == -1
+    for t, q in zip(tickets, range(8)):
+        assert lib.bqb_fused_collect(t, batches[q], _lib.dptr(outs[q])) == 0
+
+
+@pytest.mark.gpu
 def test_pending_submissions_survive_a_problem_change(lib, solved):
     """Submissions made while a launch runs wait on the host; replacing the
     problem (process_adj_matrix) first launches them for the problem they
@@ -156,3 +197,17 @@ def test_fused_solve_optimum(lib, kind, nv, seed):
     assert fused["best_value"] == serial["best_value"]
     assert fused["root_bound"] == serial["root_bound"]
     assert O.evaluateSolution(O.build_SP_L(A), fused["x"]) == fused["best_value"]
+
+
+@pytest.mark.gpu
+def test_fused_solve_depth8_optimum(lib):
+    """bqb_solve_fused with eight batches in flight reaches the optimum the
+    reference's serial B&B printed (tests/golden/bab_optima.json)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bab_optima.json")) as fh:
+        case = next(c for c in json.load(fh) if c["kind"] == "int10" and c["nv"] == 80)
+    A = instances.gnp_int(case["nv"], 0.9, 10, case["seed"])
+    r = _lib.solve(A, fused_batch=16, fused_depth=8)
+    assert r["best_value"] == case["max_value"]
+    assert O.evaluateSolution(O.build_SP_L(A), r["x"]) == r["best_value"]
