@@ -3,11 +3,20 @@ writing cut lists into a library's reference-layout globals."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
 from oracle import bqb_oracle as O
 from parallel_biqbin_maxcut_b200 import _lib, instances
+
+# Where the reference's sources and test fixtures lie (only tests that pin
+# against them read it; they skip when it is absent).
+REFERENCE_ROOT = os.environ.get("BQB_REFERENCE", "/root/reference")
+
+
+def ref_path(*parts: str) -> str:
+    return os.path.join(REFERENCE_ROOT, *parts)
 
 
 def root_L(A: np.ndarray) -> np.ndarray:
@@ -68,4 +77,4 @@ def make_problem(L_colmajor: np.ndarray, n: int, cuts: O.Cuts, mod=_lib):
     return p
 
 
-__all__ = ["root_L", "random_cuts", "cut_arrays", "set_global_cuts", "make_problem", "instances", "O"]
+__all__ = ["REFERENCE_ROOT", "ref_path", "root_L", "random_cuts", "cut_arrays", "set_global_cuts", "make_problem", "instances", "O"]

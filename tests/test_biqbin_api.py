@@ -12,11 +12,12 @@ import os
 import numpy as np
 import pytest
 
+from helpers import ref_path
 from parallel_biqbin_maxcut_b200 import _lib, biqbin, instances
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_QUBOS = ["/root/reference/tests/qubos/40/kcluster40_025_10_1.json",
-             "/root/reference/tests/qubos/80/kcluster80_025_20_1.json"]
+REF_QUBOS = [ref_path("tests", "qubos", "40", "kcluster40_025_10_1.json"),
+             ref_path("tests", "qubos", "80", "kcluster80_025_20_1.json")]
 
 
 def brute_maxcut(A):
@@ -149,7 +150,7 @@ def test_reference_qubo_fixture_through_reference_bab(tmp_path):
     A, g = biqbin.qubo_to_maxcut(Q)
     inst, prm = tmp_path / "q.rudy", tmp_path / "params"
     instances.write_rudy(str(inst), A)
-    with open("/root/reference/params") as fi:
+    with open(ref_path("params")) as fi:
         prm.write_text(fi.read())
     out = subprocess.run([refbind.REF_BAB, str(inst), str(prm)], capture_output=True, text=True, timeout=600,
                          env=dict(os.environ, OPENBLAS_NUM_THREADS="1")).stdout
@@ -157,7 +158,7 @@ def test_reference_qubo_fixture_through_reference_bab(tmp_path):
     assert best * g == pytest.approx(exp["maxcut"]["computed_val"])
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/biqbin_base.py"), reason="reference Python layer not present")
+@pytest.mark.skipif(not os.path.exists(ref_path("biqbin_base.py")), reason="reference Python layer not present")
 def test_reference_python_layer_imports_this_module(tmp_path, monkeypatch):
     """The reference's biqbin_base.py imports its six functions from this
     module: its solvers install their overrides here, and its default data
@@ -166,7 +167,7 @@ def test_reference_python_layer_imports_this_module(tmp_path, monkeypatch):
     import sys
     monkeypatch.setattr(sys, "dont_write_bytecode", True)   # nothing is written next to the reference
     monkeypatch.setitem(sys.modules, "biqbin", biqbin)
-    monkeypatch.syspath_prepend("/root/reference")
+    monkeypatch.syspath_prepend(ref_path())
     monkeypatch.delitem(sys.modules, "biqbin_base", raising=False)
     base = importlib.import_module("biqbin_base")
     try:

@@ -7,6 +7,7 @@ import os
 import numpy as np
 import pytest
 
+from helpers import ref_path
 from oracle import bqb_oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -199,12 +200,12 @@ def test_reference_build_reproduces_reference_fixtures():
     import subprocess
     import tempfile
     from oracle import refbind
-    src = "/root/reference/tests/rudy"
+    src = ref_path("tests", "rudy")
     if not (refbind.available() and os.path.isdir(src)):
         pytest.skip("reference sources or build absent")
     with tempfile.TemporaryDirectory() as td:
         params = os.path.join(td, "params")
-        with open("/root/reference/params") as fi, open(params, "w") as fo:
+        with open(ref_path("params")) as fi, open(params, "w") as fo:
             fo.write(fi.read())
         for name in ("g05_60.0", "g05_80.0", "g05_100.4"):
             inst = os.path.join(td, name)
