@@ -64,15 +64,25 @@ WORKLOAD = "G(100,0.5) ±1 weights; 512 subproblems, k~U[0,40] fixed (n=60..100)
 # Cholesky factorizations 2n^3/3): 6.0 n^3; the reference's count with its
 # second POSV is 6.33 n^3.  The smaller count is used.
 FLOP_PER_ITER_N3 = 6.0
-# DRAM traffic of the fused kernel per node, measured with ncu on a small case
-# (16 nodes of a G(60, 0.5) +-1 instance: 1.39 MB in one launch).
-NODEK_DRAM_BYTES_PER_NODE = 1.95e6 / 16
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one fused
+# launch, from an ncu capture; None until one is recorded for this workload.
+NODEK_DRAM_BYTES_PER_LAUNCH = None
+NODEK_TRAFFIC_NOTE = "not captured for the 512-node launch of this workload"
+FP64_NOMINAL_TFLOPS = 37.0
 
 
 # Time-to-optimality instance: the batched configuration's graph itself,
 # G(100, 0.5) with +-1 weights (seed 1), solved from scratch to optimality
 # with the shipped parameters.
 TTO_NAME = "G(100,0.5) +-1 weights, seed 1, full B&B, shipped params"
+TORUS_NAME = ("3D torus 7x7x7 (n = 343), couplings N(0,1) x 1e5 rounded, seed 1, full B&B, shipped params "
+              "(pentagonal and heptagonal cuts on)")
+LEG_CALLS = {
+    "fused": "bqb_solve_fused (batches of 2 x SMs, 8 in flight), FP64",
+    "fused_learned": "bqb_solve_fused (batches of 2 x SMs, 8 in flight) with the shipped warm-start model",
+    "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply)",
+    "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
+}
 
 
 def tto_instance():
@@ -420,22 +430,38 @@ def run_gpu(args):
         drop = {"value": len(idx) / (d0.elapsed_time(d1) / 1e3), "unit": "nodes/s",
                 "nodes": len(idx), "call": "Evaluate(node, SP, PP, 1), host buffers, serial"}
 
-    # ---- time to optimality: fused batches vs the plain drop-in ----
+    # ---- time to optimality: batched (+learned) vs the plain GPU drop-in ----
     tto = None
     if args.tto and rank == 0:
-        A = tto_instance()
-        t0 = time.perf_counter()
-        rf = _lib.solve(A, fused_batch=2 * arm.lib_sms(), fused_depth=4)
-        t_f = time.perf_counter() - t0
-        tto = {"instance": TTO_NAME, "fused": {"seconds": t_f, "optimum": rf["best_value"], "nodes": rf["nodes"],
-                                               "call": "bqb_solve_fused (batches of 2 x SMs, 4 in flight)"}}
-        if args.tto_plain:
-            t0 = time.perf_counter()
-            rp = _lib.solve(A)
-            t_p = time.perf_counter() - t0
-            tto["plain_dropin"] = {"seconds": t_p, "optimum": rp["best_value"], "nodes": rp["nodes"],
-                                   "call": "bqb_solve (serial best-first, one node at a time)"}
-            tto["speedup_vs_plain"] = t_p / t_f
+        from parallel_biqbin_maxcut_b200 import warm
+        p_w, _ = warm.load_model(warm.MODEL_C5)
+        sms = arm.lib_sms()
+        fused_kw = dict(fused_batch=2 * sms, fused_depth=8)
+        cases = [("n100", TTO_NAME, tto_instance(),
+                  [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w)])]
+        if args.tto_torus:
+            cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
+                          [("engines", dict(threads=16), None)]))
+        tto = {}
+        for key, name, A, legs in cases:
+            e = {"instance": name}
+            for leg, kw, model in legs:
+                warm.use_model(arm.lib, model)
+                t0 = time.perf_counter()
+                r = _lib.solve(A, **kw)
+                e[leg] = {"seconds": time.perf_counter() - t0, "optimum": r["best_value"], "nodes": r["nodes"],
+                          "root_bound": r["root_bound"], "call": LEG_CALLS[leg]}
+            warm.use_model(arm.lib, None)
+            if args.tto_plain:
+                t0 = time.perf_counter()
+                r = _lib.solve(A)
+                e["plain_dropin"] = {"seconds": time.perf_counter() - t0, "optimum": r["best_value"],
+                                     "nodes": r["nodes"], "root_bound": r["root_bound"],
+                                     "call": LEG_CALLS["plain_dropin"]}
+                best = min(e[leg]["seconds"] for leg, _, _ in legs)
+                e["speedup_batched_vs_plain"] = e["plain_dropin"]["seconds"] / best
+                assert all(e[leg]["optimum"] == e["plain_dropin"]["optimum"] for leg, _, _ in legs), e
+            tto[key] = e
         # restore the bench's problem (the solver set up its own)
         arm.reset_problem()
 
@@ -454,7 +480,7 @@ def run_gpu(args):
             warm.use_model(arm.lib, None)
             _lib.solve(A, time_limit=300, **kw)
         runs = []
-        if args.tto_plain:   # the plain GPU drop-in: serial B&B, one node at a time
+        if args.learned_plain:   # the plain GPU drop-in: serial B&B, one node at a time
             runs.append(("dropin_plain", None, dict()))
         for path, kw in paths:
             for mode in ("plain", "warm", "warm", "plain"):
@@ -509,17 +535,23 @@ def run_gpu(args):
     pk = peaks()
     kernel_ms = fst[2]
     flops = FLOP_PER_ITER_N3 * stats[0]
-    achieved = flops / (kernel_ms / 1e3) / 1e12 if kernel_ms > 0 else 0.0
+    # the pipelined launches of the fused kernel cover the timed span (a
+    # later launch starts while an earlier one's last nodes run), so the
+    # achieved rate is the counted work over the span, not over the summed
+    # (overlapping) launch durations
+    achieved = flops / (span_ms / 1e3) / 1e12 if span_ms > 0 else 0.0
     peak = pk["bf16_tflops_sustained"]
     roof = {"kernel": "nodek_kernel", "bound": "tensor", "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": NODEK_DRAM_BYTES_PER_NODE * B,
-            "traffic_note": "DRAM bytes per launch: 122 KB per node from the ncu capture of a small case "
-                            "(profiles/nodek_kernel_G60_16nodes.md, n = 60) times the nodes of a launch",
-            "peak_source": f"{pk['source']} bf16 sustained (FP64 kernel; B200 FP64 nominal 37 TFLOP/s "
-                           f"-> frac of FP64 nominal {achieved / 37.0:.4f})",
-            "launches": n_launch, "submissions": int(fst[0]), "avg_launch_us": 1e3 * kernel_ms / max(n_launch, 1),
-            "span_ms": span_ms, "kernel_ms_summed": kernel_ms,
-            "aggregate_tflops_over_span": flops / (span_ms / 1e3) / 1e12 if span_ms > 0 else 0.0,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": NODEK_DRAM_BYTES_PER_LAUNCH,
+            "traffic_note": NODEK_TRAFFIC_NOTE,
+            "peak_source": f"{pk['source']} bf16 sustained (the contract's compute denominator); the kernel "
+                           "computes in FP64 on the CUDA cores (no tensor-core instruction), so its own ceiling "
+                           f"is B200's nominal FP64 37 TFLOP/s: frac of that {achieved / FP64_NOMINAL_TFLOPS:.4f}",
+            "pipe": "fp64 (CUDA cores)", "frac_of_fp64_nominal": achieved / FP64_NOMINAL_TFLOPS,
+            "achieved_over": "span of the pipelined launches (CUDA events on the idle current stream around "
+                             "every submission and collection)",
+            "launches": n_launch, "submissions": int(fst[0]), "span_ms": span_ms,
+            "avg_launch_ms": kernel_ms / max(n_launch, 1), "kernel_ms_summed": kernel_ms,
             "flops_counted": "IPM only: sum over IPM solves of iterations * 6 n^3",
             "ipm_iterations": int(stats[2]), "ipm_problems": int(stats[1]),
             "linesearch_factorizations": int(stats[3]),
@@ -685,23 +717,37 @@ def run_reference(args):
     v = nodes / wall
     tto = None
     if args.tto:
-        import tempfile
-        A = tto_instance()
-        with tempfile.TemporaryDirectory() as td:
-            inst, prm = os.path.join(td, "g.rudy"), os.path.join(td, "params")
-            instances.write_rudy(inst, A)
-            instances.write_params(prm, _lib.PARAMS_FILE)
-            env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
-            t0 = time.perf_counter()
-            outp = subprocess.run([refbind.REF_BAB, inst, prm], capture_output=True, text=True, env=env,
-                                  timeout=1800).stdout
-            t_r = time.perf_counter() - t0
         import re
-        mv = re.search(r"Maximum value = (\S+)", outp)
-        mn = re.search(r"Nodes = (\d+)", outp)
-        tto = {"instance": TTO_NAME, "reference_serial": {
-            "seconds": t_r, "optimum": float(mv.group(1)) if mv else None, "nodes": int(mn.group(1)) if mn else None,
-            "call": "the reference's serial best-first B&B (oracle/_ref/bqb_ref_bab), 1 core, OpenBLAS 1 thread"}}
+        import tempfile
+        cases = [("n100", TTO_NAME, tto_instance())]
+        if args.tto_torus:
+            cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1)))
+        tto = {}
+
+        def ref_solve(key, name, A):
+            with tempfile.TemporaryDirectory() as td:
+                inst, prm = os.path.join(td, "g.rudy"), os.path.join(td, "params")
+                instances.write_rudy(inst, A)
+                instances.write_params(prm, _lib.PARAMS_FILE)
+                env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
+                t0 = time.perf_counter()
+                outp = subprocess.run([refbind.REF_BAB, inst, prm], capture_output=True, text=True, env=env,
+                                      timeout=1800).stdout
+                t_r = time.perf_counter() - t0
+            mv = re.search(r"Maximum value = (\S+)", outp)
+            mn = re.search(r"Nodes = (\d+)", outp)
+            tto[key] = {"instance": name, "reference_serial": {
+                "seconds": t_r, "optimum": float(mv.group(1)) if mv else None,
+                "nodes": int(mn.group(1)) if mn else None,
+                "call": "the reference's serial best-first B&B (oracle/_ref/bqb_ref_bab), 1 core, OpenBLAS 1 thread "
+                        "(the instances run side by side, one core each)"}}
+
+        # one serial process per instance, side by side on separate cores
+        ths = [threading.Thread(target=ref_solve, args=c) for c in cases]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
     ipm343 = None
     if args.ipm_large:   # the GPU arm's ipm_n343 case through the reference's own ipm_mc_pk
         os.environ["OPENBLAS_NUM_THREADS"] = "1"
@@ -728,6 +774,53 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+
+# --------------------------------------------------------------------------
+# small self-contained cases for kernel profiling (ncu -k ... -c ...)
+# --------------------------------------------------------------------------
+def run_case(args):
+    """`--case ipm`: the root of a seeded G(n, 0.5) +-1 instance through
+    ipm_mc_pk, `--repeats` times (above 128 vertices the multi-CTA IPM);
+    `--case ipm-torus`: the same for the side^3-vertex 3D torus (`--n` is
+    the side; 7 gives n = 343); `--case fused`: `--count` subproblems
+    (k ~ U[0, --kmax] fixed) of a seeded G(n, 0.5) +-1 instance bounded by
+    one fused-kernel launch, after the root on the engine path."""
+    lib = _lib.load()
+    assert lib.bqb_init(0) == 0, lib.bqb_last_error()
+    if args.case in ("ipm", "ipm-torus"):
+        A = instances.torus3d(args.n, 1) if args.case == "ipm-torus" else instances.gnp_pm1(args.n, 0.5, seed=1)
+        nv = A.shape[0]
+        Lc = _lib.colmajor(instances.root_matrix(A))
+        X = np.zeros(nv * nv)
+        phi = C.c_double()
+        for _ in range(args.repeats):
+            t0 = time.perf_counter()
+            lib.ipm_mc_pk(_lib.dptr(Lc), nv, _lib.dptr(X), C.byref(phi), 0)
+            print(f"n={nv} phi={phi.value:.6f} wall={1e3 * (time.perf_counter() - t0):.3f} ms", flush=True)
+        return
+    nv, count = args.n, args.count
+    A = np.ascontiguousarray(instances.gnp_pm1(nv, 0.5, seed=1))
+    _lib.set_params(lib, _lib.make_params(adjust_TriIneq=0, TriIneq=TRI_PER_N * nv))
+    lib.process_adj_matrix(_lib.dptr(A.copy()), nv)
+    glob = _lib.GlobalArrays(lib, nv)
+    sol = (C.c_int * _lib.NMAX)()
+    C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(sol)
+    SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+    PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
+    C.CDLL("libc.so.6").srand(2020)
+    root = _lib.BabNode()
+    rb = lib.Evaluate(C.byref(root), SP, PP, 0)
+    nodes = (_lib.BabNode * count)()
+    for q, (xf, sx) in enumerate(instances.random_fixings(nv, count, args.kmax, seed=2)):
+        nodes[q].xfixed[: nv - 1] = [int(v) for v in xf]
+        nodes[q].sol[: nv - 1] = [int(v) for v in sx]
+    b = np.zeros(count)
+    assert lib.bqb_bound_nodes_fused(nodes, count, 1, _lib.dptr(b)) == 0, lib.bqb_last_error()
+    print(f"n={nv} root={rb:.6f} nodes={count} mean_bound={b.mean():.6f} "
+          f"fallbacks={lib.bqb_fused_fallbacks()}", flush=True)
+    del glob
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -743,9 +836,13 @@ def main():
                     help="skip the learned warm-start comparison (two B&B runs, about 10 s)")
     ap.add_argument("--no-ipm-large", dest="ipm_large", action="store_false",
                     help="skip timing the n = 343 torus IPM (four calls, about 2 s with the first)")
-    ap.add_argument("--tto-plain", action="store_true",
-                    help="also time the plain drop-in solver to optimality (about 40 s on the n = 100 "
-                         "instance, and on the learned leg's instance)")
+    ap.add_argument("--no-tto-plain", dest="tto_plain", action="store_false",
+                    help="skip the plain drop-in solver's time to optimality (about 40 s on the n = 100 "
+                         "instance, 60 s on the torus)")
+    ap.add_argument("--no-tto-torus", dest="tto_torus", action="store_false",
+                    help="skip the time to optimality on the n = 343 torus")
+    ap.add_argument("--learned-plain", action="store_true",
+                    help="also time the plain drop-in solver on the learned leg's instance")
     ap.add_argument("--engine-nodes", type=int, default=128,
                     help="nodes timed through the concurrent engines (0: skip)")
     ap.add_argument("--dropin-nodes", type=int, default=16,
@@ -755,10 +852,18 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-nodes-per-step", type=int, default=256,
                     help="subproblems per step of the reference arm (bounded CPU sample)")
+    ap.add_argument("--case", choices=["ipm", "ipm-torus", "fused"], default=None,
+                    help="run one small profiling case instead of the benchmark")
+    ap.add_argument("--n", type=int, default=100, help="--case: vertices (ipm-torus: the side)")
+    ap.add_argument("--repeats", type=int, default=3, help="--case ipm/ipm-torus: calls")
+    ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
+    ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
     args = ap.parse_args()
     faulthandler.enable(all_threads=True)
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
