@@ -21,8 +21,15 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libbqb_gpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -fmad=false: no multiply and add is contracted into an FMA behind the
+# source's back.  The device bodies shared by the bounding kernels (IPM,
+# bundle, cut operators, annealing) are inlined into several kernels, and the
+# compiler's contraction choices could differ between those contexts; with
+# contraction off, every FMA is one the source writes (fma()), so every
+# kernel that runs a body computes the same bits.  The hot loops already
+# write their FMAs explicitly.
 NVCC_FLAGS = ARCH + [
-    "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+    "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden",
     "-I" + os.path.join(ROOT, "include"),
 ]
 
@@ -67,6 +74,14 @@ def _compile(src: str, hdr_mtime: float, extra: list[str]) -> str:
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
+    # objects built with other flags are rebuilt
+    stamp = os.path.join(OBJ, "flags.txt")
+    flags = " ".join(NVCC_FLAGS + CXX_FLAGS + (extra or []))
+    if not os.path.exists(stamp) or open(stamp).read() != flags:
+        for o in glob.glob(os.path.join(OBJ, "*.o")):
+            os.remove(o)
+        with open(stamp, "w") as fh:
+            fh.write(flags)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     hm = _headers_mtime()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:

@@ -157,9 +157,9 @@ Runtime& rt();
 extern std::atomic<unsigned long long> g_launches;
 #define BQB_COUNT_LAUNCH() (++::bqb::g_launches)
 
-// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The
-// limit is a per-function setting shared by every host thread, so it only
-// ever grows (a thread lowering it could invalidate another thread's launch
+// Raise a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`.  The limit is a per-(device, function) setting shared by
+// every host thread, so it only ever grows (a thread lowering it could invalidate another thread's launch
 // in flight between its own raise and launch).  Allocation-free.
 cudaError_t raise_smem_limit(const void* fn, size_t bytes);
 

@@ -55,6 +55,7 @@ void check_ipm_status_host(const double* out)
     const char* msg = status == IPM_Z_NOT_PD   ? "Problem with Cholesky factorization (Z not PD)"
                       : status == IPM_M_NOT_PD ? "problem in solving linear system (Zi.*X not PD)"
                       : status == IPM_LINESEARCH ? "line search found no positive definite step"
+                      : status == IPM_SYNC ? "a grid barrier of the multi-CTA IPM gave up waiting"
                                                  : "iteration limit reached";
     fatal("ipm_mc_pk", msg);
 }

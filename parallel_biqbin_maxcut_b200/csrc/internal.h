@@ -22,7 +22,7 @@ void ipm_device(DevBuf<double>& ws, const double* dL, double* dX, int n, double*
 // ipm_device hands larger problems to ipm_large.
 constexpr int IPM_REG_NMAX = 128;
 
-// ipm_mc_pk for n > IPM_REG_NMAX as host-orchestrated multi-CTA kernels
+// ipm_mc_pk for n > IPM_REG_NMAX as one cooperative multi-CTA launch
 // (csrc/ipm_large.cu); same arguments and results as ipm_device.
 void ipm_large(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
                const int* xslot);

@@ -16,6 +16,7 @@ enum IpmStatus : int {
     IPM_M_NOT_PD = 2,        // src/ipm_mc_pk.c:169-173 (dposv of Zi.*X failed)
     IPM_LINESEARCH = 3,      // line search did not find a PD step
     IPM_MAXITER = 4,
+    IPM_SYNC = 5,            // n > 128: a grid barrier gave up waiting (2 s)
 };
 
 // One problem.  L: n x n column-major (ld = n), read only.  X: n x n output.

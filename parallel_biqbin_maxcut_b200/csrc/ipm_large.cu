@@ -1,23 +1,41 @@
 // The basic SDP interior-point method (src/ipm_mc_pk.c:28-359) for n above
-// the register-resident limit (IPM_REG_NMAX = 128): the steps of
-// ipm_body_reg, orchestrated from the host, each step a multi-CTA kernel, so
-// that a factorisation is no longer paced by one SM reading global memory.
+// the register-resident limit (IPM_REG_NMAX = 128): ONE cooperative launch
+// per call.  Every CTA (one per SM at most) runs the whole predictor-
+// corrector loop; the phases of an iteration (the inverses, the solves, the
+// two products, the line searches' positive-definiteness tests, the step)
+// are separated by a grid barrier, and every decision (a failed pivot, the
+// line-search step, the stopping test) is taken by every CTA from the same
+// data with the same arithmetic, so all CTAs follow one control path with no
+// host round trip.
 //
 // Inverses (Zi = inv(Z), F = inv(Zi .* X)) use a blocked symmetric
-// Gauss-Jordan sweep on panels of WL_B columns.  For a panel K with
-// D = A_KK = Ld Ld^T (Cholesky in one CTA) and the columns C = A(:, K):
-// V = C Ld^{-T}, A_ij -= V_i V_j^T (i, j not in K), A_iK = V_i Ld^{-1}
-// (= C_i D^{-1}), A_KK = -D^{-1}; after the last panel A = -inv(A).  The
-// Cholesky pivots are the Schur complements of A: a non-positive one means
-// "not positive definite" and sets a flag.  The line searches' positive-
-// definiteness tests run the trailing part of the same sweep only, which is
-// a blocked right-looking Cholesky.  Going through Ld rather than the
-// explicit D^{-1} matters: at n = 343 with couplings of 1e5, M reaches a
+// Gauss-Jordan sweep on panels of CB = 32 columns.  For panel K with
+// D = A_KK = Ld Ld^T and the panel columns C = A(:, K): V = C Ld^{-T},
+// A_ij -= V_i V_j^T (i, j outside K), A_iK = W_i = V_i Ld^{-1} (= C_i D^{-1}),
+// A_KK = -D^{-1}; after the last panel A = -inv(A).  The Cholesky pivots are
+// the Schur complements of A: a non-positive one means "not positive
+// definite".  The line searches' tests run the trailing part of the sweep
+// only (a blocked right-looking Cholesky).  The Schur update goes through
+// Ld, not the explicit D^{-1}: at n = 343 with couplings of 1e5, M reaches a
 // condition number of 1e11 at the last iteration, and C D^{-1} C^T then
 // turned a pivot of the positive definite M negative.
-// Products with F replace the Cholesky solves, as in ipm_body_reg, each
-// followed by one step of iterative refinement with M = Zi .* X
-// (x <- x + F (b - M x)).
+//
+// One grid barrier per panel: every CTA factors the 32 x 32 panel block
+// itself (the same arithmetic in every CTA, hence the same decision), and
+// the owner of a 32 x 32 tile of A computes the V rows it needs itself.  The
+// writes of panel K's own row and column blocks (W and -D^{-1}) would race
+// with the other CTAs' reads of the panel columns, so they are deferred:
+// panel K leaves W_K and D^{-1}_K in side buffers, and in the next phase the
+// owner of each tile in row or column block K writes them before its own
+// update (readers of those entries take them from the side buffers).
+//
+// Products with F replace the Cholesky solves, each followed by one step of
+// iterative refinement with M = Zi .* X (x <- x + F (b - M x)).
+//
+// The grid barrier is a counter and a generation word in global memory;
+// every wait is bounded (2 s), after which the barrier sets an error word,
+// no CTA waits any more, every loop ends, and the call reports status
+// IPM_SYNC (a fatal error on the host).
 #include <math.h>
 
 #include "bqb_common.cuh"
@@ -30,563 +48,575 @@ double* ipm_stats_device();
 
 namespace {
 
-constexpr int WL_B = 32;     // panel width
-constexpr int WL_T = 256;    // threads per CTA of the elementwise kernels
-constexpr int WL_TILE = 32;  // tile of the update and GEMM kernels
+constexpr int CB = 32;          // panel and tile width
+constexpr int CT = 256;         // threads per CTA
+constexpr int CW = CT / 32;     // warps per CTA
+constexpr int LDS = CB + 1;     // padded shared-memory row
+constexpr unsigned long long BAR_TIMEOUT_NS = 2000000000ull;
 
-unsigned wl_blocks(long long count) { return (unsigned)((count + WL_T - 1) / WL_T); }
-
-// y_c = sum_r |L_rc| + 1.1, zd_c = y_c - L_cc (src/ipm_mc_pk.c:65-89)
-__global__ void wl_init_vec(const double* __restrict__ L, int n, double* __restrict__ y, double* __restrict__ zd)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    double acc = 0.0;
-    const double* Lc = L + (size_t)c * n;
-    for (int r = 0; r < n; ++r) acc += fabs(Lc[r]);
-    y[c] = acc + 1.1;
-    zd[c] = y[c] - L[c + (size_t)c * n];
-}
-
-__global__ void wl_identity(double* __restrict__ X, int n)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (size_t)n * n) return;
-    X[e] = (e % n == e / n) ? 1.0 : 0.0;
-}
-
-// One CTA: sc[0] = sum_i a_i, sc[1] = sum_i b_i, sc[2] = sum_i c_i over
-// vectors of n, or, with mode 1, the update sums zx, lx, ysum of
-// src/ipm_mc_pk.c:313-334 over X (n x n), L, zd, y.
-__global__ void wl_sums(int mode, int n, const double* __restrict__ L, const double* __restrict__ X,
-                        const double* __restrict__ y, const double* __restrict__ zd, double* __restrict__ sc)
-{
-    __shared__ double red[64];
-    double a = 0.0, b = 0.0, c = 0.0;
-    if (mode == 0) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            a += L[i + (size_t)i * n];
-            b += zd[i];
-            c += y[i];
-        }
-    } else {
-        const size_t nn = (size_t)n * n;
-        for (size_t e = threadIdx.x; e < nn; e += blockDim.x) {
-            const double xv = X[e], lv = L[e];
-            b = fma(lv, xv, b);                       // lx
-            if (e % n != e / n) a = fma(-lv, xv, a);  // zx, off-diagonal part
-        }
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            a = fma(zd[i], X[i + (size_t)i * n], a);
-            c += y[i];
-        }
-    }
-    a = block_sum(a, red);
-    b = block_sum(b, red);
-    c = block_sum(c, red);
-    if (threadIdx.x == 0) {
-        sc[0] = a;
-        sc[1] = b;
-        sc[2] = c;
-    }
-}
-
-// A = Diag(d + alpha dd) - L off the diagonal (dd may be null)
-__global__ void wl_fill_z(const double* __restrict__ L, const double* __restrict__ d, const double* __restrict__ dd,
-                          double alpha, int n, double* __restrict__ A)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (size_t)n * n) return;
-    const int i = (int)(e % n), j = (int)(e / n);
-    A[e] = i == j ? (dd ? fma(alpha, dd[i], d[i]) : d[i]) : -L[e];
-}
-
-// A = X + alpha dX
-__global__ void wl_axpy(const double* __restrict__ X, const double* __restrict__ dX, double alpha, size_t nn,
-                        double* __restrict__ A)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nn) A[e] = fma(alpha, dX[e], X[e]);
-}
-
-__global__ void wl_hadamard(const double* __restrict__ A, const double* __restrict__ B, size_t nn,
-                            double* __restrict__ C)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nn) C[e] = A[e] * B[e];
-}
-
-__global__ void wl_negate(double* __restrict__ A, size_t nn)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nn) A[e] = -A[e];
-}
-
-// ---- panel sweep ---------------------------------------------------------
-
-// One CTA: the Cholesky factor Ld of D = A[K, K] (b x b) by sequential
-// rank-1 updates in shared memory, Linv = Ld^{-1} (forward substitution,
-// one column per thread) and Dinv = Linv^T Linv.  A non-positive pivot sets
-// *flag.  Linv and Dinv are stored with leading dimension WL_B.
-__global__ void wl_panel_factor(const double* __restrict__ A, int n, int k0, int b, double* __restrict__ Linv,
-                                double* __restrict__ Dinv, double* __restrict__ flag)
-{
-    __shared__ double S[WL_B][WL_B + 1];
-    __shared__ double Li[WL_B][WL_B + 1];
-    const int tid = threadIdx.x;
-    for (int e = tid; e < WL_B * WL_B; e += blockDim.x) {
-        const int p = e % WL_B, q = e / WL_B;
-        S[p][q] = p < b && q < b ? A[(k0 + p) + (size_t)(k0 + q) * n] : 0.0;
-        Li[p][q] = 0.0;
-    }
-    __syncthreads();
-    bool pd = true;
-    // S becomes Ld column by column (lower triangle; the strict upper
-    // triangle keeps stale values and is not read)
-    for (int q = 0; q < b; ++q) {
-        const double d = S[q][q];
-        if (!(d > 0.0)) {   // d is the same value in every thread: all leave together
-            if (tid == 0) *flag = 1.0;
-            pd = false;
-            break;
-        }
-        const double l = sqrt(d);
-        __syncthreads();
-        if (tid >= q && tid < b) S[tid][q] = tid == q ? l : S[tid][q] / l;
-        __syncthreads();
-        for (int e = tid; e < b * b; e += blockDim.x) {
-            const int p = e % b, r = e / b;
-            if (p > q && r > q && r <= p) S[p][r] -= S[p][q] * S[r][q];
-        }
-        __syncthreads();
-    }
-    if (!pd) return;
-    // Li(:, t) = Ld^{-1} e_t: rows t..b-1, in order
-    if (tid < b) {
-        const int t = tid;
-        for (int i = t; i < b; ++i) {
-            double acc = i == t ? 1.0 : 0.0;
-            for (int k = t; k < i; ++k) acc = fma(-S[i][k], Li[k][t], acc);
-            Li[i][t] = acc / S[i][i];
-        }
-    }
-    __syncthreads();
-    for (int e = tid; e < WL_B * WL_B; e += blockDim.x) {
-        const int p = e % WL_B, q = e / WL_B;
-        Linv[p + (size_t)q * WL_B] = Li[p][q];
-        double acc = 0.0;
-        for (int k = p > q ? p : q; k < b; ++k) acc = fma(Li[k][p], Li[k][q], acc);
-        Dinv[p + (size_t)q * WL_B] = acc;
-    }
-}
-
-// One warp per row i outside the panel, lane q: V(i, q) = sum_{p <= q}
-// A(i, k0 + p) Linv(q, p) (V = C Ld^{-T}) and, with `full`, W(i, q) =
-// sum_{p >= q} V(i, p) Linv(p, q) (W = V Ld^{-1} = C D^{-1}; formed from V,
-// not as C times the explicit D^{-1}, whose rounding near convergence at
-// n = 343 sent the iteration off).  Panel rows get V = W = 0.
-__global__ void wl_panel_vw(const double* __restrict__ A, int n, int k0, int b, const double* __restrict__ Linv,
-                            int full, double* __restrict__ V, double* __restrict__ W)
-{
-    const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (i >= n) return;   // whole warps leave together
-    const bool outside = i < k0 || i >= k0 + b;
-    const double c = outside && lane < b ? A[i + (size_t)(k0 + lane) * n] : 0.0;
-    double v = 0.0;
-    for (int p = 0; p < b; ++p) {
-        const double cp = __shfl_sync(0xffffffffu, c, p);
-        if (p <= lane) v = fma(cp, Linv[lane + (size_t)p * WL_B], v);
-    }
-    if (lane < b) V[i + (size_t)lane * n] = v;
-    if (!full) return;
-    double w = 0.0;
-    for (int p = 0; p < b; ++p) {
-        const double vp = __shfl_sync(0xffffffffu, v, p);
-        if (p >= lane) w = fma(vp, Linv[p + (size_t)lane * WL_B], w);
-    }
-    if (lane < b) W[i + (size_t)lane * n] = w;
-}
-
-// A(i, j) -= sum_q V(i, q) V(j, q) for i, j outside the panel (with
-// `trailing`, only i, j >= k0 + b): the Schur complement through the
-// panel's Cholesky factor, which keeps the trailing pivots as accurate as
-// a blocked Cholesky (the form C D^{-1} C^T loses ~eps cond(D) and turned
-// pivots of a positive definite M negative at cond 1e11).  32 x 32 tiles,
-// 256 threads, 4 entries each; the product is symmetric in i and j.
-__global__ void wl_panel_update(double* __restrict__ A, int n, int k0, int b, const double* __restrict__ V,
-                                int trailing)
-{
-    __shared__ double si[WL_TILE][WL_B + 1];
-    __shared__ double sj[WL_TILE][WL_B + 1];
-    const int i0 = blockIdx.x * WL_TILE, j0 = blockIdx.y * WL_TILE;
-    const int lo = trailing ? k0 + b : 0;
-    if (i0 + WL_TILE <= lo || j0 + WL_TILE <= lo) return;
-    const int tid = threadIdx.x;
-    for (int e = tid; e < WL_TILE * b; e += blockDim.x) {
-        const int r = e % WL_TILE, q = e / WL_TILE;
-        const int i = i0 + r, j = j0 + r;
-        si[r][q] = i < n ? V[i + (size_t)q * n] : 0.0;
-        sj[r][q] = j < n ? V[j + (size_t)q * n] : 0.0;
-    }
-    __syncthreads();
-    const int r = tid % WL_TILE, c0 = tid / WL_TILE;   // c0 in 0..7
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int c = c0 + 8 * t;
-        const int i = i0 + r, j = j0 + c;
-        if (i >= n || j >= n || i < lo || j < lo) continue;
-        if ((i >= k0 && i < k0 + b) || (j >= k0 && j < k0 + b)) continue;
-        double acc = 0.0;
-        for (int q = 0; q < b; ++q) acc = fma(si[r][q], sj[c][q], acc);
-        A[i + (size_t)j * n] -= acc;
-    }
-}
-
-// A(i, K) = A(K, i)^T = W(i, :) for i outside the panel; A(K, K) = -Dinv.
-__global__ void wl_panel_fix(double* __restrict__ A, int n, int k0, int b, const double* __restrict__ W,
-                             const double* __restrict__ Dinv)
-{
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (long long)n * b) return;
-    const int i = (int)(e % n), q = (int)(e / n);
-    if (i >= k0 && i < k0 + b) {
-        const int p = i - k0;
-        A[i + (size_t)(k0 + q) * n] = -Dinv[p + (size_t)q * WL_B];
-    } else {
-        const double v = W[i + (size_t)q * n];
-        A[i + (size_t)(k0 + q) * n] = v;
-        A[(k0 + q) + (size_t)i * n] = v;
-    }
-}
-
-// ---- products --------------------------------------------------------------
-
-// out = F v (v null: v = -e); one warp per row r, reading column r (F is
-// symmetric).
-__global__ void wl_matvec(const double* __restrict__ F, int n, const double* __restrict__ v, double* __restrict__ out)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const double* col = F + (size_t)warp * n;
-    double acc = 0.0;
-    for (int c = lane; c < n; c += 32) acc = fma(col[c], v ? v[c] : -1.0, acc);
-    acc = warp_sum(acc);
-    if (lane == 0) out[warp] = acc;
-}
-
-// rhs_r = mu Zi_rr - sum_c Zi_rc dX1_rc dy1_c (columns r by symmetry)
-// r = b - M x (b null: b = -e); one warp per row (columns by symmetry)
-__global__ void wl_resid(const double* __restrict__ M, int n, const double* __restrict__ b,
-                         const double* __restrict__ x, double* __restrict__ r)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const double* col = M + (size_t)warp * n;
-    double acc = 0.0;
-    for (int c = lane; c < n; c += 32) acc = fma(col[c], x[c], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) r[warp] = (b ? b[warp] : -1.0) - acc;
-}
-
-__global__ void wl_rhs(const double* __restrict__ Zi, const double* __restrict__ dX1, const double* __restrict__ dy1,
-                       double mu, int n, double* __restrict__ rhs)
-{
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const size_t o = (size_t)warp * n;
-    double acc = 0.0;
-    for (int c = lane; c < n; c += 32) acc = fma(Zi[o + c] * dX1[o + c], dy1[c], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) rhs[warp] = mu * Zi[o + warp] - acc;
-}
-
-// out(r, c) = sum_k Zi(r, k) (a_k X(k, c) + b_k Y(k, c)) + e1 E1(r, c) + e2 E2(r, c)
-// (b, Y, E2 may be null).  32 x 32 tiles, k in chunks of 32.
-__global__ void wl_gemm(const double* __restrict__ Zi, const double* __restrict__ a, const double* __restrict__ X,
-                        const double* __restrict__ bv, const double* __restrict__ Y, double e1,
-                        const double* __restrict__ E1, double e2, const double* __restrict__ E2, int n,
-                        double* __restrict__ out)
-{
-    __shared__ double sa[WL_TILE][WL_TILE + 1];
-    __shared__ double sb[WL_TILE][WL_TILE + 1];
-    const int r0 = blockIdx.x * WL_TILE, c0 = blockIdx.y * WL_TILE;
-    const int tid = threadIdx.x;
-    const int r = tid % WL_TILE, cc = tid / WL_TILE;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int k0 = 0; k0 < n; k0 += WL_TILE) {
-        for (int e = tid; e < WL_TILE * WL_TILE; e += blockDim.x) {
-            const int p = e % WL_TILE, q = e / WL_TILE;
-            const int rr = r0 + p, kk = k0 + q;
-            sa[p][q] = (rr < n && kk < n) ? Zi[rr + (size_t)kk * n] : 0.0;
-            const int kb = k0 + p, cb = c0 + q;
-            double v = 0.0;
-            if (kb < n && cb < n) {
-                const size_t idx = kb + (size_t)cb * n;
-                v = a[kb] * X[idx];
-                if (bv) v = fma(bv[kb], Y[idx], v);
-            }
-            sb[p][q] = v;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < WL_TILE; ++k) {
-            const double av = sa[r][k];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) acc[t] = fma(av, sb[k][cc + 8 * t], acc[t]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int rr = r0 + r, c = c0 + cc + 8 * t;
-        if (rr >= n || c >= n) continue;
-        const size_t idx = rr + (size_t)c * n;
-        double v = acc[t] + e1 * E1[idx];
-        if (E2) v += e2 * E2[idx];
-        out[idx] = v;
-    }
-}
-
-__global__ void wl_symmetrize(double* __restrict__ A, int n)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (size_t)n * n) return;
-    const int i = (int)(e % n), j = (int)(e / n);
-    if (i <= j) return;
-    const double v = 0.5 * (A[i + (size_t)j * n] + A[j + (size_t)i * n]);
-    A[i + (size_t)j * n] = v;
-    A[j + (size_t)i * n] = v;
-}
-
-// out = alpha a
-__global__ void wl_scale(const double* __restrict__ a, double alpha, int n, double* __restrict__ out)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = alpha * a[i];
-}
-
-// c = a + b elementwise; c may be a (no __restrict__ on a and c)
-__global__ void wl_vadd(const double* a, const double* __restrict__ b, int n, double* c)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) c[i] = a[i] + b[i];
-}
-
-// X += ap dX; y += ad dy; zd += ad dy
-__global__ void wl_step(double* __restrict__ X, const double* __restrict__ dX, double ap, size_t nn,
-                        double* __restrict__ y, double* __restrict__ zd, const double* __restrict__ dy, double ad,
-                        int n)
-{
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < nn) X[e] = fma(ap, dX[e], X[e]);
-    if (e < (size_t)n) {
-        y[e] = fma(ad, dy[e], y[e]);
-        zd[e] = fma(ad, dy[e], zd[e]);
-    }
-}
-
-__global__ void wl_out(double* __restrict__ out, double phi, int iter, int status, double psi, double* stats,
-                       double n3, int ls_total)
-{
-    out[0] = phi;
-    out[1] = (double)iter;
-    out[2] = (double)status;
-    out[3] = psi;
-    if (stats) {
-        atomicAdd(&stats[0], iter * n3);
-        atomicAdd(&stats[1], 1.0);
-        atomicAdd(&stats[2], (double)iter);
-        atomicAdd(&stats[3], (double)ls_total);
-    }
-}
-
-}  // namespace
-
-namespace {
-
-struct WlBufs {
-    double *Zi, *F, *M, *T, *dX, *dX1, *W, *V, *Dinv, *Linv, *y, *zd, *dy, *dy1, *dy2, *r, *t, *sc, *flag;
+struct CoopArgs {
+    const double* L;     // n x n, read only
+    double* Xbase;       // output matrix (X = Xbase + (*xslot) n^2)
+    const int* xslot;
+    double* out;         // phi, iterations, status, <L,X>
+    double* stats;       // IPM work counters (may be null)
+    double *Zi, *F, *M, *T, *dX, *dX1;   // n x n each
+    double *Wb, *Db;                     // 2 x (n x CB), 2 x (CB x CB)
+    double *y, *zd, *dy, *dy1, *dy2, *r, *t;
+    double* part;        // gridDim.x x 4 partial sums
+    unsigned* bar;       // [0] arrivals, [1] generation, [2] error
+    int n;
 };
 
-// The panel sweep of A (n x n) on stream s.  full: the whole sweep (A
-// becomes inv(A)); otherwise only the trailing updates, for the pivots.
-// Non-positive pivots set *flag (not cleared here).
-void wl_sweep(double* A, int n, bool full, const WlBufs& w, cudaStream_t s)
+struct Smem {
+    double D[CB][LDS];    // panel block, then its Cholesky factor (lower)
+    double Li[CB][LDS];   // inverse of the factor (lower)
+    double A1[CB][LDS];   // C_I, or a GEMM operand tile
+    double A2[CB][LDS];   // C_J, or a GEMM operand tile
+    double V1[CB][LDS];   // V_I, or a GEMM operand tile
+    double V2[CB][LDS];   // V_J, or a GEMM operand tile
+    double red[CW * 4];
+    double tot[4];
+    int ok;
+    int pd;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
 {
-    const unsigned tiles = (unsigned)((n + WL_TILE - 1) / WL_TILE);
-    for (int k0 = 0; k0 < n; k0 += WL_B) {
-        const int b = n - k0 < WL_B ? n - k0 : WL_B;
-        wl_panel_factor<<<1, WL_T, 0, s>>>(A, n, k0, b, w.Linv, w.Dinv, w.flag);
-        BQB_COUNT_LAUNCH();
-        if (!full && k0 + b >= n) break;
-        wl_panel_vw<<<wl_blocks((long long)n * 32), WL_T, 0, s>>>(A, n, k0, b, w.Linv, full ? 1 : 0, w.V, w.W);
-        BQB_COUNT_LAUNCH();
-        wl_panel_update<<<dim3(tiles, tiles), WL_T, 0, s>>>(A, n, k0, b, w.V, full ? 0 : 1);
-        BQB_COUNT_LAUNCH();
-        if (full) {
-            wl_panel_fix<<<wl_blocks((long long)n * b), WL_T, 0, s>>>(A, n, k0, b, w.W, w.Dinv);
-            BQB_COUNT_LAUNCH();
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier with a bounded wait.  Returns false once any CTA has given up
+// (then nothing waits any more).  The fences around the arrival make every
+// write before the barrier visible to every read after it.
+__device__ bool grid_sync(unsigned* bar, Smem& sm)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vb = bar;
+        int ok = vb[2] == 0u;
+        if (ok) {
+            const unsigned gen = vb[1];
+            __threadfence();
+            if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                const unsigned long long t0 = global_ns();
+                while (vb[1] == gen) {
+                    if (vb[2] != 0u) {
+                        ok = 0;
+                        break;
+                    }
+                    if (global_ns() - t0 > BAR_TIMEOUT_NS) {
+                        atomicExch(bar + 2, 1u);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        sm.ok = ok;
+    }
+    __syncthreads();
+    return sm.ok != 0;
+}
+
+// Block-reduce four partial sums into part[blockIdx.x * 4 + k].
+__device__ void block_partials(double a, double b, double c, double d, Smem& sm, double* part)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    d = warp_sum(d);
+    if (lane == 0) {
+        sm.red[w * 4 + 0] = a;
+        sm.red[w * 4 + 1] = b;
+        sm.red[w * 4 + 2] = c;
+        sm.red[w * 4 + 3] = d;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int q = 0; q < CW; ++q) s += sm.red[q * 4 + threadIdx.x];
+        part[blockIdx.x * 4 + threadIdx.x] = s;
+    }
+}
+
+// The totals of the partial sums (after a barrier), in CTA order: the same
+// value in every CTA.
+__device__ void grid_totals(const double* part, Smem& sm)
+{
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int g = 0; g < (int)gridDim.x; ++g) s += part[g * 4 + threadIdx.x];
+        sm.tot[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// ---- the panel sweep ---------------------------------------------------------
+
+// Step Q of the register Cholesky of a 32 x 32 block held by one warp
+// (lane p holds row p in s[]): column Q of the factor, then the rank-1
+// update of the rows below.  Instantiated for every Q so that every index
+// into s[] is a constant and s[] stays in registers.  No early exit: after a
+// non-positive pivot (the same d in every lane) the steps go on with a unit
+// pivot and the caller discards the result.
+template <int Q>
+__device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
+{
+    if constexpr (Q < CB) {
+        double d = __shfl_sync(0xffffffffu, s[Q], Q);
+        if (!(d > 0.0)) {
+            pd = 0;
+            d = 1.0;
+        }
+        const double l = sqrt(d);
+        const double lpq = p == Q ? l : s[Q] / l;
+        s[Q] = lpq;
+#pragma unroll
+        for (int r = Q + 1; r < CB; ++r) {
+            const double lrq = __shfl_sync(0xffffffffu, lpq, r);
+            if (r <= p) s[r] = fma(-lpq, lrq, s[r]);
+        }
+        chol_step<Q + 1>(s, p, pd);
+    }
+}
+
+// Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
+// in shared memory.  Warp 0 factors in registers (lane p holds row p; the
+// block is padded to 32 x 32 with the identity), then lane t forms column t
+// of Li by forward substitution.  Returns false (in every thread) on a
+// non-positive pivot.
+__device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm)
+{
+    const int tid = threadIdx.x;
+    for (int e = tid; e < CB * CB; e += CT) {
+        const int p = e % CB, q = e / CB;
+        sm.D[p][q] = p < b && q < b ? A[(k0 + p) + (size_t)(k0 + q) * n] : (p == q ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    if (tid < 32) {
+        const int p = tid;
+        double s[CB];
+#pragma unroll
+        for (int r = 0; r < CB; ++r) s[r] = sm.D[p][r];
+        int pd = 1;
+        chol_step<0>(s, p, pd);
+        if (p == 0) sm.pd = pd;
+        if (pd) {
+#pragma unroll
+            for (int r = 0; r < CB; ++r) sm.D[p][r] = r <= p ? s[r] : 0.0;
+        }
+        __syncwarp();
+        if (pd) {
+            const int t = p;
+            for (int i = 0; i < t; ++i) sm.Li[i][t] = 0.0;
+            for (int i = t; i < CB; ++i) {
+                double acc = i == t ? 1.0 : 0.0;
+                for (int k = t; k < i; ++k) acc = fma(-sm.D[i][k], sm.Li[k][t], acc);
+                sm.Li[i][t] = acc / sm.D[i][i];
+            }
         }
     }
-    if (full) {
-        wl_negate<<<wl_blocks((long long)n * n), WL_T, 0, s>>>(A, (size_t)n * n);
-        BQB_COUNT_LAUNCH();
+    __syncthreads();
+    return sm.pd != 0;
+}
+
+// C rows of tile block I (32 x b): the panel columns of A for rows I, or, for
+// the row block of the previous panel (whose entries still wait for their
+// fix), W_{K-1} transposed.  Then V = C Ld^{-T}: V(r, q) = sum_{p <= q}
+// C(r, p) Li(q, p).
+__device__ void load_v(const double* A, int n, int I, int k0, int b, const double* Wprev, bool from_w,
+                       double (*Cs)[LDS], double (*Vs)[LDS], Smem& sm)
+{
+    const int i0 = I * CB;
+    for (int e = threadIdx.x; e < CB * CB; e += CT) {
+        const int r = e % CB, p = e / CB;
+        const int i = i0 + r;
+        double v = 0.0;
+        if (i < n && p < b) v = from_w ? Wprev[(k0 + p) + (size_t)r * n] : A[i + (size_t)(k0 + p) * n];
+        Cs[r][p] = v;
     }
-    check_launch("ipm_large sweep");
-}
-
-double read_flag(const WlBufs& w, cudaStream_t s)
-{
-    double f = 0.0;
-    BQB_CUDA(cudaMemcpyAsync(&f, w.flag, sizeof(double), cudaMemcpyDeviceToHost, s));
-    BQB_CUDA(cudaStreamSynchronize(s));
-    return f;
-}
-
-}  // namespace
-
-size_t ipm_large_ws_doubles(int n)
-{
-    const size_t nn = (size_t)n * n;
-    return 6 * nn + 2 * (size_t)n * WL_B + 2 * (size_t)WL_B * WL_B + 8 * (size_t)n + 16;
-}
-
-// ipm_mc_pk for n > IPM_REG_NMAX: the same steps as ipm_body_reg, each a
-// multi-CTA kernel on stream s; synchronises with the host at every
-// positive-definiteness decision.  xslot (optional, device): write X into
-// dXbase + (*xslot) * n * n.  Results in dout[0..3] (phi, iterations,
-// status, psi).
-void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, double* dout, cudaStream_t s,
-               const int* xslot)
-{
-    const size_t nn = (size_t)n * n;
-    double* p = wsbuf.ensure(ipm_large_ws_doubles(n));
-    WlBufs w;
-    w.Zi = p;
-    w.F = w.Zi + nn;
-    w.M = w.F + nn;
-    w.T = w.M + nn;
-    w.dX = w.T + nn;
-    w.dX1 = w.dX + nn;
-    w.W = w.dX1 + nn;
-    w.V = w.W + (size_t)n * WL_B;
-    w.Dinv = w.V + (size_t)n * WL_B;
-    w.Linv = w.Dinv + (size_t)WL_B * WL_B;
-    w.y = w.Linv + (size_t)WL_B * WL_B;
-    w.zd = w.y + n;
-    w.dy = w.zd + n;
-    w.dy1 = w.dy + n;
-    w.dy2 = w.dy1 + n;
-    w.r = w.dy2 + n;
-    w.t = w.r + n;
-    w.sc = w.t + n;
-    w.flag = w.sc + 8;
-    double* X = Xbase;
-    if (xslot) {
-        int slot = 0;
-        BQB_CUDA(cudaMemcpyAsync(&slot, xslot, sizeof(int), cudaMemcpyDeviceToHost, s));
-        BQB_CUDA(cudaStreamSynchronize(s));
-        X += (size_t)slot * nn;
+    __syncthreads();
+    for (int e = threadIdx.x; e < CB * CB; e += CT) {
+        const int r = e % CB, q = e / CB;
+        double v = 0.0;
+        for (int p = 0; p <= q; ++p) v = fma(Cs[r][p], sm.Li[q][p], v);
+        Vs[r][q] = q < b ? v : 0.0;
     }
-    const unsigned bn = wl_blocks(n), bnn = wl_blocks((long long)nn), bw = wl_blocks((long long)n * 32);
-    const unsigned tiles = (unsigned)((n + WL_TILE - 1) / WL_TILE);
-    double hs[3];
-    // x = M^{-1} b (b null: -e): x = F b, then one refinement step
-    auto solve = [&](const double* b, double* x) {
-        wl_matvec<<<bw, WL_T, 0, s>>>(w.F, n, b, x);
-        BQB_COUNT_LAUNCH();
-        wl_resid<<<bw, WL_T, 0, s>>>(w.M, n, b, x, w.r);
-        BQB_COUNT_LAUNCH();
-        wl_matvec<<<bw, WL_T, 0, s>>>(w.F, n, w.r, w.t);
-        BQB_COUNT_LAUNCH();
-        wl_vadd<<<bn, WL_T, 0, s>>>(x, w.t, n, x);
-        BQB_COUNT_LAUNCH();
-    };
-    auto sums = [&](int mode) {
-        wl_sums<<<1, 1024, 0, s>>>(mode, n, L, X, w.y, w.zd, w.sc);
-        BQB_COUNT_LAUNCH();
-        BQB_CUDA(cudaMemcpyAsync(hs, w.sc, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        BQB_CUDA(cudaStreamSynchronize(s));
-    };
+    __syncthreads();
+}
 
-    // ---- initial point (src/ipm_mc_pk.c:65-99) ----
-    wl_init_vec<<<bn, WL_T, 0, s>>>(L, n, w.y, w.zd);
-    BQB_COUNT_LAUNCH();
-    wl_identity<<<bnn, WL_T, 0, s>>>(X, n);
-    BQB_COUNT_LAUNCH();
-    sums(0);
-    double psi = hs[0];
-    double mu = hs[1] / (2.0 * n);
-    double phi = hs[2];
+// Phase K of the sweep for tile (I, J).  FULL: the pending fix of panel
+// K - 1 (tiles in its row or column block), the update (I, J != K), W_K of
+// row block I (diagonal tiles) and D^{-1}_K (tile (K, K)).  Trailing only:
+// the update.
+template <bool FULL>
+__device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, const double* Wprev,
+                          const double* Dprev, double* Wcur, double* Dcur, Smem& sm)
+{
+    const bool fixI = FULL && K > 0 && I == K - 1;
+    const bool fixJ = FULL && K > 0 && J == K - 1;
+    const bool upd = I != K && J != K;
+    if (!upd && !fixI && !fixJ && !(FULL && I == K && J == K)) return;
+    if (upd) {
+        load_v(A, n, I, k0, b, Wprev, fixI, sm.A1, sm.V1, sm);
+        if (J != I) load_v(A, n, J, k0, b, Wprev, fixJ, sm.A2, sm.V2, sm);
+    }
+    double (*VJ)[LDS] = J != I ? sm.V2 : sm.V1;
+    const int i0 = I * CB, j0 = J * CB, kp0 = (K - 1) * CB;
+    if (upd || fixI || fixJ) {
+        for (int e = threadIdx.x; e < CB * CB; e += CT) {
+            const int r = e % CB, c = e / CB;
+            const int i = i0 + r, j = j0 + c;
+            if (i >= n || j >= n) continue;
+            double v;
+            if (fixI && fixJ) v = -Dprev[(i - kp0) + (size_t)(j - kp0) * CB];
+            else if (fixJ) v = Wprev[i + (size_t)(j - kp0) * n];
+            else if (fixI) v = Wprev[j + (size_t)(i - kp0) * n];
+            else v = A[i + (size_t)j * n];
+            if (upd) {
+                double acc = 0.0;
+                for (int q = 0; q < b; ++q) acc = fma(sm.V1[r][q], VJ[c][q], acc);
+                v -= acc;
+            }
+            A[i + (size_t)j * n] = v;
+        }
+    }
+    if (FULL && upd && I == J) {
+        // W_K(i, q) = sum_{p >= q} V(i, p) Li(p, q)
+        for (int e = threadIdx.x; e < CB * CB; e += CT) {
+            const int r = e % CB, q = e / CB;
+            const int i = i0 + r;
+            if (i >= n || q >= b) continue;
+            double w = 0.0;
+            for (int p = q; p < b; ++p) w = fma(sm.V1[r][p], sm.Li[p][q], w);
+            Wcur[i + (size_t)q * n] = w;
+        }
+    }
+    if (FULL && I == K && J == K) {
+        // D^{-1}_K = Li^T Li
+        for (int e = threadIdx.x; e < CB * CB; e += CT) {
+            const int p = e % CB, q = e / CB;
+            double acc = 0.0;
+            for (int k = p > q ? p : q; k < b; ++k) acc = fma(sm.Li[k][p], sm.Li[k][q], acc);
+            Dcur[p + (size_t)q * CB] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+// The panel sweep of A (n x n).  FULL: A becomes inv(A); otherwise only the
+// trailing updates run, for the pivots.  Returns 1 (positive definite), 0
+// (a non-positive pivot; every CTA returns 0 at the same panel) or -1 (a
+// barrier gave up).
+template <bool FULL>
+__device__ int sweep(double* A, const CoopArgs& a, Smem& sm)
+{
+    const int n = a.n;
+    const int T = (n + CB - 1) / CB;
+    for (int K = 0; K < T; ++K) {
+        const int k0 = K * CB, b = n - k0 < CB ? n - k0 : CB;
+        if (!panel_factor(A, n, k0, b, sm)) return 0;
+        if (!FULL && K == T - 1) return 1;
+        const double* Wprev = a.Wb + (size_t)((K + 1) & 1) * n * CB;
+        const double* Dprev = a.Db + (size_t)((K + 1) & 1) * CB * CB;
+        double* Wcur = a.Wb + (size_t)(K & 1) * n * CB;
+        double* Dcur = a.Db + (size_t)(K & 1) * CB * CB;
+        const int t0 = FULL ? 0 : K + 1;
+        const int Tt = T - t0;
+        for (int q = blockIdx.x; q < Tt * Tt; q += gridDim.x)
+            tile_step<FULL>(A, n, K, k0, b, t0 + q % Tt, t0 + q / Tt, Wprev, Dprev, Wcur, Dcur, sm);
+        if (!grid_sync(a.bar, sm)) return -1;
+    }
+    if (FULL) {
+        // the last panel's fix, and A = -A
+        const int K = T;
+        const double* Wl = a.Wb + (size_t)((K + 1) & 1) * n * CB;
+        const double* Dl = a.Db + (size_t)((K + 1) & 1) * CB * CB;
+        const int kp0 = (K - 1) * CB;
+        for (int q = blockIdx.x; q < T * T; q += gridDim.x) {
+            const int I = q % T, J = q / T;
+            const bool fixI = I == K - 1, fixJ = J == K - 1;
+            for (int e = threadIdx.x; e < CB * CB; e += CT) {
+                const int i = I * CB + e % CB, j = J * CB + e / CB;
+                if (i >= n || j >= n) continue;
+                double v;
+                if (fixI && fixJ) v = -Dl[(i - kp0) + (size_t)(j - kp0) * CB];
+                else if (fixJ) v = Wl[i + (size_t)(j - kp0) * n];
+                else if (fixI) v = Wl[j + (size_t)(i - kp0) * n];
+                else v = A[i + (size_t)j * n];
+                A[i + (size_t)j * n] = -v;
+            }
+        }
+        if (!grid_sync(a.bar, sm)) return -1;
+    }
+    return 1;
+}
+
+// ---- products ------------------------------------------------------------------
+
+// out = sym(Zi (Diag(-a) X + Diag(-b) Y) + e1 E1 + e2 E2) (b, Y, E2 may be
+// null; the row scales enter negated, -(a_k X_kc) being exactly
+// (-a_k) X_kc): the owner of the tile pair (I, J), (J, I) forms both
+// products and writes the symmetric part.  k in chunks of 32; thread
+// (r, cc) holds P(I0 + r, J0 + c) and P(J0 + c, I0 + r) for c = cc + 8t.
+__device__ void gemm_sym(const double* Zi, const double* av, const double* X, const double* bv, const double* Y,
+                         double e1, const double* E1, double e2, const double* E2, int n, double* out, Smem& sm)
+{
+    const int T = (n + CB - 1) / CB;
+    const int tid = threadIdx.x, r = tid % CB, cc = tid / CB;
+    const int npairs = T * (T + 1) / 2;
+    for (int pq = blockIdx.x; pq < npairs; pq += gridDim.x) {
+        int I = 0, rem = pq;
+        while (rem >= T - I) {
+            rem -= T - I;
+            ++I;
+        }
+        const int J = I + rem;
+        const int i0 = I * CB, j0 = J * CB;
+        double acc1[4] = {0.0, 0.0, 0.0, 0.0}, acc2[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k0 = 0; k0 < n; k0 += CB) {
+            for (int e = tid; e < CB * CB; e += CT) {
+                const int p = e % CB, q = e / CB;
+                const int kk = k0 + q, kb = k0 + p;
+                sm.A1[p][q] = (i0 + p < n && kk < n) ? Zi[(i0 + p) + (size_t)kk * n] : 0.0;
+                sm.A2[p][q] = (j0 + p < n && kk < n) ? Zi[(j0 + p) + (size_t)kk * n] : 0.0;
+                double v1 = 0.0, v2 = 0.0;
+                if (kb < n && j0 + q < n) {
+                    const size_t idx = kb + (size_t)(j0 + q) * n;
+                    v1 = -av[kb] * X[idx];
+                    if (bv) v1 = fma(-bv[kb], Y[idx], v1);
+                }
+                if (kb < n && i0 + q < n) {
+                    const size_t idx = kb + (size_t)(i0 + q) * n;
+                    v2 = -av[kb] * X[idx];
+                    if (bv) v2 = fma(-bv[kb], Y[idx], v2);
+                }
+                sm.V1[p][q] = v1;   // B(k, J0 + q)
+                sm.V2[p][q] = v2;   // B(k, I0 + q)
+            }
+            __syncthreads();
+#pragma unroll 4
+            for (int k = 0; k < CB; ++k) {
+                const double a1 = sm.A1[r][k];
+                const double b2 = sm.V2[k][r];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int c = cc + 8 * t;
+                    acc1[t] = fma(a1, sm.V1[k][c], acc1[t]);
+                    acc2[t] = fma(sm.A2[c][k], b2, acc2[t]);
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int i = i0 + r, j = j0 + cc + 8 * t;
+            if (i >= n || j >= n) continue;
+            const size_t ij = i + (size_t)j * n, ji = j + (size_t)i * n;
+            double vij = acc1[t] + e1 * E1[ij];
+            double vji = acc2[t] + e1 * E1[ji];
+            if (E2) {
+                vij += e2 * E2[ij];
+                vji += e2 * E2[ji];
+            }
+            const double v = i == j ? vij : 0.5 * (vij + vji);
+            out[ij] = v;
+            out[ji] = v;
+        }
+    }
+}
+
+// One warp per row i (the grid's warps in turn): out_i = sum_c F(c, i) v_c
+// (F symmetric; v null: v = -e).
+__device__ void warp_rows_matvec(const double* F, int n, const double* v, double* out)
+{
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * CW;
+    for (int i = blockIdx.x * CW + (threadIdx.x >> 5); i < n; i += nw) {
+        const double* col = F + (size_t)i * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc = fma(col[c], v ? v[c] : -1.0, acc);
+        acc = warp_sum(acc);
+        if (lane == 0) out[i] = acc;
+    }
+}
+
+// r_i = b_i - sum_c M(c, i) x_c (b null: -1)
+__device__ void warp_rows_resid(const double* M, int n, const double* b, const double* x, double* r)
+{
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * CW;
+    for (int i = blockIdx.x * CW + (threadIdx.x >> 5); i < n; i += nw) {
+        const double* col = M + (size_t)i * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc = fma(col[c], x[c], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) r[i] = (b ? b[i] : -1.0) - acc;
+    }
+}
+
+// t = F r; x += t (row i of both by the same warp)
+__device__ void warp_rows_refine(const double* F, int n, const double* r, double* t, double* x)
+{
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * CW;
+    for (int i = blockIdx.x * CW + (threadIdx.x >> 5); i < n; i += nw) {
+        const double* col = F + (size_t)i * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc = fma(col[c], r[c], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            t[i] = acc;
+            x[i] = x[i] + acc;
+        }
+    }
+}
+
+// rhs_i = mu Zi_ii - sum_c Zi_ic dX1_ic dy1_c (columns i by symmetry)
+__device__ void warp_rows_rhs(const double* Zi, const double* dX1, const double* dy1, double mu, int n, double* rhs)
+{
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * CW;
+    for (int i = blockIdx.x * CW + (threadIdx.x >> 5); i < n; i += nw) {
+        const size_t o = (size_t)i * n;
+        double acc = 0.0;
+        for (int c = lane; c < n; c += 32) acc = fma(Zi[o + c] * dX1[o + c], dy1[c], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) rhs[i] = mu * Zi[o + i] - acc;
+    }
+}
+
+// x = M^{-1} b (b null: -e): x = F b, then one refinement step.  Three
+// phases; returns false when a barrier gave up.
+__device__ bool solve(const CoopArgs& a, const double* b, double* x, Smem& sm)
+{
+    warp_rows_matvec(a.F, a.n, b, x);
+    if (!grid_sync(a.bar, sm)) return false;
+    warp_rows_resid(a.M, a.n, b, x, a.r);
+    if (!grid_sync(a.bar, sm)) return false;
+    warp_rows_refine(a.F, a.n, a.r, a.t, x);
+    return grid_sync(a.bar, sm);
+}
+
+__global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    const int n = a.n;
+    const size_t nn = (size_t)n * n;
+    const size_t gtid = (size_t)blockIdx.x * CT + threadIdx.x, gstride = (size_t)gridDim.x * CT;
+    const double* __restrict__ L = a.L;
+    double* X = a.Xbase + (a.xslot ? (size_t)(*a.xslot) * nn : 0);
+
+    // ---- initial point (src/ipm_mc_pk.c:65-99): y_c = sum_r |L_rc| + 1.1,
+    // zd = y - diag(L), X = I; psi = trace(L), mu = sum(zd) / 2n, phi = sum(y)
+    {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (size_t c = gtid; c < (size_t)n; c += gstride) {
+            double acc = 0.0;
+            const double* Lc = L + c * n;
+            for (int r = 0; r < n; ++r) acc += fabs(Lc[r]);
+            const double yc = acc + 1.1;
+            const double zc = yc - Lc[c];
+            a.y[c] = yc;
+            a.zd[c] = zc;
+            s0 += Lc[c];
+            s1 += zc;
+            s2 += yc;
+        }
+        for (size_t e = gtid; e < nn; e += gstride) X[e] = (e % n == e / n) ? 1.0 : 0.0;
+        block_partials(s0, s1, s2, 0.0, sm, a.part);
+    }
+    bool alive = grid_sync(a.bar, sm);
+    grid_totals(a.part, sm);
+    double psi = sm.tot[0];
+    double mu = sm.tot[1] / (2.0 * n);
+    double phi = sm.tot[2];
     double gap = fabs(phi - psi);
     int iter = 0, ls_total = 0, status = IPM_OK;
 
-    while (gap > 1e-2) {
+    while (alive && gap > 1e-2) {
         if (++iter > IPM_MAX_ITERS) {
             status = IPM_MAXITER;
             break;
         }
-        BQB_CUDA(cudaMemsetAsync(w.flag, 0, sizeof(double), s));
         // Zi = inv(Z), Z = Diag(zd) - L off the diagonal
-        wl_fill_z<<<bnn, WL_T, 0, s>>>(L, w.zd, nullptr, 0.0, n, w.Zi);
-        BQB_COUNT_LAUNCH();
-        wl_sweep(w.Zi, n, true, w, s);
-        if (read_flag(w, s) != 0.0) {
+        for (size_t e = gtid; e < nn; e += gstride) {
+            const int i = (int)(e % n), j = (int)(e / n);
+            a.Zi[e] = i == j ? a.zd[i] : -L[e];
+        }
+        if (!(alive = grid_sync(a.bar, sm))) break;
+        int pd = sweep<true>(a.Zi, a, sm);
+        if (pd < 0) {
+            alive = false;
+            break;
+        }
+        if (!pd) {
             status = IPM_Z_NOT_PD;
             break;
         }
-        // F = inv(Zi .* X); dy1 = F (-e)
-        wl_hadamard<<<bnn, WL_T, 0, s>>>(w.Zi, X, nn, w.M);
-        BQB_COUNT_LAUNCH();
-        BQB_CUDA(cudaMemcpyAsync(w.F, w.M, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        wl_sweep(w.F, n, true, w, s);
-        if (read_flag(w, s) != 0.0) {
+        // M = Zi .* X, F = inv(M); dy1 = F (-e)
+        for (size_t e = gtid; e < nn; e += gstride) {
+            const double m = a.Zi[e] * X[e];
+            a.M[e] = m;
+            a.F[e] = m;
+        }
+        if (!(alive = grid_sync(a.bar, sm))) break;
+        pd = sweep<true>(a.F, a, sm);
+        if (pd < 0) {
+            alive = false;
+            break;
+        }
+        if (!pd) {
             status = IPM_M_NOT_PD;
             break;
         }
-        solve(nullptr, w.dy1);
-        // dX1 = Zi (-Diag(dy1) X) - X, symmetrised; the sign goes into the
-        // row scale: a_k = -dy1_k
-        wl_scale<<<bn, WL_T, 0, s>>>(w.dy1, -1.0, n, w.dy2);   // dy2 = -dy1 (scratch)
-        BQB_COUNT_LAUNCH();
-        wl_gemm<<<dim3(tiles, tiles), WL_T, 0, s>>>(w.Zi, w.dy2, X, nullptr, nullptr, -1.0, X, 0.0, nullptr, n,
-                                                     w.dX1);
-        BQB_COUNT_LAUNCH();
-        wl_symmetrize<<<bnn, WL_T, 0, s>>>(w.dX1, n);
-        BQB_COUNT_LAUNCH();
+        if (!(alive = solve(a, nullptr, a.dy1, sm))) break;
+        // dX1 = sym(Zi (-Diag(dy1) X) - X)
+        gemm_sym(a.Zi, a.dy1, X, nullptr, nullptr, -1.0, X, 0.0, nullptr, n, a.dX1, sm);
+        if (!(alive = grid_sync(a.bar, sm))) break;
         // corrector: rhs = mu diag(Zi) - (Zi .* dX1) dy1; dy2 = F rhs
-        wl_rhs<<<bw, WL_T, 0, s>>>(w.Zi, w.dX1, w.dy1, mu, n, w.dy);
-        BQB_COUNT_LAUNCH();
-        solve(w.dy, w.dy2);
-        // dX = Zi (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1, symmetrised
-        wl_scale<<<bn, WL_T, 0, s>>>(w.dy2, -1.0, n, w.dy);   // dy = -dy2
-        BQB_COUNT_LAUNCH();
-        wl_scale<<<bn, WL_T, 0, s>>>(w.dy1, -1.0, n, w.T);    // T[0..n) = -dy1 (T is free here)
-        BQB_COUNT_LAUNCH();
-        wl_gemm<<<dim3(tiles, tiles), WL_T, 0, s>>>(w.Zi, w.dy, X, w.T, w.dX1, 1.0, w.dX1, mu, w.Zi, n, w.dX);
-        BQB_COUNT_LAUNCH();
-        wl_symmetrize<<<bnn, WL_T, 0, s>>>(w.dX, n);
-        BQB_COUNT_LAUNCH();
-        wl_vadd<<<bn, WL_T, 0, s>>>(w.dy1, w.dy2, n, w.dy);
-        BQB_COUNT_LAUNCH();
+        warp_rows_rhs(a.Zi, a.dX1, a.dy1, mu, n, a.dy);
+        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (!(alive = solve(a, a.dy, a.dy2, sm))) break;
+        // dX = sym(Zi (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1)
+        gemm_sym(a.Zi, a.dy2, X, a.dy1, a.dX1, 1.0, a.dX1, mu, a.Zi, n, a.dX, sm);
+        if (!(alive = grid_sync(a.bar, sm))) break;
+        for (size_t c = gtid; c < (size_t)n; c += gstride) a.dy[c] = a.dy1[c] + a.dy2[c];
 
         // primal line search: X + ap dX positive definite
         double ap = 1.0;
         int trials = 0;
         bool ok = false;
         while (true) {
-            BQB_CUDA(cudaMemsetAsync(w.flag, 0, sizeof(double), s));
-            wl_axpy<<<bnn, WL_T, 0, s>>>(X, w.dX, ap, nn, w.T);
-            BQB_COUNT_LAUNCH();
-            wl_sweep(w.T, n, false, w, s);
-            if (read_flag(w, s) == 0.0) {
+            for (size_t e = gtid; e < nn; e += gstride) a.T[e] = fma(ap, a.dX[e], X[e]);
+            if (!(alive = grid_sync(a.bar, sm))) break;
+            pd = sweep<false>(a.T, a, sm);
+            if (pd < 0) {
+                alive = false;
+                break;
+            }
+            // every CTA leaves the trailing sweep after reading the panel
+            // block; the next trial rewrites T, so wait for all of them
+            if (!(alive = grid_sync(a.bar, sm))) break;
+            if (pd) {
                 ok = true;
                 break;
             }
             if (++trials >= IPM_MAX_TRIALS) break;
             ap *= 0.8;
         }
+        if (!alive) break;
         ls_total += trials + 1;
         if (!ok) {
             status = IPM_LINESEARCH;
@@ -598,17 +628,25 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
         trials = 0;
         ok = false;
         while (true) {
-            BQB_CUDA(cudaMemsetAsync(w.flag, 0, sizeof(double), s));
-            wl_fill_z<<<bnn, WL_T, 0, s>>>(L, w.zd, w.dy, ad, n, w.T);
-            BQB_COUNT_LAUNCH();
-            wl_sweep(w.T, n, false, w, s);
-            if (read_flag(w, s) == 0.0) {
+            for (size_t e = gtid; e < nn; e += gstride) {
+                const int i = (int)(e % n), j = (int)(e / n);
+                a.T[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
+            }
+            if (!(alive = grid_sync(a.bar, sm))) break;
+            pd = sweep<false>(a.T, a, sm);
+            if (pd < 0) {
+                alive = false;
+                break;
+            }
+            if (!(alive = grid_sync(a.bar, sm))) break;
+            if (pd) {
                 ok = true;
                 break;
             }
             if (++trials >= IPM_MAX_TRIALS) break;
             ad *= 0.8;
         }
+        if (!alive) break;
         ls_total += trials + 1;
         if (!ok) {
             status = IPM_LINESEARCH;
@@ -616,18 +654,135 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
         }
         if (ad < 1.0) ad *= 0.95;
 
-        // update (src/ipm_mc_pk.c:313-334)
-        wl_step<<<bnn, WL_T, 0, s>>>(X, w.dX, ap, nn, w.y, w.zd, w.dy, ad, n);
-        BQB_COUNT_LAUNCH();
-        sums(1);
-        mu = hs[0] / (2.0 * n);
+        // update (src/ipm_mc_pk.c:313-334): X += ap dX, y += ad dy,
+        // zd += ad dy, and the sums zx = <Z, X>, lx = <L, X>, sum(y) of the
+        // new point.  The diagonal of X goes with the vectors (the thread
+        // that moves zd_i also moves X_ii).
+        {
+            double zx = 0.0, lx = 0.0, ys = 0.0;
+            for (size_t e = gtid; e < nn; e += gstride) {
+                const int i = (int)(e % n), j = (int)(e / n);
+                if (i == j) continue;
+                const double xv = fma(ap, a.dX[e], X[e]);
+                X[e] = xv;
+                const double lv = L[e];
+                lx = fma(lv, xv, lx);
+                zx = fma(-lv, xv, zx);
+            }
+            for (size_t c = gtid; c < (size_t)n; c += gstride) {
+                const size_t e = c * n + c;
+                const double xv = fma(ap, a.dX[e], X[e]);
+                X[e] = xv;
+                const double yv = fma(ad, a.dy[c], a.y[c]);
+                const double zv = fma(ad, a.dy[c], a.zd[c]);
+                a.y[c] = yv;
+                a.zd[c] = zv;
+                lx = fma(L[e], xv, lx);
+                zx = fma(zv, xv, zx);
+                ys += yv;
+            }
+            block_partials(zx, lx, ys, 0.0, sm, a.part);
+        }
+        if (!(alive = grid_sync(a.bar, sm))) break;
+        grid_totals(a.part, sm);
+        mu = sm.tot[0] / (2.0 * n);
         if (ap + ad > 1.6) mu *= 0.5;
         if (ap + ad > 1.9) mu *= 0.2;
-        phi = hs[2];
-        psi = hs[1];
+        phi = sm.tot[2];
+        psi = sm.tot[1];
         gap = fabs(phi - psi);
+        // (the partials are rewritten only after the next iteration's
+        // barriers, so no barrier is needed here)
     }
-    wl_out<<<1, 1, 0, s>>>(dout, phi, iter, status, psi, ipm_stats_device(), (double)n * n * n, ls_total);
+    if (!alive) status = IPM_SYNC;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out[0] = phi;
+        a.out[1] = (double)iter;
+        a.out[2] = (double)status;
+        a.out[3] = psi;
+        if (a.stats) {
+            const double n3 = (double)n * n * n;
+            atomicAdd(&a.stats[0], iter * n3);
+            atomicAdd(&a.stats[1], 1.0);
+            atomicAdd(&a.stats[2], (double)iter);
+            atomicAdd(&a.stats[3], (double)ls_total);
+        }
+    }
+}
+
+struct CoopConfig {
+    int grid = 0;
+    size_t smem = 0;
+};
+
+// Grid size for n: one CTA per 32 x 32 tile of the sweep, at most as many
+// as can be co-resident (one per SM at this register count).
+CoopConfig coop_config(int n)
+{
+    static int max_blocks = -1;
+    static std::atomic<int> ready{0};
+    CoopConfig c;
+    c.smem = sizeof(Smem);
+    BQB_SMEM_LIMIT(ipm_coop_kernel, c.smem);   // per device (cached)
+    if (!ready.load()) {
+        int per_sm = 0;
+        BQB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ipm_coop_kernel, CT, c.smem));
+        max_blocks = per_sm * rt().num_sms;
+        ready.store(1);
+    }
+    const int T = (n + CB - 1) / CB;
+    int g = T * T;
+    if (g > max_blocks) g = max_blocks;
+    if (g < 1) g = 1;
+    c.grid = g;
+    return c;
+}
+
+}  // namespace
+
+size_t ipm_large_ws_doubles(int n)
+{
+    const size_t nn = (size_t)n * n;
+    return 6 * nn + 2 * (size_t)n * CB + 2 * (size_t)CB * CB + 8 * (size_t)n + 4 * 1024 + 16;
+}
+
+// ipm_mc_pk for n > IPM_REG_NMAX: one cooperative launch on stream s, no
+// host synchronisation.  xslot (optional, device): write X into
+// Xbase + (*xslot) * n * n.  Results in dout[0..3] (phi, iterations, status,
+// psi); status IPM_SYNC when a grid barrier gave up waiting.
+void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, double* dout, cudaStream_t s,
+               const int* xslot)
+{
+    const size_t nn = (size_t)n * n;
+    double* p = wsbuf.ensure(ipm_large_ws_doubles(n));
+    CoopArgs a;
+    a.L = L;
+    a.Xbase = Xbase;
+    a.xslot = xslot;
+    a.out = dout;
+    a.stats = ipm_stats_device();
+    a.n = n;
+    a.Zi = p;
+    a.F = a.Zi + nn;
+    a.M = a.F + nn;
+    a.T = a.M + nn;
+    a.dX = a.T + nn;
+    a.dX1 = a.dX + nn;
+    a.Wb = a.dX1 + nn;
+    a.Db = a.Wb + 2 * (size_t)n * CB;
+    a.y = a.Db + 2 * (size_t)CB * CB;
+    a.zd = a.y + n;
+    a.dy = a.zd + n;
+    a.dy1 = a.dy + n;
+    a.dy2 = a.dy1 + n;
+    a.r = a.dy2 + n;
+    a.t = a.r + n;
+    a.part = a.t + n;
+    a.bar = reinterpret_cast<unsigned*>(a.part + 4 * 1024);
+    const CoopConfig c = coop_config(n);
+    BQB_CUDA(cudaMemsetAsync(a.bar, 0, 4 * sizeof(unsigned), s));
+    void* args[] = {&a};
+    BQB_CUDA(cudaLaunchCooperativeKernel((const void*)ipm_coop_kernel, dim3(c.grid), dim3(CT), args, c.smem, s));
     BQB_COUNT_LAUNCH();
     check_launch("ipm_large");
 }

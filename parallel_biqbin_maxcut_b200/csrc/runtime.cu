@@ -76,17 +76,24 @@ void fatal(const char* where, const char* msg)
 
 cudaError_t raise_smem_limit(const void* fn, size_t bytes)
 {
-    constexpr int kMaxFns = 64;
+    // the attribute is a setting of the function on the current device:
+    // one cached limit per (device, function)
+    constexpr int kMax = 256;
     static std::mutex mu;
-    static const void* fns[kMaxFns];
-    static size_t limit[kMaxFns];
+    static const void* fns[kMax];
+    static int devs[kMax];
+    static size_t limit[kMax];
     static int used = 0;
+    int dev = 0;
+    const cudaError_t ge = cudaGetDevice(&dev);
+    if (ge != cudaSuccess) return ge;
     std::lock_guard<std::mutex> lock(mu);
     int i = 0;
-    while (i < used && fns[i] != fn) ++i;
+    while (i < used && !(fns[i] == fn && devs[i] == dev)) ++i;
     if (i == used) {
-        if (used == kMaxFns) return cudaErrorInvalidValue;
+        if (used == kMax) return cudaErrorInvalidValue;
         fns[used] = fn;
+        devs[used] = dev;
         limit[used] = 0;
         ++used;
     }
