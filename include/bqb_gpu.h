@@ -375,11 +375,15 @@ int bqb_ipm_batch_device(const double *const *Ls, double *const *Xs, const int *
  * allocation).  L, X: device pointers, n x n column-major; out: device, 4
  * doubles (phi, iterations, status, <L,X>).  Scratch is a fixed array in the
  * library's static device memory (3 * 128^2 doubles per GPU, held until
- * exit), so n <= BQB_IPM_NOALLOC_NMAX; larger n returns 1 with a message in
- * bqb_last_error().  The first call on a device resolves the array's address
- * and should precede any stream capture.  Calls share the array: calls that
- * overlap on the GPU race.  Asynchronous on `stream` (a cudaStream_t; NULL =
- * the legacy default stream).  Returns 0 on success, 2 on a CUDA error. */
+ * exit), so n <= BQB_IPM_NOALLOC_NMAX.  The first call on a device resolves
+ * the array's address and should precede any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race.  Asynchronous on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).  Returns 0 on success;
+ * 1, with a message in bqb_last_error(), when n < 1 or n > 128, when L, X or
+ * out is NULL, or when the IPM's placement for this n on this device needs
+ * more scratch than the array holds (the placement keeps the Cholesky
+ * workspace in shared memory; a device with less opt-in shared memory than
+ * a B200 would need it in the array); 2 on a CUDA error. */
 #define BQB_IPM_NOALLOC_NMAX 128
 int bqb_ipm_noalloc(const double *L, double *X, int n, double *out, void *stream);
 
