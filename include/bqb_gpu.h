@@ -238,6 +238,17 @@ void bqb_set_heuristic_hook(bqb_heuristic_fn fn);
  * calls are not counted). */
 long long bqb_heuristic_runs(int reset);
 
+/* Tensor-core product D = A B^T (tcgen05.mma kind::tf32, FP32 accumulation
+ * in tensor memory, operands staged by TMA): the kernel behind the batched
+ * Goemans-Williamson projection S = Lf V of many hyperplanes at once (the
+ * reference projects one hyperplane at a time, src/heuristic.c:142-151).
+ * A: M x K and B: N x K row-major FP32 device arrays with row pitch Kp (a
+ * multiple of 32, zeros beyond K, 16-byte aligned); D: M x N column-major
+ * FP32 (leading dimension M).  Synchronous on the library stream.  Returns
+ * 0; 1 on bad sizes or no tensor-map encoder; 2 on a CUDA error or a
+ * bounded wait inside the kernel that ran out.  No reference counterpart. */
+int bqb_tc_gemm_tf32(const float *A, const float *B, float *D, int M, int N, int Kp);
+
 /* The same B&B with the nodes bounded in batches by the fused node kernel
  * (bqb_fused_submit / bqb_fused_collect): after the root (rank 0, library
  * globals), batches of at most `batch` open nodes with the largest parent
