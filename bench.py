@@ -80,7 +80,8 @@ TORUS_NAME = ("3D torus 7x7x7 (n = 343), couplings N(0,1) x 1e5 rounded, seed 1,
 LEG_CALLS = {
     "fused": "bqb_solve_fused (batches of 2 x SMs, 8 in flight), FP64",
     "fused_learned": "bqb_solve_fused (batches of 2 x SMs, 8 in flight) with the shipped warm-start model",
-    "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply)",
+    "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply), "
+               "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32)",
     "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
 }
 
@@ -441,7 +442,7 @@ def run_gpu(args):
                   [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w)])]
         if args.tto_torus:
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
-                          [("engines", dict(threads=16), None)]))
+                          [("engines", dict(threads=16, gw_hyperplanes=4096), None)]))
         tto = {}
         for key, name, A, legs in cases:
             e = {"instance": name}

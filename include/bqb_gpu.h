@@ -248,6 +248,16 @@ long long bqb_heuristic_runs(int reset);
  * 0; 1 on bad sizes or no tensor-map encoder; 2 on a CUDA error or a
  * bounded wait inside the kernel that ran out.  No reference counterpart. */
 int bqb_tc_gemm_tf32(const float *A, const float *B, float *D, int M, int N, int Kp);
+/* Hyperplanes per Goemans-Williamson round of the concurrent engines'
+ * heuristic (bqb_bound_nodes, bqb_solve_parallel, and the engines behind
+ * bqb_solve_fused above 128 vertices).  0, the default: the reference's
+ * P0_N hyperplanes per round, drawn on the host in rand() order
+ * (src/heuristic.c:83,142-143).  H > 0: H hyperplanes per round drawn on the
+ * device and projected at once by bqb_tc_gemm_tf32's kernel with the sign
+ * in its epilogue, then 1-opt and exact evaluation of every cut as before.
+ * The drop-in entry points always follow the reference.  Clamped to
+ * 0..65536.  No reference counterpart. */
+void bqb_set_gw_hyperplanes(int H);
 
 /* The same B&B with the nodes bounded in batches by the fused node kernel
  * (bqb_fused_submit / bqb_fused_collect): after the root (rank 0, library

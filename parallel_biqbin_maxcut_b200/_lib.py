@@ -123,6 +123,7 @@ SIGNATURES = {
     "bqb_fused_phase_calls": (None, [C.POINTER(C.c_longlong)]),
     "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),
+    "bqb_set_gw_hyperplanes": (None, [C.c_int]),
     "bqb_warm_train": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_uint, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "bqb_warm_grad": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
@@ -228,12 +229,15 @@ def make_params(**overrides) -> Params:
 
 
 def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: int = 4,
-          **param_overrides) -> dict:
+          gw_hyperplanes: int = 0, **param_overrides) -> dict:
     """Solve Max-Cut on ``adj`` to optimality (best-first B&B, GPU bounding;
     ``threads`` > 1 bounds that many nodes concurrently on engines;
     ``fused_batch`` > 0 bounds batches of up to that many nodes with the
-    fused node kernel, ``fused_depth`` batches in flight)."""
+    fused node kernel, ``fused_depth`` batches in flight; ``gw_hyperplanes``
+    > 0: the engines' GW rounds project that many hyperplanes at once on
+    the tensor cores)."""
     lib = load()
+    lib.bqb_set_gw_hyperplanes(int(gw_hyperplanes))
     A = np.ascontiguousarray(adj, dtype=np.float64)
     p = make_params(**param_overrides)
     res = SolveResult()

@@ -7,6 +7,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <vector>
 
 #include "engine.h"
@@ -76,15 +77,46 @@ double gw_round_host(HeurState& st, Rng& rng, const double* dPL, int n, const do
     return num > 0 ? st.hval.p[0] : -BIG_NUMBER;
 }
 
+// A GW round of H hyperplanes at once: the hyperplanes are drawn on the
+// device from a seed taken from the engine's stream (two draws), projected
+// on the tensor cores with the sign in the epilogue (gw_project_tf32), then
+// 1-opt, lifting, exact evaluation and the first best as in every round.
+double gw_round_batched(HeurState& st, Rng& rng, const double* dPL, int n, const double* dP0L, int N0, int H,
+                        int* x, cudaStream_t s)
+{
+    const unsigned long long seed =
+        ((unsigned long long)(unsigned)rng.next() << 31) ^ (unsigned long long)(unsigned)rng.next();
+    BQB_CUDA(cudaMemsetAsync(st.status.p, 0, 2 * sizeof(int), s));
+    const cudaError_t e = gw_project_tf32(st.Z.p, n, H, seed, st.x.p, st.Vf, st.tcerr, s);
+    if (e != cudaSuccess) fatal("GW_heuristic (batched projection)", cudaGetErrorString(e));
+    gw_round_finish(st, dPL, n, dP0L, N0, H, s);
+    int terr = 0;
+    BQB_CUDA(cudaMemcpyAsync(st.hbest.p, st.best.p, (size_t)N0 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(st.hval.p, st.bestval.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(st.hstat.p, st.status.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaMemcpyAsync(&terr, st.tcerr.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BQB_CUDA(cudaStreamSynchronize(s));
+    if (terr) fatal("GW_heuristic", "a bounded wait in the tensor-core projection ran out");
+    if (st.hstat.p[1]) fatal("GW_heuristic", "1-opt did not terminate");
+    memcpy(x, st.hbest.p + 1, (size_t)(N0 - 1) * sizeof(int));
+    return st.hval.p[0];
+}
+
+std::atomic<int> g_gw_hyperplanes{0};
+
 }  // namespace
 
+int gw_hyperplanes() { return g_gw_hyperplanes.load(); }
+
 // runHeuristic_unpacked (src/heuristic.c:19-115) with device-resident X, P_L
-// and P0_L.  x: host, length N0 - 1.
+// and P0_L.  x: host, length N0 - 1.  hyperplanes > 0: every GW round
+// projects that many device-drawn hyperplanes at once on the tensor cores
+// (gw_round_batched) instead of N0 host-drawn ones in rand() order.
 double heuristic_device(HeurState& st, Rng& rng, const double* dX, const double* dPL, int n, const double* dP0L,
-                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s)
+                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s, int hyperplanes)
 {
     const int N = N0 - 1;
-    const int num = N0;
+    const int num = hyperplanes > 0 ? hyperplanes : N0;
     ensure_round_buffers(st, n, N0, num);
     upload_fixed(st, xfixed, sol, N, s);
 
@@ -122,7 +154,8 @@ double heuristic_device(HeurState& st, Rng& rng, const double* dX, const double*
             fatal("runHeuristic_unpacked", "Problem with Cholesky factorization");
             return heur_val;
         }
-        heur_val = gw_round_host(st, rng, dPL, n, dP0L, N0, num, x, s);
+        heur_val = hyperplanes > 0 ? gw_round_batched(st, rng, dPL, n, dP0L, N0, num, x, s)
+                                   : gw_round_host(st, rng, dPL, n, dP0L, N0, num, x, s);
         if (heur_val > fh) {
             done = 0;
             fh = heur_val;
@@ -231,4 +264,14 @@ BQB_API int update_best(int* xbest, int* xnew, double* best, int P0_N)
         return 1;
     }
     return 0;
+}
+
+// Hyperplanes per GW round for the concurrent engines and the solvers built
+// on them (0, the default: the reference's P0_N hyperplanes drawn on the host
+// in rand() order; H > 0: H hyperplanes drawn on the device and projected at
+// once on the tensor cores).  The drop-in entry points always follow the
+// reference.  Values above 65536 are clamped.
+BQB_API void bqb_set_gw_hyperplanes(int H)
+{
+    g_gw_hyperplanes.store(H < 0 ? 0 : (H > 65536 ? 65536 : H));
 }

@@ -235,6 +235,11 @@ void gw_round_device(HeurState& st, const double* dPL, int n, const double* dP0L
     dim3 pg((n + 127) / 128, num);
     gw_project_kernel<<<pg, 128, 0, s>>>(st.Z.p, st.V.p, n, st.x.p);
     BQB_COUNT_LAUNCH();
+    gw_round_finish(st, dPL, n, dP0L, N0, num, s);
+}
+
+void gw_round_finish(HeurState& st, const double* dPL, int n, const double* dP0L, int N0, int num, cudaStream_t s)
+{
     one_opt_device(st, dPL, n, num, s);
     eval_kernel<<<num, 128, 0, s>>>(dP0L, N0, st.x.p, n, st.fixed.p, st.sols.p, st.vals.p, 1);
     BQB_COUNT_LAUNCH();

@@ -16,6 +16,8 @@ struct HeurState {
     DevBuf<int> fixed;         // 2 x (N0-1): xfixed, sol
     DevBuf<int> status;        // [0] potrf status, [1] 1-opt overflow
     DevBuf<double> P0L, PL, Xs; // staging for host-pointer entry points
+    DevBuf<float> Vf;          // batched rounding: FP32 factor and hyperplanes
+    DevBuf<int> tcerr;         // batched rounding: the tensor-core kernel's error word
     HostBuf<double> hV;
     HostBuf<int> hbest;
     HostBuf<double> hval;
@@ -34,6 +36,16 @@ void remix_device(double* dZ, const double* dX, const double* dxh, double c, int
 // Results: st.best (device), st.bestval (device).
 void gw_round_device(HeurState& st, const double* dPL, int n, const double* dP0L, int N0, int num,
                      cudaStream_t s);
+
+// The steps of a GW round after the projection (cuts already in st.x):
+// 1-opt, lift, evaluate, keep the first best.
+void gw_round_finish(HeurState& st, const double* dPL, int n, const double* dP0L, int N0, int num, cudaStream_t s);
+
+// Batched rounding on the tensor cores (csrc/gw_tc.cu): x[h * n + i] =
+// sign((Lf v_h)_i) for H hyperplanes drawn on the device from `seed`, Lf the
+// lower factor in st.Z.
+cudaError_t gw_project_tf32(const double* Lf, int n, int H, unsigned long long seed, int* x, DevBuf<float>& ws,
+                            DevBuf<int>& err, cudaStream_t s);
 
 // 1-opt alone on `count` cuts stored as rows of st.x (n ints each); writes
 // the final cost of cut h to st.vals[h].

@@ -39,6 +39,10 @@ std::vector<CutRec> pack_global_cuts(const Problem* P);
 // runHeuristic_unpacked (src/heuristic.c:19-115) with device X, P_L and
 // P0_L, device state st and random stream rng.  x: host, length N0 - 1.
 double heuristic_device(HeurState& st, Rng& rng, const double* dX, const double* dPL, int n, const double* dP0L,
-                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s);
+                        int N0, const int* xfixed, const int* sol, int* x, cudaStream_t s, int hyperplanes = 0);
+
+// Hyperplanes per GW round of the engines' heuristic (bqb_set_gw_hyperplanes;
+// 0: the reference's count N0 with host draws in rand() order).
+int gw_hyperplanes();
 
 }  // namespace bqb

@@ -153,7 +153,8 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             BQB_CUDA(cudaStreamSynchronize(s));
             hook(SP_->L, N0, hostL.data(), n, node->xfixed, node->sol.X, x.data());
         } else {
-            heuristic_device(E.heur, E.rng, dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s);
+            heuristic_device(E.heur, E.rng, dX, dL, n, nd.P0L.p, N0, node->xfixed, node->sol.X, x.data(), s,
+                             E.is_default ? 0 : gw_hyperplanes());
         }
         updateSolution(x.data());
     };
