@@ -272,6 +272,20 @@ void bqb_set_gw_hyperplanes(int H);
 int bqb_solve_fused(const double *adj, int num_vertices, const BiqBinParameters *prm, int batch, int depth,
                     bqb_solve_result *out);
 
+/* The same B&B with the open-node pool on the device: after the root (rank
+ * 0, library globals), one persistent launch of the fused node kernel runs
+ * the whole tree, each CTA popping the open node with the largest parent
+ * bound (src/heap.c:27-133), bounding it with rank 1, branching it as the
+ * reference's workers do (src/bab_functions.c:224-336, getBranchingVariable)
+ * and pushing its two children, until no node is open; the incumbent lives
+ * on the device.  Nodes the kernel flags are bounded by engines on the host
+ * and their children pushed back.  pool_nodes: node records on the device
+ * (<= 0: 65536).  Problems above 128 vertices go to bqb_solve_parallel.
+ * Returns 0, 1 on bad input or a full pool, 2 on an engine error.  No
+ * reference counterpart (the reference keeps one heap per MPI process). */
+int bqb_solve_device(const double *adj, int num_vertices, const BiqBinParameters *prm, int pool_nodes,
+                     bqb_solve_result *out);
+
 /* Bound `count` independent nodes of the problem set up by
  * process_adj_matrix (SP) with `threads` concurrent engines: bounds[i] is
  * SDPbound(nodes[i], SP, <engine subproblem>, rank) (src/bounding.c:24-342)

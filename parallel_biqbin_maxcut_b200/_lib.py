@@ -110,6 +110,7 @@ SIGNATURES = {
     "bqb_solve": (C.c_int, [D, C.c_int, C.c_void_p, C.c_void_p]),
     "bqb_solve_parallel": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "bqb_solve_fused": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "bqb_solve_device": (C.c_int, [D, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "bqb_bound_nodes": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_void_p), D]),
     "bqb_bound_nodes_fused": (C.c_int, [C.POINTER(BabNode), C.c_int, C.c_int, D]),
@@ -229,13 +230,14 @@ def make_params(**overrides) -> Params:
 
 
 def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: int = 4,
-          gw_hyperplanes: int = 0, **param_overrides) -> dict:
+          gw_hyperplanes: int = 0, device_pool: bool = False, pool_nodes: int = 0, **param_overrides) -> dict:
     """Solve Max-Cut on ``adj`` to optimality (best-first B&B, GPU bounding;
     ``threads`` > 1 bounds that many nodes concurrently on engines;
     ``fused_batch`` > 0 bounds batches of up to that many nodes with the
     fused node kernel, ``fused_depth`` batches in flight; ``gw_hyperplanes``
     > 0: the engines' GW rounds project that many hyperplanes at once on
-    the tensor cores)."""
+    the tensor cores; ``device_pool``: the whole tree in one persistent
+    launch with the open-node pool on the device)."""
     lib = load()
     lib.bqb_set_gw_hyperplanes(int(gw_hyperplanes))
     A = np.ascontiguousarray(adj, dtype=np.float64)
@@ -243,7 +245,9 @@ def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: 
     res = SolveResult()
     pp = C.cast(C.pointer(p), C.c_void_p)
     rp = C.cast(C.pointer(res), C.c_void_p)
-    if fused_batch > 0:
+    if device_pool:
+        rc = lib.bqb_solve_device(dptr(A), A.shape[0], pp, int(pool_nodes), rp)
+    elif fused_batch > 0:
         rc = lib.bqb_solve_fused(dptr(A), A.shape[0], pp, int(fused_batch), int(fused_depth), rp)
     elif threads > 1:
         rc = lib.bqb_solve_parallel(dptr(A), A.shape[0], pp, int(threads), rp)

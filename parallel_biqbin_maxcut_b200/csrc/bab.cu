@@ -775,3 +775,74 @@ BQB_API int bqb_solve_fused(const double* adj, int num_vertices, const BiqBinPar
     }
     return rc;
 }
+
+// ---- B&B with the node pool on the device -------------------------------
+// The root is bounded with rank 0 on the library globals (sets diff) as the
+// reference's master does; its two children seed the device-resident pool
+// (fused_pool_bab: nodek_kernel pops the open node with the largest parent
+// bound, bounds it with rank 1, branches it (src/bab_functions.c:224-336)
+// and pushes its children, all on the device).  Problems the fused kernel
+// does not take (N0 > 128) go to bqb_solve_parallel.  `pool_nodes`: node
+// records on the device (<= 0: 65536).
+BQB_API int bqb_solve_device(const double* adj, int num_vertices, const BiqBinParameters* prm, int pool_nodes,
+                             bqb_solve_result* out)
+{
+    if (num_vertices < 3 || num_vertices > BQB_NMAX) return 1;
+    if (num_vertices > 128) return bqb_solve_parallel(adj, num_vertices, prm, 16, out);
+    if (prm) {
+        params = *prm;
+    } else {
+        bqb_default_params(&params);
+        params.init_bundle_iter = 5;
+        params.violated_TriIneq = 0.05;
+    }
+    std::vector<double> A(adj, adj + (size_t)num_vertices * num_vertices);
+    process_adj_matrix(A.data(), num_vertices);
+    if (params.adjust_TriIneq) params.TriIneq = SP->n * 10;
+    srand(2020);
+    BabSol = solver_solution();
+    g_LB.store(0.0);
+    g_num_nodes = 0;
+    stopped = 0;
+    diff = 0.0;
+    alloc_globals(SP->n);
+
+    TIME = wtime();
+    BabNode* root = new_node(nullptr);
+    g_num_nodes = 1;
+    root_bound = Evaluate(root, SP, PP, 0);
+    root->upper_bound = root_bound;
+    std::vector<BabNode> open;
+    if (Bab_LBGet() + 1.0 < root->upper_bound && !params.root) {
+        const int ic = getBranchingVariable(root);
+        for (int xic = 0; xic <= 1; ++xic) {
+            BabNode child = *root;
+            child.xfixed[ic] = 1;
+            child.sol.X[ic] = xic;
+            child.upper_bound = root->upper_bound;
+            child.level = root->level + 1;
+            open.push_back(child);
+        }
+    }
+    free(root);
+    int rc = 0;
+    if (!open.empty()) {
+        long long created = 0, evaluated = 0;
+        int st = 0;
+        const double budget = params.time_limit > 0 ? params.time_limit - (wtime() - TIME) : 0.0;
+        rc = bqb::fused_pool_bab(open, pool_nodes > 0 ? pool_nodes : 65536, budget > 0 ? budget : 0.0, &created,
+                            &evaluated, &st);
+        g_num_nodes = 1 + (int)created;
+        stopped = st;
+    }
+    if (out) {
+        out->best_value = Bab_LBGet();
+        out->root_bound = root_bound;
+        out->nodes = g_num_nodes;
+        out->stopped = stopped;
+        out->seconds = wtime() - TIME;
+        out->num_vertices = num_vertices;
+        for (int i = 0; i < BQB_NMAX; ++i) out->solution[i] = (i < BabPbSize) ? BabSol->X[i] : 0;
+    }
+    return rc;
+}

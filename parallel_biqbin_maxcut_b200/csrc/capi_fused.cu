@@ -43,6 +43,7 @@ extern "C" {
 double Bab_LBGet(void);
 int Bab_LBUpd(double new_lb, BabSolution* bs);
 int bqb_bound_nodes(BabNode* nodes, int count, int rank, int threads, const double* const* L_dev, double* bounds);
+int getBranchingVariable(BabNode* node);
 extern double diff;
 }
 
@@ -417,7 +418,253 @@ int collect(FusedState& F, FusedSub& S, BabNode* nodes, double* bounds)
     return 0;
 }
 
+// The device-resident node pool's buffers (one pool per process).
+struct PoolState {
+    int cap = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf<int> xf, sx, heap, pstate, host_list, status, hsol;
+    DevBuf<double> ub, bound, fracsol, hval;
+    DevBuf<unsigned long long> lb, node_ns, deadline;
+    DevBuf<unsigned char> arena;
+    HostBuf<int> hst;
+    HostBuf<unsigned long long> hlb;
+};
+
+PoolState& pstate_host()
+{
+    static PoolState s;
+    return s;
+}
+
 }  // namespace
+
+// Best-first B&B over the open nodes `open` (priority: their upper_bound)
+// with the node pool on the device (nodek_kernel in pool mode): CTAs pop,
+// bound, branch and push until no node is open.  Nodes the kernel flags go
+// to the host, are bounded by engines, branched there and pushed back, and
+// the kernel runs again.  Returns 0, 1 when the pool is full or a lock wait
+// ran out, 2 on an engine error; *created counts the node records (open
+// nodes included), *evaluated the nodes bounded.
+int fused_pool_bab(const std::vector<BabNode>& open, int cap, double budget_s, long long* created,
+                   long long* evaluated, int* stopped)
+{
+    FusedState& F = fstate();
+    std::lock_guard<std::mutex> lock(F.mu);
+    PoolState& Q = pstate_host();
+    Runtime& R = rt();
+    const int N0 = SP->n, N = N0 - 1;
+    if (!Q.stream) BQB_CUDA(cudaStreamCreateWithFlags(&Q.stream, cudaStreamNonBlocking));
+    cudaStream_t s = Q.stream;
+    if (cap < (int)open.size() + 2) cap = (int)open.size() + 2;
+    Q.cap = cap;
+    const size_t cN = (size_t)cap * N;
+    Q.xf.ensure(cN);
+    Q.sx.ensure(cN);
+    Q.heap.ensure(cap);
+    Q.pstate.ensure(NKQ_WORDS);
+    Q.host_list.ensure(cap);
+    Q.status.ensure(cap);
+    Q.hsol.ensure(cN);
+    Q.ub.ensure(cap);
+    Q.bound.ensure(cap);
+    Q.fracsol.ensure(cN);
+    Q.hval.ensure(cap);
+    Q.lb.ensure(1);
+    Q.node_ns.ensure(cap);
+    Q.deadline.ensure(1);
+    int* hst = Q.hst.ensure(NKQ_WORDS);
+
+    // the open nodes, highest priority first (a sorted array is a heap)
+    std::vector<int> order(open.size());
+    for (size_t i = 0; i < open.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return open[a].upper_bound > open[b].upper_bound; });
+    std::vector<int> hx((size_t)open.size() * N), hs((size_t)open.size() * N), hheap(open.size());
+    std::vector<double> hub(open.size()), hhv(open.size(), -1e300);
+    for (size_t q = 0; q < open.size(); ++q) {
+        memcpy(&hx[q * N], open[q].xfixed, N * sizeof(int));
+        memcpy(&hs[q * N], open[q].sol.X, N * sizeof(int));
+        hub[q] = open[q].upper_bound;
+        hheap[q] = order[q];
+    }
+    const int m = (int)open.size();
+    if (m > 0) {
+        BQB_CUDA(cudaMemcpyAsync(Q.xf.p, hx.data(), hx.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaMemcpyAsync(Q.sx.p, hs.data(), hs.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaMemcpyAsync(Q.ub.p, hub.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaMemcpyAsync(Q.hval.p, hhv.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaMemcpyAsync(Q.heap.p, hheap.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    for (int w = 0; w < NKQ_WORDS; ++w) hst[w] = 0;
+    hst[NKQ_SIZE] = m;
+    hst[NKQ_CREATED] = m;
+    BQB_CUDA(cudaMemcpyAsync(Q.pstate.p, hst, NKQ_WORDS * sizeof(int), cudaMemcpyHostToDevice, s));
+    BQB_CUDA(cudaStreamSynchronize(s));
+    if (budget_s > 0) nk_deadline(Q.deadline.p, (unsigned long long)(budget_s * 1e9), s);
+
+    // P0L on the device (the same copy the fused launches use)
+    const unsigned gen = g_sp_generation.load();
+    if (F.P0L_src != SP->L || F.P0N != N0 || F.P0L_gen != gen) {
+        for (int q = 0; q < NK_LAUNCHES; ++q)
+            if (F.run[q].refs > 0) BQB_CUDA(cudaStreamSynchronize(F.run[q].stream));
+        F.P0L.ensure((size_t)N0 * N0);
+        BQB_CUDA(cudaMemcpy(F.P0L.p, SP->L, (size_t)N0 * N0 * sizeof(double), cudaMemcpyHostToDevice));
+        F.P0L_src = SP->L;
+        F.P0N = N0;
+        F.P0L_gen = gen;
+    }
+    if (!F.prof.p) {
+        F.prof.ensure(2 * NKP_COUNT);
+        BQB_CUDA(cudaMemset(F.prof.p, 0, 2 * NKP_COUNT * sizeof(unsigned long long)));
+    }
+    *evaluated = 0;
+    *stopped = 0;
+    int rc = 0;
+    int made_total = m;
+    while (true) {
+        FusedCfg c;
+        fill_cfg(c, N0, 0, 1, F.seed + 0x632BE59BD9B4E019ull * (unsigned long long)(*evaluated + 1), R.smem_optin);
+        const size_t slot_bytes = nk_layout(c);
+        const int slots = R.num_sms;
+        Q.arena.ensure(slot_bytes * slots);
+        unsigned long long* hlb = Q.hlb.ensure(1);
+        hlb[0] = host_ordered(Bab_LBGet());
+        BQB_CUDA(cudaMemcpyAsync(Q.lb.p, hlb, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+        c.P0L = F.P0L.p;
+        c.xfixed = Q.xf.p;
+        c.solx = Q.sx.p;
+        c.bound = Q.bound.p;
+        c.fracsol = Q.fracsol.p;
+        c.hval = Q.hval.p;
+        c.hsol = Q.hsol.p;
+        c.status = Q.status.p;
+        c.node_ns = Q.node_ns.p;
+        c.lb = Q.lb.p;
+        c.ipm_stats = ipm_stats_device();
+        c.prof = F.prof.p;
+        c.warm_p = warm_device_params();
+        c.warm_stats = c.warm_p ? warm_device_stats() : nullptr;
+        c.pool = 1;
+        c.pool_cap = cap;
+        c.branching = params.branchingStrategy;
+        c.heap = Q.heap.p;
+        c.ub = Q.ub.p;
+        c.pstate = Q.pstate.p;
+        c.host_list = Q.host_list.p;
+        c.deadline = budget_s > 0 ? Q.deadline.p : nullptr;
+        c.arena = Q.arena.p;
+        nk_launch(c, slots, s);
+        BQB_CUDA(cudaMemcpyAsync(hst, Q.pstate.p, NKQ_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+        ++F.st_launches;
+        const int made = hst[NKQ_CREATED] < cap ? hst[NKQ_CREATED] : cap;
+        made_total = made;
+        // heuristic improvements: the best value any node reported
+        std::vector<double> hv(made);
+        BQB_CUDA(cudaMemcpy(hv.data(), Q.hval.p, made * sizeof(double), cudaMemcpyDeviceToHost));
+        int bi = -1;
+        for (int q = 0; q < made; ++q)
+            if (hv[q] > Bab_LBGet() && (bi < 0 || hv[q] > hv[bi])) bi = q;
+        if (bi >= 0) {
+            BabSolution bs;
+            memset(&bs, 0, sizeof bs);
+            BQB_CUDA(cudaMemcpy(bs.X, Q.hsol.p + (size_t)bi * N, N * sizeof(int), cudaMemcpyDeviceToHost));
+            Bab_LBUpd(hv[bi], &bs);
+        }
+        *evaluated += hst[NKQ_EVALUATED];
+        if (hst[NKQ_ERROR]) {
+            set_error("bqb_solve_device", (hst[NKQ_ERROR] & 2) ? "the device node pool is full"
+                                                             : "a lock wait in the node pool ran out");
+            rc = 1;
+            break;
+        }
+        if (hst[NKQ_STOPPED]) {
+            *stopped = 1;
+            break;
+        }
+        // nodes the kernel flagged: engines bound them, the host branches
+        const int h = hst[NKQ_HOST];
+        std::vector<int> hl(h);
+        if (h > 0)
+            BQB_CUDA(cudaMemcpy(hl.data(), Q.host_list.p, h * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<BabNode> hn(h);
+        std::vector<double> hb(h, 0.0);
+        for (int q = 0; q < h; ++q) {
+            memset(&hn[q], 0, sizeof(BabNode));
+            BQB_CUDA(cudaMemcpy(hn[q].xfixed, Q.xf.p + (size_t)hl[q] * N, N * sizeof(int), cudaMemcpyDeviceToHost));
+            BQB_CUDA(cudaMemcpy(hn[q].sol.X, Q.sx.p + (size_t)hl[q] * N, N * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        if (h > 0) {
+            F.fallbacks += h;
+            const int e = bqb_bound_nodes(hn.data(), h, 1, h < 16 ? h : 16, nullptr, hb.data());
+            if (e) {
+                rc = 2;
+                break;
+            }
+        }
+        // their children, then the open nodes left on the device
+        int size = hst[NKQ_SIZE], made2 = made;
+        std::vector<int> heap(size);
+        std::vector<double> ubh(made2);
+        if (size > 0) BQB_CUDA(cudaMemcpy(heap.data(), Q.heap.p, size * sizeof(int), cudaMemcpyDeviceToHost));
+        BQB_CUDA(cudaMemcpy(ubh.data(), Q.ub.p, made2 * sizeof(double), cudaMemcpyDeviceToHost));
+        bool added = false;
+        for (int q = 0; q < h; ++q) {
+            if (!(Bab_LBGet() + 1.0 < hb[q])) continue;
+            hn[q].upper_bound = hb[q];
+            const int ic = getBranchingVariable(&hn[q]);
+            if (ic < 0) continue;
+            for (int xic = 0; xic <= 1; ++xic) {
+                if (made2 >= cap) {
+                    set_error("bqb_solve_device", "the device node pool is full");
+                    rc = 1;
+                    break;
+                }
+                std::vector<int> cx(hn[q].xfixed, hn[q].xfixed + N), cs(hn[q].sol.X, hn[q].sol.X + N);
+                cx[ic] = 1;
+                cs[ic] = xic;
+                const double nb = -1e300;
+                BQB_CUDA(cudaMemcpy(Q.xf.p + (size_t)made2 * N, cx.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+                BQB_CUDA(cudaMemcpy(Q.sx.p + (size_t)made2 * N, cs.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+                BQB_CUDA(cudaMemcpy(Q.ub.p + made2, &hb[q], sizeof(double), cudaMemcpyHostToDevice));
+                BQB_CUDA(cudaMemcpy(Q.hval.p + made2, &nb, sizeof(double), cudaMemcpyHostToDevice));
+                ubh.push_back(hb[q]);
+                // sift up in the host copy of the heap
+                heap.push_back(made2);
+                int i = (int)heap.size() - 1;
+                while (i > 0) {
+                    const int pi = (i - 1) / 2;
+                    if (!(ubh[heap[pi]] < ubh[heap[i]])) break;
+                    std::swap(heap[pi], heap[i]);
+                    i = pi;
+                }
+                ++made2;
+                added = true;
+            }
+            if (rc) break;
+        }
+        made_total = made2;
+        if (rc) break;
+        if (heap.empty()) break;
+        if (added || h > 0) {
+            size = (int)heap.size();
+            BQB_CUDA(cudaMemcpy(Q.heap.p, heap.data(), size * sizeof(int), cudaMemcpyHostToDevice));
+            for (int w = 0; w < NKQ_WORDS; ++w) hst[w] = 0;
+            hst[NKQ_SIZE] = size;
+            hst[NKQ_CREATED] = made2;
+            BQB_CUDA(cudaMemcpy(Q.pstate.p, hst, NKQ_WORDS * sizeof(int), cudaMemcpyHostToDevice));
+        } else {
+            // open nodes left without a flagged node: CTAs that waited too
+            // long for work left; run again
+            hst[NKQ_HOST] = 0;
+            hst[NKQ_EVALUATED] = 0;
+            hst[NKQ_ACTIVE] = 0;
+            BQB_CUDA(cudaMemcpy(Q.pstate.p, hst, NKQ_WORDS * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    *created = made_total;
+    return rc;
+}
 
 // Launch every submission still waiting on the host: process_adj_matrix
 // calls this before it replaces the problem they were made for.

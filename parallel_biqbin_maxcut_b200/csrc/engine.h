@@ -89,5 +89,8 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
 
 // Launch the fused submissions still waiting on the host (capi_fused.cu).
 void fused_launch_pending();
+// Best-first B&B with the open-node pool on the device (capi_fused.cu).
+int fused_pool_bab(const std::vector<BabNode>& open, int cap, double budget_s, long long* created,
+                   long long* evaluated, int* stopped);
 
 }  // namespace bqb

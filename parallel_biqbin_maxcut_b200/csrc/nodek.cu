@@ -1351,6 +1351,209 @@ __device__ double nk_bound(const FusedCfg& c, Nk& k)
     return f + k.fixedvalue;
 }
 
+// Bound node `node` of the launch's arrays in this CTA's slot.
+__device__ double nk_run_node(const FusedCfg& c, Nk& k, int node)
+{
+    const unsigned long long t_node = threadIdx.x == 0 ? nk_now() : 0ull;
+    k.node = node;
+    k.xf = c.xfixed + (size_t)node * k.N;
+    k.sx = c.solx + (size_t)node * k.N;
+    k.status = 0;
+    k.best_h = -NK_BIG;
+    k.hseed = nk_mix(c.seed, 2ull * node + 1ull);
+    k.saseed = nk_mix(c.seed, 2ull * node + 2ull);
+    k.hctr = 0;
+    k.sacalls = 0;
+    if (threadIdx.x == 0) c.hval[node] = -NK_BIG;
+    __syncthreads();
+    nk_subproblem(c, k);
+    double b = 0.0;
+    if (k.n > NK_NMAX)
+        k.status |= NKS_SIZE;
+    else
+        b = nk_bound(c, k);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c.bound[node] = b;
+        c.status[node] = k.status;
+        c.node_ns[node] = nk_now() - t_node;
+    }
+    __syncthreads();
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident node pool (src/heap.c:27-133, src/bab_functions.c:224-336
+// on the device): a max-heap of open nodes keyed on the parent's bound,
+// behind a lock that thread 0 of a CTA takes with a bounded wait.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long NKQ_LOCK_NS = 1000000000ull;    // 1 s
+constexpr unsigned long long NKQ_IDLE_NS = 20000000000ull;   // 20 s without work: the CTA leaves
+
+__device__ bool nkq_lock(const FusedCfg& c)
+{
+    const unsigned long long t0 = nk_now();
+    while (atomicCAS(&c.pstate[NKQ_LOCK], 0, 1) != 0) {
+        if (nk_now() - t0 > NKQ_LOCK_NS) {
+            atomicOr(&c.pstate[NKQ_ERROR], 1);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+    return true;
+}
+
+__device__ void nkq_unlock(const FusedCfg& c)
+{
+    __threadfence();
+    atomicExch(&c.pstate[NKQ_LOCK], 0);
+}
+
+// (lock held) push node q
+__device__ void nkq_push(const FusedCfg& c, int q)
+{
+    volatile int* st = c.pstate;
+    int i = st[NKQ_SIZE];
+    const double v = c.ub[q];
+    while (i > 0) {
+        const int p = (i - 1) >> 1;
+        if (!(((volatile double*)c.ub)[c.heap[p]] < v)) break;
+        c.heap[i] = c.heap[p];
+        i = p;
+    }
+    c.heap[i] = q;
+    st[NKQ_SIZE] = st[NKQ_SIZE] + 1;
+}
+
+// (lock held) pop the open node with the largest parent bound
+__device__ int nkq_pop(const FusedCfg& c)
+{
+    volatile int* st = c.pstate;
+    const volatile double* ub = c.ub;
+    const int size = st[NKQ_SIZE] - 1;
+    const int top = c.heap[0];
+    const int last = c.heap[size];
+    st[NKQ_SIZE] = size;
+    int i = 0;
+    while (true) {
+        int ch = 2 * i + 1;
+        if (ch >= size) break;
+        if (ch + 1 < size && ub[c.heap[ch + 1]] > ub[c.heap[ch]]) ++ch;
+        if (!(ub[c.heap[ch]] > ub[last])) break;
+        c.heap[i] = c.heap[ch];
+        i = ch;
+    }
+    if (size > 0) c.heap[i] = last;
+    return top;
+}
+
+// Thread 0: the next node to bound, -1 when the pool is finished (no open
+// node and no CTA working), the deadline passed, or this CTA waited
+// NKQ_IDLE_NS without work (the others go on).  Open nodes whose parent bound
+// no longer exceeds the incumbent by more than 1 are dropped unbounded.
+__device__ int nkq_next(const FusedCfg& c)
+{
+    const unsigned long long t0 = nk_now();
+    volatile int* st = c.pstate;
+    while (true) {
+        if (st[NKQ_ERROR]) return -1;
+        if (c.deadline && nk_now() > *c.deadline) {
+            atomicExch(&c.pstate[NKQ_STOPPED], 1);
+            return -1;
+        }
+        if (!nkq_lock(c)) return -1;
+        const double lb = ordered_to_dbl(*(volatile unsigned long long*)c.lb);
+        int node = -1;
+        while (st[NKQ_SIZE] > 0) {
+            const int q = nkq_pop(c);
+            if (lb + 1.0 < ((volatile double*)c.ub)[q]) {
+                node = q;
+                break;
+            }
+            st[NKQ_PRUNED] = st[NKQ_PRUNED] + 1;
+        }
+        if (node >= 0) {
+            st[NKQ_ACTIVE] = st[NKQ_ACTIVE] + 1;
+            nkq_unlock(c);
+            return node;
+        }
+        const bool finished = st[NKQ_ACTIVE] == 0;
+        nkq_unlock(c);
+        if (finished || nk_now() - t0 > NKQ_IDLE_NS) return -1;
+        __nanosleep(2000);
+    }
+}
+
+// After bounding `node` (bound b): hand a flagged node to the host, or
+// branch on the variable getBranchingVariable picks (src/bab_functions.c:
+// 387-423) when the bound exceeds the incumbent by more than 1 and push both
+// children with b as their priority; then leave the active count.
+__device__ void nkq_finish(const FusedCfg& c, Nk& k, int node, double b)
+{
+    __shared__ int s_ic, s_base;
+    const int N = k.N;
+    const bool flagged = c.status[node] != 0;
+    const double lb = nk_lb(c);
+    const bool branch = !flagged && lb + 1.0 < b;
+    if (threadIdx.x == 0) {
+        s_ic = -1;
+        s_base = -1;
+        if (flagged) {
+            const int h = atomicAdd(&c.pstate[NKQ_HOST], 1);
+            if (h < c.pool_cap) c.host_list[h] = node;
+            else atomicOr(&c.pstate[NKQ_ERROR], 2);
+        } else if (branch) {
+            const double* fs = c.fracsol + (size_t)node * N;
+            int ic = -1;
+            double best = c.branching == 0 ? -NK_BIG : NK_BIG;
+            for (int i = 0; i < N; ++i) {
+                if (k.xf[i]) continue;
+                const double d = fabs(0.5 - fs[i]);
+                if (c.branching == 0 ? d > best : d < best) {
+                    best = d;
+                    ic = i;
+                }
+            }
+            s_ic = ic;
+            if (ic >= 0) {
+                const int base = atomicAdd(&c.pstate[NKQ_CREATED], 2);
+                if (base + 2 <= c.pool_cap) s_base = base;
+                else atomicOr(&c.pstate[NKQ_ERROR], 2);
+            }
+        }
+    }
+    __syncthreads();
+    const int ic = s_ic, base = s_base;
+    if (base >= 0) {
+        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) {
+            const int ch = i / N, v = i % N;
+            int* xf = (int*)c.xfixed + (size_t)(base + ch) * N;
+            int* sx = (int*)c.solx + (size_t)(base + ch) * N;
+            xf[v] = v == ic ? 1 : k.xf[v];
+            sx[v] = v == ic ? ch : k.sx[v];
+        }
+        if (threadIdx.x < 2) {
+            c.ub[base + threadIdx.x] = b;
+            c.hval[base + threadIdx.x] = -NK_BIG;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&c.pstate[NKQ_EVALUATED], 1);
+        __threadfence();
+        if (nkq_lock(c)) {
+            if (base >= 0) {
+                nkq_push(c, base);
+                nkq_push(c, base + 1);
+            }
+            c.pstate[NKQ_ACTIVE] = ((volatile int*)c.pstate)[NKQ_ACTIVE] - 1;
+            nkq_unlock(c);
+        }
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
 {
     Nk k;
@@ -1360,36 +1563,17 @@ __global__ void __launch_bounds__(NKT, 1) nodek_kernel(FusedCfg c)
     while (true) {
         int node = 0;
         if (threadIdx.x == 0) {
-            const int q = atomicAdd(c.next, 1);
-            node = q < c.count ? c.order[q] : c.count;
+            if (c.pool) {
+                node = nkq_next(c);
+            } else {
+                const int q = atomicAdd(c.next, 1);
+                node = q < c.count ? c.order[q] : -1;
+            }
         }
         node = bcast_i(node);
-        if (node >= c.count) break;
-        const unsigned long long t_node = threadIdx.x == 0 ? nk_now() : 0ull;
-        k.node = node;
-        k.xf = c.xfixed + (size_t)node * k.N;
-        k.sx = c.solx + (size_t)node * k.N;
-        k.status = 0;
-        k.best_h = -NK_BIG;
-        k.hseed = nk_mix(c.seed, 2ull * node + 1ull);
-        k.saseed = nk_mix(c.seed, 2ull * node + 2ull);
-        k.hctr = 0;
-        k.sacalls = 0;
-        if (threadIdx.x == 0) c.hval[node] = -NK_BIG;
-        __syncthreads();
-        nk_subproblem(c, k);
-        double b = 0.0;
-        if (k.n > NK_NMAX)
-            k.status |= NKS_SIZE;
-        else
-            b = nk_bound(c, k);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            c.bound[node] = b;
-            c.status[node] = k.status;
-            c.node_ns[node] = nk_now() - t_node;
-        }
-        __syncthreads();
+        if (node < 0) break;
+        const double b = nk_run_node(c, k, node);
+        if (c.pool) nkq_finish(c, k, node, b);
     }
 }
 
@@ -1474,6 +1658,20 @@ size_t nk_layout(FusedCfg& c)
     }
     c.slot_bytes = off;
     return off;
+}
+
+namespace {
+__global__ void nk_deadline_kernel(unsigned long long* out, unsigned long long budget_ns)
+{
+    *out = nk_now() + budget_ns;
+}
+}  // namespace
+
+void nk_deadline(unsigned long long* out, unsigned long long budget_ns, cudaStream_t s)
+{
+    nk_deadline_kernel<<<1, 1, 0, s>>>(out, budget_ns);
+    BQB_COUNT_LAUNCH();
+    check_launch("nk_deadline_kernel");
 }
 
 void nk_launch(const FusedCfg& cfg, int slots, cudaStream_t s)

@@ -33,6 +33,20 @@ enum NkStatus : int {
     NKS_SIZE = 32,         // subproblem too large for the fused kernel
 };
 
+// Words of the device node pool's state (FusedCfg::pstate).
+enum NkPoolWord : int {
+    NKQ_LOCK,        // heap lock
+    NKQ_SIZE,        // open nodes in the heap
+    NKQ_CREATED,     // node records in use
+    NKQ_ACTIVE,      // CTAs bounding a node
+    NKQ_ERROR,       // bit 1: a lock wait ran out; bit 2: the pool is full
+    NKQ_EVALUATED,   // nodes bounded on the device
+    NKQ_HOST,        // nodes handed back to the host (host_list entries)
+    NKQ_PRUNED,      // open nodes dropped unbounded (parent bound <= incumbent + 1)
+    NKQ_STOPPED,     // the deadline passed
+    NKQ_WORDS
+};
+
 // Phases timed inside the fused kernel (globaltimer, thread 0 of each CTA).
 enum NkPhase : int {
     NKP_SUB, NKP_IPM, NKP_HEUR, NKP_TRISEP, NKP_TRILIST, NKP_KGON, NKP_CUTS, NKP_OPBT, NKP_OPB, NKP_LAMBDA,
@@ -75,6 +89,18 @@ struct FusedCfg {
     // {kept, rejected} proposal counters
     const void* warm_p;
     unsigned long long* warm_stats;
+    // device-resident node pool (pool != 0): the CTAs pop the open node with
+    // the largest parent bound, bound it, branch it on the device and push
+    // its children, until no node is open and no CTA is working.  The node
+    // I/O arrays above are then indexed by pool node (pool_cap records).
+    int pool;
+    int pool_cap;
+    int branching;          // params.branchingStrategy (0 least, 1 most fractional)
+    int* heap;              // pool_cap node indices, a max-heap on ub
+    double* ub;             // pool_cap: the parent's bound of each node
+    int* pstate;            // NKQ_* words
+    int* host_list;         // pool_cap: nodes the kernel hands back to the host
+    const unsigned long long* deadline;   // globaltimer value after which no node is popped (null: none)
     // slot arena
     unsigned char* arena;
     size_t slot_bytes;
@@ -93,5 +119,7 @@ size_t nk_smem_bytes(int N0, int T, int bcap, size_t smem_optin);
 size_t nk_layout(FusedCfg& cfg);
 
 void nk_launch(const FusedCfg& cfg, int slots, cudaStream_t s);
+// *out = the device's globaltimer + budget_ns (the pool's deadline).
+void nk_deadline(unsigned long long* out, unsigned long long budget_ns, cudaStream_t s);
 
 }  // namespace bqb
