@@ -83,6 +83,7 @@ LEG_CALLS = {
     "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply), "
                "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32)",
     "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
+    "device_pool": "bqb_solve_device: the whole tree in one persistent launch, open-node pool on the device",
 }
 
 
@@ -439,7 +440,8 @@ def run_gpu(args):
         sms = arm.lib_sms()
         fused_kw = dict(fused_batch=2 * sms, fused_depth=8)
         cases = [("n100", TTO_NAME, tto_instance(),
-                  [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w)])]
+                  [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w),
+                   ("device_pool", dict(device_pool=True), None)])]
         if args.tto_torus:
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
                           [("engines", dict(threads=16, gw_hyperplanes=4096), None)]))
