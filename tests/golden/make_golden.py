@@ -184,9 +184,14 @@ def main():
         # the last four: the QUBO configuration at n = 100 (Max-Cut on 101
         # vertices) and two held-out instances of the learned warm start's
         # family, G(n, 0.9) with integer weights in [-10, 10]
+        # and the 7 x 7 x 7 torus (n = 343, couplings N(0,1) x 1e5; about 5
+        # minutes of the reference's serial B&B)
         for kind, nv, seed in (("unit", 40, 1), ("unit", 60, 2), ("pm1", 40, 3), ("qubo", 30, 4),
-                               ("qubo", 100, 1), ("qubo", 100, 2), ("int10", 60, 911), ("int10", 80, 913)):
-            if kind == "unit":
+                               ("qubo", 100, 1), ("qubo", 100, 2), ("int10", 60, 911), ("int10", 80, 913),
+                               ("torus", 343, 1)):
+            if kind == "torus":
+                A = instances.torus3d(7, seed)
+            elif kind == "unit":
                 A = instances.gnp_unit(nv, 0.5, seed)
             elif kind == "pm1":
                 A = instances.gnp_pm1(nv, 0.5, seed)

