@@ -508,16 +508,40 @@ namespace {
 
 std::mutex g_pool_mu;
 std::vector<bqb::Engine*> g_pool;
+std::vector<char> g_pool_busy;
 
-// At least k private engines, sized for problems up to N x N.  Engine i
-// draws random numbers from the stream srand(2021 + i) would give.
-std::vector<bqb::Engine*>& engine_pool(int k, int N)
-{
-    std::lock_guard<std::mutex> lock(g_pool_mu);
-    while ((int)g_pool.size() < k) g_pool.push_back(bqb::engine_create(2021u + (unsigned)g_pool.size()));
-    for (int i = 0; i < k; ++i) g_pool[i]->ensure_private(N);
-    return g_pool;
-}
+// k private engines leased to the caller alone (concurrent callers get
+// different engines; an engine and its buffers are never shared by two
+// bounding threads), sized for problems up to N x N.  The first free
+// engines are taken in creation order, so a single caller always gets
+// engines 0..k-1; engine i draws random numbers from the stream srand(2021 + i)
+// would give.  The lease ends when the returned object goes away.
+struct EngineLease {
+    std::vector<bqb::Engine*> e;
+    EngineLease(int k, int N)
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        for (size_t i = 0; i < g_pool.size() && (int)e.size() < k; ++i)
+            if (!g_pool_busy[i]) {
+                g_pool_busy[i] = 1;
+                e.push_back(g_pool[i]);
+            }
+        while ((int)e.size() < k) {
+            g_pool.push_back(bqb::engine_create(2021u + (unsigned)g_pool.size()));
+            g_pool_busy.push_back(1);
+            e.push_back(g_pool.back());
+        }
+        for (bqb::Engine* x : e) x->ensure_private(N);
+    }
+    ~EngineLease()
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        for (bqb::Engine* x : e)
+            for (size_t i = 0; i < g_pool.size(); ++i)
+                if (g_pool[i] == x) g_pool_busy[i] = 0;
+    }
+    bqb::Engine* operator[](int t) const { return e[t]; }
+};
 
 }  // namespace
 
@@ -534,7 +558,7 @@ BQB_API int bqb_bound_nodes(BabNode* nodes, int count, int rank, int threads, co
     bqb::rt();
     if (threads < 1) threads = 1;
     if (threads > count) threads = count;
-    std::vector<bqb::Engine*>& pool = engine_pool(threads, SP->n);
+    const EngineLease pool(threads, SP->n);
     std::atomic<int> next{0};
     const int dev = bqb::rt().device;
     auto work = [&](int t) {
@@ -613,7 +637,7 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
         branch(root);
     free(root);
 
-    std::vector<bqb::Engine*>& pool = engine_pool(threads, SP->n);
+    const EngineLease pool(threads, SP->n);
     const int dev = bqb::rt().device;
     auto work = [&](int t) {
         bqb::t_pool_worker = t > 0;
