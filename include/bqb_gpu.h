@@ -438,7 +438,7 @@ int bqb_ipm_batch(const double *const *Ls, double *const *Xs, const int *ns, int
  * scale (mean |L_ij|); FP32 training (Adam) with this library's kernels,
  * BF16-weight inference.  Parameters: BQB_WARM_NPARAM floats, layout
  * W1[12][32], b1[32], W2[32][32], b2[32], w3[32], b3. */
-#define BQB_WARM_NPARAM 1505
+#define BQB_WARM_NPARAM 1569
 /* out[3] = {features per cut, hidden units, parameters}. */
 void bqb_warm_dims(int *out);
 /* Train from params (in/out) on N rows: feats[N x 12], targets[N]; Adam,
@@ -465,10 +465,12 @@ void bqb_warm_dataset_clear(void);
 void bqb_warm_stats(long long *out, int reset);
 /* The features of m triangle cuts (cuts: m x {type, i, j, k}, values: their
  * violations) at X and the objective L (host, n x n column-major) into
- * out[m x 12]; for checking against the oracle.  Returns 0, or -1 on bad
+ * out[m x 14]; parent_gamma (may be NULL): the multiplier each cut ended
+ * with in the parent node's final cut list, -1 for a cut the parent did not
+ * hold.  For checking against the oracle.  Returns 0, or -1 on bad
  * arguments (an index outside 0..n-1, a type outside 1..4). */
 int bqb_warm_features(const double *X, const double *L, int n, const int *cuts, const double *values, int m,
-                      double viol3, double gap, float *out);
+                      double viol3, double gap, const double *parent_gamma, float *out);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,7 @@ The network has no counterpart in the reference; it is this project's
 learned warm start of the bundle multipliers.  Layout and arithmetic follow
 the GPU kernels (parallel_biqbin_maxcut_b200/csrc/warm.h, warm.cu):
 
-    features x (F = 12) -> h1 = relu(x W1 + b1) (H = 32)
+    features x (F = 14) -> h1 = relu(x W1 + b1) (H = 32)
                         -> h2 = relu(h1 W2 + b2) (H)
                         -> z = h2 . w3 + b3,  gamma = softplus(z)
     loss = mean over the rows of (gamma - y)^2
@@ -18,7 +18,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F, H = 12, 32
+F, H = 14, 32
 OFF_W1 = 0
 OFF_B1 = OFF_W1 + F * H
 OFF_W2 = OFF_B1 + H
@@ -90,13 +90,14 @@ def bf16(a):
     return r.astype(np.uint32).view(np.float32)
 
 
-def features(X, L, cuts, values, viol3, gap):
+def features(X, L, cuts, values, viol3, gap, parent_gamma=None):
     """The per-cut features the GPU computes (csrc/warm_body.cuh), float64:
     the violation v, v / viol3, viol3, the signed X entries of the cut's
     inequality s_ij X_ij + s_ik X_ik + s_jk X_jk <= 1 (sorted), the signed
     objective entries s L / scale (sorted; scale = mean |L_ij|, i != j),
-    n / 128, log(1 + m) / 10 and log(1 + gap / scale).  cuts: m x 4
-    (type, i, j, k)."""
+    n / 128, log(1 + m) / 10, log(1 + gap / scale), and the parent's final
+    multiplier of the same cut / scale with a flag 1 (parent_gamma[c] >= 0),
+    or 0, 0 (parent_gamma None or < 0).  cuts: m x 4 (type, i, j, k)."""
     X = np.asarray(X, dtype=np.float64)
     L = np.asarray(L, dtype=np.float64)
     n = X.shape[0]
@@ -110,6 +111,7 @@ def features(X, L, cuts, values, viol3, gap):
         xs = sorted([s[0] * X[i, j], s[1] * X[i, k], s[2] * X[j, k]])
         ls = sorted([s[0] * L[i, j] / sc, s[1] * L[i, k] / sc, s[2] * L[j, k] / sc])
         v = values[c]
+        pg = -1.0 if parent_gamma is None else float(parent_gamma[c])
         out[c] = [v, v / viol3 if viol3 > 1e-12 else 0.0, viol3, *xs, *ls, n / 128.0, np.log1p(m) / 10.0,
-                  np.log1p(max(gap, 0.0) / sc)]
+                  np.log1p(max(gap, 0.0) / sc), pg / sc if pg >= 0 else 0.0, 1.0 if pg >= 0 else 0.0]
     return out

@@ -136,7 +136,8 @@ SIGNATURES = {
     "bqb_warm_dataset": (C.c_longlong, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_longlong]),
     "bqb_warm_dataset_clear": (None, []),
     "bqb_warm_stats": (None, [C.POINTER(C.c_longlong), C.c_int]),
-    "bqb_warm_features": (C.c_int, [D, D, C.c_int, I, D, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_float)]),
+    "bqb_warm_features": (C.c_int, [D, D, C.c_int, I, D, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                    C.POINTER(C.c_float)]),
     "bqb_warm_dims": (None, [C.POINTER(C.c_int)]),
     "bqb_set_heuristic_hook": (None, [C.c_void_p]),
     "bqb_heuristic_runs": (C.c_longlong, [C.c_int]),

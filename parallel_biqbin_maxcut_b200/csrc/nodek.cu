@@ -1175,7 +1175,7 @@ __device__ __noinline__ double nk_warm(const FusedCfg& c, Nk& k, double viol3, d
                          : type == 3 ? xij - xik + xjk - 1.0
                                      : xij + xik - xjk - 1.0;
         float xf[WARM_F];
-        warm_cut_features(type, i, j, kk, v, k.X, k.L, n, m, viol3, gap, sc, xf);
+        warm_cut_features(type, i, j, kk, v, k.X, k.L, n, m, viol3, gap, sc, -1.0, xf);
         const double g = sc * (double)warm_mlp_bf16(xf, P);
         k.gtest[q] = g;
         sg += g;

@@ -49,12 +49,14 @@ __global__ void warm_scale_kernel(const double* __restrict__ L, int n, double* _
 // Features of each cut (warm_cut_features), one thread per cut.
 __global__ void warm_feat_kernel(const int4* __restrict__ cut, const double* __restrict__ val, int m,
                                  const double* __restrict__ X, const double* __restrict__ L, int n, double viol3,
-                                 double gap, const double* __restrict__ scale, float* __restrict__ F)
+                                 double gap, const double* __restrict__ scale, const double* __restrict__ pgam,
+                                 float* __restrict__ F)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m) return;
     const int4 q = cut[c];
-    warm_cut_features(q.x, q.y, q.z, q.w, val[c], X, L, n, m, viol3, gap, *scale, F + (size_t)c * WARM_F);
+    warm_cut_features(q.x, q.y, q.z, q.w, val[c], X, L, n, m, viol3, gap, *scale, pgam ? pgam[c] : -1.0,
+                      F + (size_t)c * WARM_F);
 }
 
 // Inference with BF16 weights, FP32 arithmetic; one thread per cut.  The
@@ -250,7 +252,7 @@ bool warm_active() { return wg().enabled.load() && wg().loaded; }
 bool warm_recording() { return wg().recording.load(); }
 
 void warm_features(WarmDev& w, const Triangle_Inequality* cuts, int m, const double* dX, const double* dL, int n,
-                   double viol3, double gap, cudaStream_t s)
+                   double viol3, double gap, cudaStream_t s, const double* parent_gam)
 {
     if (m <= 0) return;
     int4* hc = w.hcut.ensure(m);
@@ -264,10 +266,16 @@ void warm_features(WarmDev& w, const Triangle_Inequality* cuts, int m, const dou
     float* df = w.feat.ensure((size_t)m * WARM_F);
     BQB_CUDA(cudaMemcpyAsync(dc, hc, (size_t)m * sizeof(int4), cudaMemcpyHostToDevice, s));
     BQB_CUDA(cudaMemcpyAsync(dv, hv, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
+    double* dpg = nullptr;
+    if (parent_gam) {
+        dpg = w.pgam.ensure(m);
+        BQB_CUDA(cudaMemcpyAsync(dpg, parent_gam, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
+        BQB_CUDA(cudaStreamSynchronize(s));   // the caller's host array may go away
+    }
     double* dsc = w.scale.ensure(1);
     warm_scale_kernel<<<1, WT, 0, s>>>(dL, n, dsc);
     BQB_COUNT_LAUNCH();
-    warm_feat_kernel<<<blocks(m), WT, 0, s>>>(dc, dv, m, dX, dL, n, viol3, gap, dsc, df);
+    warm_feat_kernel<<<blocks(m), WT, 0, s>>>(dc, dv, m, dX, dL, n, viol3, gap, dsc, dpg, df);
     BQB_COUNT_LAUNCH();
     check_launch("warm_feat_kernel");
 }
@@ -494,9 +502,11 @@ BQB_API void bqb_warm_dims(int* out)
 
 // The warm start's features of m triangle cuts (cuts: m x {type, i, j, k};
 // values: their violations) at X and the objective L (n x n, column-major,
-// host); out: m x 12 floats.  For tests against the oracle.
+// host); parent_gamma (m entries, may be NULL): the parent's final
+// multiplier of each cut, -1 for one the parent did not hold; out: m x
+// WARM_F floats.  For tests against the oracle.
 BQB_API int bqb_warm_features(const double* Xh, const double* Lh, int n, const int* cuts, const double* values,
-                              int m, double viol3, double gap, float* out)
+                              int m, double viol3, double gap, const double* parent_gamma, float* out)
 {
     if (!Xh || !Lh || !cuts || !values || !out || n <= 0 || m <= 0) return -1;
     static WarmDev w;
@@ -519,7 +529,7 @@ BQB_API int bqb_warm_features(const double* Xh, const double* Lh, int n, const i
             t[c].k >= n)
             return -1;
     }
-    warm_features(w, t.data(), m, dX.p, dL.p, n, viol3, gap, s);
+    warm_features(w, t.data(), m, dX.p, dL.p, n, viol3, gap, s, parent_gamma);
     std::vector<float> f;
     warm_fetch_features(w, m, f, s);
     memcpy(out, f.data(), f.size() * sizeof(float));

@@ -26,7 +26,7 @@
 
 namespace bqb {
 
-constexpr int WARM_F = 12;   // features per cut
+constexpr int WARM_F = 14;   // features per cut
 constexpr int WARM_H = 32;   // hidden units per layer
 // parameter layout (float): W1[F][H], b1[H], W2[H][H], b2[H], w3[H], b3
 constexpr int WARM_OFF_W1 = 0;
@@ -46,6 +46,7 @@ struct WarmDev {
     DevBuf<double> gam;     // proposed multipliers
     DevBuf<double> X;       // the IPM solution at the proposal
     DevBuf<double> scale;   // the node's objective scale (mean |L_ij|, i != j)
+    DevBuf<double> pgam;    // per cut: the parent's final multiplier (-1: not in the parent's list)
     HostBuf<double> hscale;
     HostBuf<int4> hcut;
     HostBuf<double> hval;
@@ -61,9 +62,11 @@ bool warm_recording();
 // Features of the m triangle cuts at the device matrices dX and dL (the
 // node's objective), n x n, on stream s into w.feat (and the objective's
 // scale into w.scale).  viol3: the separation's largest violation; gap:
-// the node's bound minus the incumbent.
+// the node's bound minus the incumbent; parent_gam (host, m entries, may be
+// null): the multiplier each cut ended with in the parent node's final cut
+// list, -1 for a cut the parent did not hold.
 void warm_features(WarmDev& w, const Triangle_Inequality* cuts, int m, const double* dX, const double* dL, int n,
-                   double viol3, double gap, cudaStream_t s);
+                   double viol3, double gap, cudaStream_t s, const double* parent_gam = nullptr);
 // The proposal for the m cuts whose features are in w.feat, into w.gam.
 void warm_infer(WarmDev& w, int m, cudaStream_t s);
 // The features of the last warm_features call (m cuts), copied to the

@@ -15,11 +15,14 @@ __device__ __forceinline__ float warm_softplus(float z) { return z > 20.f ? z : 
 // s_ij X_ij + s_ik X_ik + s_jk X_jk <= 1 with the type's signs
 // (src/cutting_planes.c:20-39): its violation v, v relative to the largest
 // violation viol3, viol3, the three signed X entries (sorted), the signed
-// objective entries s L / scale (sorted), n / 128, log(1 + m) / 10 and
-// log(1 + gap / scale).
+// objective entries s L / scale (sorted), n / 128, log(1 + m) / 10,
+// log(1 + gap / scale), and from the parent node: the multiplier the same
+// cut ended with in the parent's final list / scale and 1 (pg >= 0), or 0
+// and 0 when the parent did not hold the cut (pg < 0; also every cut of a
+// node bounded without its parent's list).
 __device__ inline void warm_cut_features(int type, int i, int j, int k, double v, const double* X,
                                          const double* L, int n, int m, double viol3, double gap, double sc,
-                                         float* f)
+                                         double pg, float* f)
 {
     const double sij = (type == 3 || type == 4) ? 1.0 : -1.0;
     const double sik = (type == 2 || type == 4) ? 1.0 : -1.0;
@@ -47,6 +50,8 @@ __device__ inline void warm_cut_features(int type, int i, int j, int k, double v
     f[9] = (float)(n / 128.0);
     f[10] = (float)(log1p((double)m) / 10.0);
     f[11] = (float)log1p(fmax(gap, 0.0) / sc);
+    f[12] = pg >= 0.0 ? (float)(pg / sc) : 0.f;
+    f[13] = pg >= 0.0 ? 1.f : 0.f;
 }
 
 // The network on one feature row, BF16 weights, FP32 arithmetic; returns

@@ -232,10 +232,16 @@ def test_gpu_features_match_oracle(lib):
     out = np.zeros((len(cuts), W.F), np.float32)
     ci = np.ascontiguousarray(np.array(cuts, dtype=np.int32).ravel())
     assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(ci),
-                                 _lib.dptr(values), len(cuts), 0.9, 12.5, _lib.fptr(out)) == 0
+                                 _lib.dptr(values), len(cuts), 0.9, 12.5, None, _lib.fptr(out)) == 0
     ref = W.features(Xm, L, cuts, values, 0.9, 12.5)
     np.testing.assert_allclose(out, ref, rtol=1e-6, atol=1e-6)
+    # with the parent's multipliers: half the cuts were in the parent's list
+    pg = np.where(np.arange(len(cuts)) % 2 == 0, rng.uniform(0, 3, len(cuts)), -1.0)
+    assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(ci),
+                                 _lib.dptr(values), len(cuts), 0.9, 12.5, pg.ctypes.data,
+                                 _lib.fptr(out)) == 0
+    np.testing.assert_allclose(out, W.features(Xm, L, cuts, values, 0.9, 12.5, pg), rtol=1e-6, atol=1e-6)
     bad = ci.copy()
     bad[1] = n   # index out of range: rejected before any device work
     assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(bad),
-                                 _lib.dptr(values), len(cuts), 0.9, 12.5, _lib.fptr(out)) == -1
+                                 _lib.dptr(values), len(cuts), 0.9, 12.5, None, _lib.fptr(out)) == -1
