@@ -23,6 +23,7 @@
 #include <atomic>
 #include <condition_variable>
 #include <mutex>
+#include <unordered_map>
 #include <thread>
 #include <vector>
 
@@ -623,7 +624,10 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
     std::condition_variable cv;
     int active = 0;
     bool stop = false;
-    auto branch = [&](BabNode* node) {
+    // with the learned warm start or the recorder on, each child bounds with
+    // its parent's final cuts (bqb::Engine::parent)
+    std::unordered_map<BabNode*, std::shared_ptr<bqb::ParentCuts>> parent_of;
+    auto branch = [&](BabNode* node, const std::shared_ptr<bqb::ParentCuts>& cuts = nullptr) {
         const int ic = getBranchingVariable(node);
         for (int xic = 0; xic <= 1; ++xic) {
             BabNode* child = new_node(node);
@@ -631,10 +635,11 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
             child->sol.X[ic] = xic;
             ++g_num_nodes;
             heap.push(child);
+            if (cuts) parent_of[child] = cuts;
         }
     };
     if (Bab_LBGet() + 1.0 < root->upper_bound && !params.root)
-        branch(root);
+        branch(root, std::move(bqb::default_engine().final_cuts));
     free(root);
 
     const EngineLease pool(threads, SP->n);
@@ -659,12 +664,21 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
             }
             BabNode* node = heap.pop();
             ++active;
+            std::shared_ptr<bqb::ParentCuts> pc;
+            auto it = parent_of.find(node);
+            if (it != parent_of.end()) {
+                pc = std::move(it->second);
+                parent_of.erase(it);
+            }
             lk.unlock();
             P.L = E.PPL.data();
             createSubproblem(node, SP, &P);
+            E.parent = pc.get();
             node->upper_bound = bqb::sdp_bound(E, node, SP, &P, 1);
+            E.parent = nullptr;
+            std::shared_ptr<bqb::ParentCuts> mine = std::move(E.final_cuts);
             lk.lock();
-            if (Bab_LBGet() + 1.0 < node->upper_bound) branch(node);
+            if (Bab_LBGet() + 1.0 < node->upper_bound) branch(node, mine);
             free(node);
             --active;
             cv.notify_all();
@@ -675,6 +689,7 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
     work(0);
     for (auto& x : th) x.join();
     while (!heap.empty()) free(heap.pop());
+    parent_of.clear();
 
     if (out) {
         out->best_value = Bab_LBGet();

@@ -63,6 +63,11 @@ struct Engine {
     uint64_t sa_calls = 0;   // ... and the separation calls made so far
     DevBuf<double> ipm_ws;
     WarmDev warm;            // learned warm start of the bundle multipliers
+    // set by a B&B driver before sdp_bound: the parent node's final cuts
+    // (null: none); sdp_bound leaves the node's own final cuts in
+    // final_cuts when the warm start or the recorder is on
+    const ParentCuts* parent = nullptr;
+    std::shared_ptr<ParentCuts> final_cuts;
     // private host state (extra engines only)
     std::vector<Triangle_Inequality> cuts_v;
     std::vector<Pentagonal_Inequality> pcuts_v, plist_v;

@@ -13,6 +13,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <unordered_map>
 #include <vector>
 
 #include "internal.h"
@@ -104,6 +105,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     NodeDev& nd = E.nd;
     HostState H = E.host();
     const int n = PP_->n;
+    E.final_cuts.reset();
     const int N0 = SP_->n;
     const int NB = N0 - 1;   // BabPbSize
     const size_t nn = (size_t)n * n;
@@ -200,39 +202,128 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     // IPM) and start the bundle there when their dual value is below the
     // plain start's (gamma = 0, where the dual value is the basic bound f).
     // Any gamma >= 0 gives a valid bound; the bundle then runs to its own
-    // stopping rules.  Recording keeps the first-separation cuts' features
-    // and, at the end, the multipliers they finish with (training pairs).
+    // stopping rules.  With the parent's final cuts (a B&B driver sets
+    // E.parent), every cut gets the parent's multiplier as a feature, and
+    // the parent's cuts that the child's separation did not find are
+    // candidates: those whose predicted multiplier reaches
+    // WARM_SHORTLIST_MIN join the first cut list (the shortlist); when the
+    // proposal is rejected the list goes back to the child's own cuts.
+    // Recording keeps the first cut list's features and, at the end, the
+    // multipliers those cuts finish with (training pairs); while recording
+    // without a model every parent candidate joins the list, so the pairs
+    // say which of them the bundle keeps.
+    const bool warm_on = warm_active();
     const bool warm_rec = warm_recording();
     std::vector<float> warm_feats;
     std::vector<Triangle_Inequality> warm_first;
     double warm_scale = 1.0;
-    if (warm_rec || warm_active()) {
-        warm_features(E.warm, H.cuts, PP_->NIneq, dX, dL, n, viol3, bound - Bab_LBGet(), s);
-        if (warm_rec) {
-            warm_scale = warm_fetch_features(E.warm, PP_->NIneq, warm_feats, s);
-            warm_first.assign(H.cuts, H.cuts + PP_->NIneq);
-        }
+    std::vector<int> orig;   // subproblem vertex -> original vertex
+    const int n_own = PP_->NIneq;
+    if (warm_on || warm_rec) {
+        orig.resize(n);
+        int idx = 0;
+        for (int i = 0; i < NB && idx < n - 1; ++i)
+            if (!node->xfixed[i]) orig[idx++] = i;
+        orig[n - 1] = NB;
     }
-    if (warm_active()) {
-        const int mw = PP_->NIneq;
-        warm_infer(E.warm, mw, s);
+    std::vector<double> pg;
+    if ((warm_on || warm_rec) && E.parent) {
+        const ParentCuts& PC = *E.parent;
+        pg.assign(n_own, -1.0);
+        std::unordered_map<uint64_t, int> have;
+        have.reserve((size_t)n_own * 2 + 16);
+        for (int c = 0; c < n_own; ++c) {
+            const Triangle_Inequality& t = H.cuts[c];
+            const uint64_t key = orig_cut_key(t.type, orig[t.i], orig[t.j], orig[t.k]);
+            have[key] = c;
+            auto it = PC.index.find(key);
+            if (it != PC.index.end()) pg[c] = it->second;
+        }
+        std::vector<int> cidx(NB + 1, -1);
+        for (int q = 0; q < n; ++q) cidx[orig[q]] = q;
+        int m = n_own;
+        for (size_t c = 0; c < PC.key.size() && m < BQB_MAX_TRI_INEQ; ++c) {
+            if (!(PC.gam[c] > 0.0) || have.count(PC.key[c])) continue;
+            const int type = (int)(PC.key[c] >> 48);
+            const int a = cidx[(PC.key[c] >> 32) & 0xFFFF], bb = cidx[(PC.key[c] >> 16) & 0xFFFF],
+                      cc = cidx[PC.key[c] & 0xFFFF];
+            if (a < 0 || bb < 0 || cc < 0) continue;   // a vertex the child fixed
+            Triangle_Inequality& t = H.cuts[m++];
+            t.type = type;
+            t.i = a;
+            t.j = bb;
+            t.k = cc;
+            t.value = NAN;   // evaluated at X by the feature kernel
+            t.y = 0.0;
+            pg.push_back(PC.gam[c]);
+        }
+        PP_->NIneq = m;
+    }
+    std::vector<float> feats_all;   // (recording) the features of every candidate of the first list
+    std::vector<int> rows;          // (recording) first list -> row of feats_all
+    if (warm_on || warm_rec) {
+        warm_features(E.warm, H.cuts, PP_->NIneq, dX, dL, n, viol3, bound - Bab_LBGet(), s,
+                      pg.empty() ? nullptr : pg.data());
+        if (warm_rec) warm_scale = warm_fetch_features(E.warm, PP_->NIneq, feats_all, s);
+        for (int c = 0; c < PP_->NIneq; ++c) rows.push_back(c);
+    }
+    for (int c = n_own; c < PP_->NIneq; ++c) H.cuts[c].value = 0.0;
+    if (warm_on) {
+        const int mall = PP_->NIneq;
+        warm_infer(E.warm, mall, s);
+        double* hg = E.warm.hgam.ensure(mall);
+        BQB_CUDA(cudaMemcpyAsync(hg, E.warm.gam.p, (size_t)mall * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaMemcpyAsync(E.warm.hscale.ensure(1), E.warm.scale.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+        const double sc = E.warm.hscale.p[0];
+        // the shortlist: candidates whose predicted multiplier is large enough
+        std::vector<double> prop(hg, hg + n_own);
+        rows.resize(n_own);
+        int m = n_own;
+        for (int c = n_own; c < mall; ++c)
+            if (hg[c] >= WARM_SHORTLIST_MIN * sc) {
+                H.cuts[m] = H.cuts[c];
+                prop.push_back(hg[c]);
+                rows.push_back(c);
+                ++m;
+            }
+        PP_->NIneq = m;
+        upload_cuts(E, H, PP_);
+        BQB_CUDA(cudaMemcpyAsync(E.warm.gam.p, prop.data(), (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
         opBt_launch(nd.cuts, nd.L0.p, n, E.warm.gam.p, s);
         double* Xw = E.warm.X.ensure(nn);
         ipm_device(E.ipm_ws, nd.L0.p, Xw, n, dout, s);
-        double* hg = E.warm.hgam.ensure(mw);
-        BQB_CUDA(cudaMemcpyAsync(hg, E.warm.gam.p, (size_t)mw * sizeof(double), cudaMemcpyDeviceToHost, s));
         BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
         BQB_CUDA(cudaStreamSynchronize(s));
         double fw = nd.hs.p[0];
-        for (int i = 0; i < mw; ++i) fw += hg[i];
+        for (int i = 0; i < m; ++i) fw += prop[i];
         const bool keep = (int)nd.hs.p[2] == IPM_OK && fw < f;
         warm_count(keep);
         if (keep) {
-            for (int i = 0; i < mw; ++i) H.dual_gamma[i] = hg[i];
+            for (int i = 0; i < m; ++i) H.dual_gamma[i] = prop[i];
             BQB_CUDA(cudaMemcpyAsync(dX, Xw, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
             f = fw;
+        } else if (m != n_own) {
+            PP_->NIneq = n_own;   // back to the child's own cuts
+            rows.resize(n_own);
+            upload_cuts(E, H, PP_);
         }
+        if (!keep)
+            for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = 0.0;
+    } else {
+        if (PP_->NIneq != n_own) {
+            for (int i = n_own; i < PP_->NIneq; ++i) H.dual_gamma[i] = 0.0;
+            upload_cuts(E, H, PP_);
+        }
+    }
+    if (warm_rec) {
+        // the features of the first list as it stands (own cuts, then the
+        // shortlisted or, without a model, all parent candidates)
+        warm_feats.resize(rows.size() * WARM_F);
+        for (size_t r = 0; r < rows.size(); ++r)
+            memcpy(&warm_feats[r * WARM_F], &feats_all[(size_t)rows[r] * WARM_F], WARM_F * sizeof(float));
+        warm_first.assign(H.cuts, H.cuts + PP_->NIneq);
     }
     BundleDev& b = nd.b;
     b.ensure_cap(1 + bdl_iter + 2, n, s);
@@ -342,15 +433,28 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         bdl_iter += count % 2;
         bdl_iter = (bdl_iter < params.max_bundle_iter) ? bdl_iter : params.max_bundle_iter;
     }
-    if (warm_rec && !warm_first.empty()) {
+    if (warm_on || warm_rec) {
         std::vector<double> fg(PP_->NIneq > 0 ? PP_->NIneq : 1);
         if (PP_->NIneq > 0) {
             BQB_CUDA(cudaMemcpyAsync(fg.data(), b.gam.p, (size_t)PP_->NIneq * sizeof(double), cudaMemcpyDeviceToHost,
                                      s));
             BQB_CUDA(cudaStreamSynchronize(s));
         }
-        warm_record(warm_feats, warm_scale, warm_first.data(), (int)warm_first.size(), H.cuts, fg.data(),
-                    PP_->NIneq);
+        if (warm_rec && !warm_first.empty())
+            warm_record(warm_feats, warm_scale, warm_first.data(), (int)warm_first.size(), H.cuts, fg.data(),
+                        PP_->NIneq);
+        // the node's final triangle cuts, for its children
+        auto fc = std::make_shared<ParentCuts>();
+        fc->key.reserve(PP_->NIneq);
+        fc->gam.reserve(PP_->NIneq);
+        for (int c = 0; c < PP_->NIneq; ++c) {
+            const Triangle_Inequality& t = H.cuts[c];
+            const uint64_t key = orig_cut_key(t.type, orig[t.i], orig[t.j], orig[t.k]);
+            fc->key.push_back(key);
+            fc->gam.push_back(fg[c]);
+            fc->index[key] = fg[c];
+        }
+        E.final_cuts = std::move(fc);
     }
     bound = f + fixedvalue;
     if (rank == 0) diff = basic_bound - bound;

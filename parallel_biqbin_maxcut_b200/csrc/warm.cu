@@ -55,7 +55,15 @@ __global__ void warm_feat_kernel(const int4* __restrict__ cut, const double* __r
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m) return;
     const int4 q = cut[c];
-    warm_cut_features(q.x, q.y, q.z, q.w, val[c], X, L, n, m, viol3, gap, *scale, pgam ? pgam[c] : -1.0,
+    double v = val[c];
+    if (isnan(v)) {   // a cut the separation did not evaluate: its violation at X (src/cutting_planes.c:20-39)
+        const double xij = X[q.y + (size_t)q.z * n], xik = X[q.y + (size_t)q.w * n], xjk = X[q.z + (size_t)q.w * n];
+        v = q.x == 1 ? -xij - xik - xjk - 1.0
+            : q.x == 2 ? -xij + xik + xjk - 1.0
+            : q.x == 3 ? xij - xik + xjk - 1.0
+                       : xij + xik - xjk - 1.0;
+    }
+    warm_cut_features(q.x, q.y, q.z, q.w, v, X, L, n, m, viol3, gap, *scale, pgam ? pgam[c] : -1.0,
                       F + (size_t)c * WARM_F);
 }
 

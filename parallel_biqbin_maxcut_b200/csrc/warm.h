@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <vector_types.h>
 
+#include <memory>
+#include <unordered_map>
 #include <vector>
 
 #include "bqb_common.cuh"
@@ -53,6 +55,24 @@ struct WarmDev {
     HostBuf<float> hfeat;
     HostBuf<double> hgam;
 };
+
+// A node's final triangle cuts in the original problem's vertex numbering
+// (the subproblem's free vertices in order, then the last vertex), with
+// the multipliers they end with: what a child node inherits.  A triangle
+// keeps its orientation (i > j > k) and its type under this numbering, so
+// the same key names the same inequality in parent and child.
+struct ParentCuts {
+    std::vector<uint64_t> key;
+    std::vector<double> gam;
+    std::unordered_map<uint64_t, double> index;
+};
+inline uint64_t orig_cut_key(int type, int a, int b, int c)
+{
+    return ((uint64_t)type << 48) | ((uint64_t)a << 32) | ((uint64_t)b << 16) | (uint64_t)c;
+}
+// Parent cuts whose predicted multiplier (in units of the objective's scale)
+// reaches this value join the child's first cut list (the shortlist).
+constexpr double WARM_SHORTLIST_MIN = 0.01;
 
 // A model is loaded and warm starts are switched on.
 bool warm_active();
