@@ -237,6 +237,11 @@ void bqb_set_heuristic_hook(bqb_heuristic_fn fn);
  * since the last reset (reset != 0 resets after reading; the fused kernel's
  * calls are not counted). */
 long long bqb_heuristic_runs(int reset);
+/* Bundle iterations (one fct_eval each, src/bundle.c:9-239) run by SDPbound
+ * on the default engine and on engines since the last reset (reset != 0
+ * resets after reading; the fused kernel's are not counted).  No reference
+ * counterpart. */
+long long bqb_bundle_iterations(int reset);
 
 /* Tensor-core product D = A B^T (tcgen05.mma kind::tf32, FP32 accumulation
  * in tensor memory, operands staged by TMA): the kernel behind the batched

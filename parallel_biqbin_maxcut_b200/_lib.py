@@ -141,6 +141,7 @@ SIGNATURES = {
     "bqb_warm_dims": (None, [C.POINTER(C.c_int)]),
     "bqb_set_heuristic_hook": (None, [C.c_void_p]),
     "bqb_heuristic_runs": (C.c_longlong, [C.c_int]),
+    "bqb_bundle_iterations": (C.c_longlong, [C.c_int]),
     "bqb_kgon_sa": (C.c_int, [D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, D, I]),
     "bqb_init": (C.c_int, [C.c_int]),
     "bqb_last_error": (C.c_char_p, []),

@@ -32,6 +32,7 @@ namespace bqb {
 
 std::atomic<bqb_heuristic_fn> g_heuristic_hook{nullptr};
 std::atomic<long long> g_heuristic_runs{0};
+std::atomic<long long> g_bundle_iters{0};
 
 void upload_cuts(Engine& E, const HostState& H, const Problem* P)
 {
@@ -83,6 +84,7 @@ double bundle_iterations(Engine& E, int bdl_iter, double* t)
     BQB_CUDA(cudaMemcpyAsync(b.istate.p + BI_CAP, nd.hi.p + BI_CAP, sizeof(int), cudaMemcpyHostToDevice, s));
     nd.hs.p[0] = *t;
     BQB_CUDA(cudaMemcpyAsync(b.dstate.p + BD_T, nd.hs.p, sizeof(double), cudaMemcpyHostToDevice, s));
+    g_bundle_iters.fetch_add(bdl_iter);
     for (int it = 0; it < bdl_iter; ++it) {
         lambda_eta_launch(b, nullptr, s);
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, nd.L.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -473,6 +475,13 @@ BQB_API void bqb_set_heuristic_hook(bqb_heuristic_fn fn) { g_heuristic_hook.stor
 BQB_API long long bqb_heuristic_runs(int reset)
 {
     return reset ? g_heuristic_runs.exchange(0) : g_heuristic_runs.load();
+}
+
+// Bundle iterations (src/bundle.c:9-239, one fct_eval each) run by SDPbound
+// on the default engine and on engines since the last reset.
+BQB_API long long bqb_bundle_iterations(int reset)
+{
+    return reset ? g_bundle_iters.exchange(0) : g_bundle_iters.load();
 }
 
 // SDPbound (src/bounding.c:24-342) in the default engine: the reference's

@@ -134,6 +134,58 @@ def record_pairs(lib, sizes_seeds, nodes_per_instance=48, kmax=30, threads=16, n
     return feats, targets
 
 
+def record_pairs_bab(lib, sizes_seeds, threads=16, time_limit=60):
+    """Training pairs from B&B trees solved by the plain method (no model),
+    so that every child node sees its parent's final cuts: its features
+    carry the parent's multipliers, and the parent's cuts its own
+    separation did not find join its first list (targets then say which of
+    them the bundle keeps).  Each instance runs to optimality or
+    `time_limit` seconds.  Returns (features, targets)."""
+    lib.bqb_warm_enable(0)
+    lib.bqb_warm_dataset_clear()
+    lib.bqb_warm_record(1)
+    try:
+        for n, seed in sizes_seeds:
+            _lib.solve(c5_instance(n, seed), threads=threads, time_limit=time_limit)
+    finally:
+        lib.bqb_warm_record(0)
+    F = dims(lib)[0]
+    count = lib.bqb_warm_dataset(None, None, 0)
+    feats = np.zeros((count, F), np.float32)
+    targets = np.zeros(count, np.float32)
+    lib.bqb_warm_dataset(_lib.fptr(feats), _lib.fptr(targets), count)
+    return feats, targets
+
+
+def evaluate_bab(lib, A, params, threads=16, time_limit=300):
+    """The same B&B plain and warm-started (parent-informed proposals and
+    shortlist), in the order plain, warm: seconds, nodes, bundle iterations
+    per node, IPM calls per node, proposals kept / rejected, the optimum (or
+    the incumbent at the time limit) and whether it stopped early."""
+    out = {}
+    for name, p in (("plain", None), ("warm", params)):
+        use_model(lib, p)
+        st = (C.c_longlong * 2)()
+        lib.bqb_warm_stats(st, 1)
+        lib.bqb_bundle_iterations(1)
+        lib.bqb_stats_reset()
+        lib.bqb_stats_enable(1)
+        t0 = time.perf_counter()
+        r = _lib.solve(A, threads=threads, time_limit=time_limit)
+        sec = time.perf_counter() - t0
+        ipm = (C.c_double * 6)()
+        lib.bqb_ipm_stats(ipm)
+        lib.bqb_stats_enable(0)
+        bi = lib.bqb_bundle_iterations(1)
+        lib.bqb_warm_stats(st, 1)
+        out[name] = {"seconds": sec, "nodes": r["nodes"], "optimum": r["best_value"], "stopped": r["stopped"],
+                     "root_bound": r["root_bound"], "bundle_iterations_per_node": bi / max(r["nodes"], 1),
+                     "ipm_calls_per_node": float(ipm[1]) / max(r["nodes"], 1),
+                     "proposals_kept": int(st[0]), "proposals_rejected": int(st[1])}
+    use_model(lib, None)
+    return out
+
+
 def init_params(seed=0, lib=None):
     """He-normal weights, zero biases (the output bias starts at -2, so the
     first proposals are small multipliers)."""
@@ -232,22 +284,45 @@ MODEL_C5 = os.path.join(os.path.dirname(__file__), "warm_model_c5.json")
 TRAIN_C5 = [(80, 1), (80, 2), (100, 3), (100, 4), (120, 5), (120, 6), (150, 7), (150, 8)]
 
 
+# held-out instances of the same family (seeds disjoint from TRAIN_C5's)
+EVAL_C5 = [(150, 901), (150, 902), (100, 903), (100, 904)]
+
+
 def main(argv):
     """python -m parallel_biqbin_maxcut_b200.warm train <out.json>: record
-    pairs on the training instances and train (the shipped model's recipe;
-    recording order across engines is not deterministic, so a new model is
-    close to, not identical with, the shipped one)."""
-    if len(argv) != 2 or argv[0] != "train":
+    pairs from B&B trees of the training instances (each child with its
+    parent's final cuts) and train (the shipped model's recipe; recording
+    order across engines is not deterministic, so a new model is close to,
+    not identical with, the shipped one).
+    python -m parallel_biqbin_maxcut_b200.warm evaluate <model.json> <out.json>:
+    plain against warm-started B&B on the held-out instances."""
+    if len(argv) < 2 or argv[0] not in ("train", "evaluate"):
         print(main.__doc__)
         return 2
     lib = _lib.load()
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
-    feats, targets = record_pairs(lib, TRAIN_C5, nodes_per_instance=48, kmax=30, threads=16)
+    if argv[0] == "evaluate":
+        p, _ = load_model(argv[1])
+        res = {f"G({n},0.9) seed {sd}": evaluate_bab(lib, c5_instance(n, sd), p) for n, sd in EVAL_C5}
+        with open(argv[2], "w") as fh:
+            json.dump(res, fh, indent=1)
+        print(json.dumps(res, indent=1))
+        return 0
+    feats, targets = record_pairs_bab(lib, TRAIN_C5, threads=16, time_limit=60)
     p, losses = train(lib, feats, targets, steps=6000, batch=4096, lr=1e-3, seed=0)
-    save_model(argv[1], p, {"train_instances": TRAIN_C5, "pairs": int(len(targets)),
+    save_model(argv[1], p, {"family": "G(n, 0.9), integer weights uniform in [-10, 10] (warm.c5_instance)",
+                            "train_instances": TRAIN_C5,
+                            "nodes": "every node of plain B&B trees (16 engines, 60 s per instance), each child "
+                                     "with its parent's final cuts (record_pairs_bab)",
+                            "pairs": int(len(targets)), "parent_pairs": int((feats[:, 13] > 0).sum()),
+                            "training": "bqb_warm_train, Adam lr 1e-3, 6000 steps, batch 4096, seed 0, "
+                                        "standardized features folded into layer 1",
                             "final_minibatch_mse": float(losses[-200:].mean()),
-                            "target_variance": float(targets.var())})
-    print(f"{len(targets)} pairs, final minibatch MSE {losses[-200:].mean():.5f} (target variance {targets.var():.5f})")
+                            "target_variance": float(targets.var()),
+                            "command": "python -m parallel_biqbin_maxcut_b200.warm train "
+                                       "parallel_biqbin_maxcut_b200/warm_model_c5.json"})
+    print(f"{len(targets)} pairs ({int((feats[:, 13] > 0).sum())} with a parent multiplier), final minibatch "
+          f"MSE {losses[-200:].mean():.5f} (target variance {targets.var():.5f})")
     return 0
 
 
