@@ -339,8 +339,10 @@ def run_gpu(args):
         return outs
 
     stream = torch.cuda.current_stream()
-    # warm-up (sizes every pipe's arena and buffers)
-    pipelined([arm.node_array(batches[s]) for s in range(args.warmup)], args.depth)
+    # warm-up: at least twice the window, so that every launch record's
+    # arena and buffers are sized before the timed region
+    nwarm = max(args.warmup, 2 * args.depth)
+    pipelined([arm.node_array(batches[s % len(batches)]) for s in range(nwarm)], args.depth)
 
     # ---- value: the fused kernel (+ any node it hands back to an engine),
     # device time from CUDA events around the launch on its stream ----

@@ -616,9 +616,17 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
 
     TIME = wtime();
     NodeHeap heap;
+    const EngineLease pool(threads, SP->n);
     BabNode* root = new_node(nullptr);
     ++g_num_nodes;
-    root_bound = Evaluate(root, SP, PP, 0);
+    {
+        // the root on engine 0 (rank 0 sets diff): its heuristic and k-gonal
+        // separation run on the device as every other node's do
+        bqb::Engine& E0 = *pool[0];
+        E0.PP.L = E0.PPL.data();
+        createSubproblem(root, SP, &E0.PP);
+        root_bound = bqb::sdp_bound(E0, root, SP, &E0.PP, 0);
+    }
     root->upper_bound = root_bound;
     std::mutex mu;
     std::condition_variable cv;
@@ -639,10 +647,9 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
         }
     };
     if (Bab_LBGet() + 1.0 < root->upper_bound && !params.root)
-        branch(root, std::move(bqb::default_engine().final_cuts));
+        branch(root, std::move(pool[0]->final_cuts));
     free(root);
 
-    const EngineLease pool(threads, SP->n);
     const int dev = bqb::rt().device;
     auto work = [&](int t) {
         bqb::t_pool_worker = t > 0;
