@@ -445,6 +445,9 @@ def run_gpu(args):
                   [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w),
                    ("device_pool", dict(device_pool=True), None)])]
         if args.tto_torus:
+            # the multi-CTA IPM's per-size schedule for the torus's sizes
+            # (n = 343 and its subproblems, the same panel count)
+            tto_sched = _lib.autotune_ipm([343], reps=2)
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
                           [("engines", dict(threads=16, gw_hyperplanes=4096), None)]))
         tto = {}
@@ -466,6 +469,8 @@ def run_gpu(args):
                 best = min(e[leg]["seconds"] for leg, _, _ in legs)
                 e["speedup_batched_vs_plain"] = e["plain_dropin"]["seconds"] / best
                 assert all(e[leg]["optimum"] == e["plain_dropin"]["optimum"] for leg, _, _ in legs), e
+            if key == "torus343":
+                e["ipm_schedule"] = tto_sched
             tto[key] = e
         # restore the bench's problem (the solver set up its own)
         arm.reset_problem()

@@ -408,6 +408,15 @@ void bqb_ipm_plan_destroy(bqb_ipm_plan *plan);
 int bqb_ipm_batch_device(const double *const *Ls, double *const *Xs, const int *ns, int nprob,
                          double *out, void *stream);
 
+/* Per-size schedule of the multi-CTA IPM (n > 128, one cooperative launch
+ * per call): bqb_ipm_schedule_set uses `grid` CTAs for every n with the
+ * same number of 32-column panels (grid <= 0: back to one CTA per 32 x 32
+ * tile).  bqb_ipm_autotune times `reps` calls for each candidate grid on a
+ * seeded problem of size n and keeps the fastest (best_grid / best_ms may
+ * be NULL); returns 0, 1 for n <= 128.  No reference counterpart. */
+void bqb_ipm_schedule_set(int n, int grid);
+int bqb_ipm_autotune(int n, int reps, int *best_grid, double *best_ms);
+
 /* Basic SDP bound of one problem without any device allocation.  No
  * counterpart in the reference: it exists for callers that may not call
  * cudaMalloc while they run (e.g. inside a host application whose memory

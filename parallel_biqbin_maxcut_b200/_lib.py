@@ -125,6 +125,8 @@ SIGNATURES = {
     "bqb_fused_node_times": (C.c_int, [D, C.c_int]),
     "bqb_reset_incumbent": (None, [C.c_double]),
     "bqb_set_gw_hyperplanes": (None, [C.c_int]),
+    "bqb_ipm_schedule_set": (None, [C.c_int, C.c_int]),
+    "bqb_ipm_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "bqb_warm_train": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_uint, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "bqb_warm_grad": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
@@ -299,3 +301,32 @@ class GlobalArrays:
 
 def set_params(cdll, p: Params) -> None:
     Params.in_dll(cdll, "params").__init__(*[getattr(p, f) for f, _ in Params._fields_])
+
+
+def autotune_ipm(sizes, path=None, reps=2) -> dict:
+    """Tune the multi-CTA IPM's grid for each size in `sizes` (n > 128) on
+    the GPU (bqb_ipm_autotune) and, with `path`, write the schedule as JSON
+    ({"n": {"grid": g, "ms": t}}) for load_ipm_schedule."""
+    import json
+    lib = load()
+    table = {}
+    for n in sizes:
+        g = C.c_int()
+        ms = C.c_double()
+        if lib.bqb_ipm_autotune(int(n), int(reps), C.byref(g), C.byref(ms)) == 0:
+            table[str(int(n))] = {"grid": int(g.value), "ms": float(ms.value)}
+    if path:
+        with open(path, "w") as fh:
+            json.dump(table, fh, indent=1)
+    return table
+
+
+def load_ipm_schedule(path) -> dict:
+    """Apply a schedule written by autotune_ipm."""
+    import json
+    lib = load()
+    with open(path) as fh:
+        table = json.load(fh)
+    for n, e in table.items():
+        lib.bqb_ipm_schedule_set(int(n), int(e["grid"]))
+    return table

@@ -38,6 +38,10 @@
 // IPM_SYNC (a fatal error on the host).
 #include <math.h>
 
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "bqb_common.cuh"
 #include "internal.h"
 #include "ipm.cuh"
@@ -715,8 +719,15 @@ struct CoopConfig {
     size_t smem = 0;
 };
 
-// Grid size for n: one CTA per 32 x 32 tile of the sweep, at most as many
-// as can be co-resident (one per SM at this register count).
+// The per-size schedule: the grid (CTAs) to use for T = ceil(n / 32) tiles
+// per dimension, filled by the autotuner (bqb_ipm_autotune) or set by hand
+// (bqb_ipm_schedule_set); sizes without an entry use one CTA per tile.
+std::mutex g_sched_mu;
+std::map<int, int> g_sched;
+
+// Grid size for n: the schedule's entry for its tile count, else one CTA
+// per 32 x 32 tile of the sweep; at most as many as can be co-resident (one
+// per SM at this register count).
 CoopConfig coop_config(int n)
 {
     static int max_blocks = -1;
@@ -732,6 +743,11 @@ CoopConfig coop_config(int n)
     }
     const int T = (n + CB - 1) / CB;
     int g = T * T;
+    {
+        std::lock_guard<std::mutex> lock(g_sched_mu);
+        auto it = g_sched.find(T);
+        if (it != g_sched.end()) g = it->second;
+    }
     if (g > max_blocks) g = max_blocks;
     if (g < 1) g = 1;
     c.grid = g;
@@ -788,3 +804,91 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
 }
 
 }  // namespace bqb
+
+using namespace bqb;
+
+// Use `grid` CTAs for the multi-CTA IPM of every n with the same tile count
+// as n (grid <= 0 removes the entry).  No reference counterpart.
+BQB_API void bqb_ipm_schedule_set(int n, int grid)
+{
+    if (n <= 0) return;
+    const int T = (n + CB - 1) / CB;
+    std::lock_guard<std::mutex> lock(g_sched_mu);
+    if (grid > 0) g_sched[T] = grid;
+    else g_sched.erase(T);
+}
+
+// Autotune the multi-CTA IPM's grid for size n (> 128): time `reps` calls
+// for each candidate (one CTA per tile, half, a quarter, an eighth, and the
+// SM count) on a seeded problem of that size (the Laplacian of a random
+// +-1 graph, as the B&B's subproblems are), keep the fastest in the
+// schedule.  best_grid / best_ms (may be null) receive the choice and its
+// time per call.  Returns 0, 1 for n <= 128.  No reference counterpart.
+BQB_API int bqb_ipm_autotune(int n, int reps, int* best_grid, double* best_ms)
+{
+    if (n <= 128) return 1;
+    if (reps < 1) reps = 1;
+    Runtime& R = rt();
+    cudaStream_t s = R.stream;
+    const size_t nn = (size_t)n * n;
+    std::vector<double> L(nn, 0.0);
+    unsigned long long z = 0x5eedull + (unsigned long long)n;
+    auto next = [&]() {
+        z += 0x9E3779B97F4A7C15ull;
+        unsigned long long x = z;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    };
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < i; ++j) {
+            const unsigned long long r = next();
+            if (r & 1) continue;                       // edge with probability 1/2
+            const double w = (r & 2) ? 1.0 : -1.0;     // weight +-1
+            L[i + (size_t)j * n] = L[j + (size_t)i * n] = -w;
+            L[i + (size_t)i * n] += w;
+            L[j + (size_t)j * n] += w;
+        }
+    for (double& v : L) v *= 0.25;
+    DevBuf<double> dL, dX, ws, out;
+    BQB_CUDA(cudaMemcpy(dL.ensure(nn), L.data(), nn * sizeof(double), cudaMemcpyHostToDevice));
+    dX.ensure(nn);
+    out.ensure(4);
+    const int T = (n + CB - 1) / CB;
+    std::vector<int> cand = {T * T, (T * T + 1) / 2, (T * T + 3) / 4, (T * T + 7) / 8, R.num_sms};
+    int keep = -1;
+    {
+        std::lock_guard<std::mutex> lock(g_sched_mu);
+        auto it = g_sched.find(T);
+        if (it != g_sched.end()) keep = it->second;
+    }
+    cudaEvent_t e0, e1;
+    BQB_CUDA(cudaEventCreate(&e0));
+    BQB_CUDA(cudaEventCreate(&e1));
+    int bg = T * T;
+    double bms = 1e300;
+    for (int g : cand) {
+        if (g < 1) continue;
+        bqb_ipm_schedule_set(n, g);
+        ipm_large(ws, dL.p, dX.p, n, out.p, s, nullptr);   // warm-up
+        BQB_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < reps; ++r) ipm_large(ws, dL.p, dX.p, n, out.p, s, nullptr);
+        BQB_CUDA(cudaEventRecord(e1, s));
+        BQB_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        BQB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        double h[4];
+        BQB_CUDA(cudaMemcpy(h, out.p, sizeof h, cudaMemcpyDeviceToHost));
+        if ((int)h[2] == IPM_OK && ms / reps < bms) {
+            bms = ms / reps;
+            bg = g;
+        }
+    }
+    BQB_CUDA(cudaEventDestroy(e0));
+    BQB_CUDA(cudaEventDestroy(e1));
+    (void)keep;
+    bqb_ipm_schedule_set(n, bg);   // the fastest candidate stays in the schedule
+    if (best_grid) *best_grid = bg;
+    if (best_ms) *best_ms = bms;
+    return 0;
+}
