@@ -79,6 +79,7 @@ struct Smem {
     double A2[CB][LDS];   // C_J, or a GEMM operand tile
     double V1[CB][LDS];   // V_I, or a GEMM operand tile
     double V2[CB][LDS];   // V_J, or a GEMM operand tile
+    double R[CB];         // reciprocals of the factor's diagonal
     double red[CW * 4];
     double tot[4];
     int ok;
@@ -194,6 +195,23 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
     }
 }
 
+// Step I of the inverse of the lower factor for the calling lane's column t:
+// li[I] = (delta_It - sum_{k < I} D[I][k] li[k]) / D[I][I] (zero above the
+// diagonal, where every term is zero).  Instantiated for every I so that li[]
+// stays in registers; the D entries are shared-memory broadcasts that do not
+// depend on the chain.
+template <int I>
+__device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int t)
+{
+    if constexpr (I < CB) {
+        double acc = I == t ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < I; ++k) acc = fma(-sm.D[I][k], li[k], acc);
+        li[I] = acc * sm.R[I];
+        linv_step<I + 1>(li, sm, t);
+    }
+}
+
 // Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
 // in shared memory.  Warp 0 factors in registers (lane p holds row p; the
 // block is padded to 32 x 32 with the identity), then lane t forms column t
@@ -218,16 +236,16 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm)
         if (pd) {
 #pragma unroll
             for (int r = 0; r < CB; ++r) sm.D[p][r] = r <= p ? s[r] : 0.0;
+#pragma unroll
+            for (int r = 0; r < CB; ++r)
+                if (r == p) sm.R[p] = 1.0 / s[r];
         }
         __syncwarp();
         if (pd) {
-            const int t = p;
-            for (int i = 0; i < t; ++i) sm.Li[i][t] = 0.0;
-            for (int i = t; i < CB; ++i) {
-                double acc = i == t ? 1.0 : 0.0;
-                for (int k = t; k < i; ++k) acc = fma(-sm.D[i][k], sm.Li[k][t], acc);
-                sm.Li[i][t] = acc / sm.D[i][i];
-            }
+            double li[CB];
+            linv_step<0>(li, sm, p);
+#pragma unroll
+            for (int i = 0; i < CB; ++i) sm.Li[i][p] = li[i];
         }
     }
     __syncthreads();
