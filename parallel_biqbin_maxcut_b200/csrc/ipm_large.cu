@@ -64,7 +64,7 @@ struct CoopArgs {
     const int* xslot;
     double* out;         // phi, iterations, status, <L,X>
     double* stats;       // IPM work counters (may be null)
-    double *Zi, *F, *M, *T, *dX, *dX1;   // n x n each
+    double *Zi, *F, *M, *T, *T2, *dX, *dX1;   // n x n each (T, T2: the line searches' trial matrices)
     double *Wb, *Db;                     // 2 x (n x CB), 2 x (CB x CB)
     double *y, *zd, *dy, *dy1, *dy2, *r, *t;
     double* part;        // gridDim.x x 4 partial sums
@@ -616,21 +616,23 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         if (!(alive = grid_sync(a.bar, sm))) break;
         for (size_t c = gtid; c < (size_t)n; c += gstride) a.dy[c] = a.dy1[c] + a.dy2[c];
 
-        // primal line search: X + ap dX positive definite
+        // primal line search: X + ap dX positive definite.  Consecutive
+        // trials (primal, then dual) alternate between T and T2: a CTA may
+        // still read the last panel block of one trial while the others fill
+        // the next, so no barrier is needed after a trial's sweep.
+        int tr = 0;
         double ap = 1.0;
         int trials = 0;
         bool ok = false;
         while (true) {
-            for (size_t e = gtid; e < nn; e += gstride) a.T[e] = fma(ap, a.dX[e], X[e]);
+            double* Tt = (tr++ & 1) ? a.T2 : a.T;
+            for (size_t e = gtid; e < nn; e += gstride) Tt[e] = fma(ap, a.dX[e], X[e]);
             if (!(alive = grid_sync(a.bar, sm))) break;
-            pd = sweep<false>(a.T, a, sm);
+            pd = sweep<false>(Tt, a, sm);
             if (pd < 0) {
                 alive = false;
                 break;
             }
-            // every CTA leaves the trailing sweep after reading the panel
-            // block; the next trial rewrites T, so wait for all of them
-            if (!(alive = grid_sync(a.bar, sm))) break;
             if (pd) {
                 ok = true;
                 break;
@@ -650,17 +652,17 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         trials = 0;
         ok = false;
         while (true) {
+            double* Tt = (tr++ & 1) ? a.T2 : a.T;
             for (size_t e = gtid; e < nn; e += gstride) {
                 const int i = (int)(e % n), j = (int)(e / n);
-                a.T[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
+                Tt[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
             }
             if (!(alive = grid_sync(a.bar, sm))) break;
-            pd = sweep<false>(a.T, a, sm);
+            pd = sweep<false>(Tt, a, sm);
             if (pd < 0) {
                 alive = false;
                 break;
             }
-            if (!(alive = grid_sync(a.bar, sm))) break;
             if (pd) {
                 ok = true;
                 break;
@@ -777,7 +779,7 @@ CoopConfig coop_config(int n)
 size_t ipm_large_ws_doubles(int n)
 {
     const size_t nn = (size_t)n * n;
-    return 6 * nn + 2 * (size_t)n * CB + 2 * (size_t)CB * CB + 8 * (size_t)n + 4 * 1024 + 16;
+    return 7 * nn + 2 * (size_t)n * CB + 2 * (size_t)CB * CB + 8 * (size_t)n + 4 * 1024 + 16;
 }
 
 // ipm_mc_pk for n > IPM_REG_NMAX: one cooperative launch on stream s, no
@@ -800,7 +802,8 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
     a.F = a.Zi + nn;
     a.M = a.F + nn;
     a.T = a.M + nn;
-    a.dX = a.T + nn;
+    a.T2 = a.T + nn;
+    a.dX = a.T2 + nn;
     a.dX1 = a.dX + nn;
     a.Wb = a.dX1 + nn;
     a.Db = a.Wb + 2 * (size_t)n * CB;
