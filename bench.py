@@ -794,9 +794,27 @@ def run_case(args):
     `--case ipm-torus`: the same for the side^3-vertex 3D torus (`--n` is
     the side; 7 gives n = 343); `--case fused`: `--count` subproblems
     (k ~ U[0, --kmax] fixed) of a seeded G(n, 0.5) +-1 instance bounded by
-    one fused-kernel launch, after the root on the engine path."""
+    one fused-kernel launch, after the root on the engine path;
+    `--case torus-root`: the 7x7x7 torus's root node on one engine."""
     lib = _lib.load()
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
+    if args.case == "torus-root":
+        # the torus's root node on one engine (rank 0), batched GW rounding
+        A = np.ascontiguousarray(instances.torus3d(7, 1))
+        nv = A.shape[0]
+        _lib.set_params(lib, _lib.make_params())
+        lib.process_adj_matrix(_lib.dptr(A.copy()), nv)
+        lib.bqb_set_gw_hyperplanes(args.hyperplanes)
+        for _ in range(args.repeats):
+            nodes = (_lib.BabNode * 1)()
+            b = np.zeros(1)
+            lib.bqb_reset_incumbent(0.0)
+            t0 = time.perf_counter()
+            assert lib.bqb_bound_nodes(nodes, 1, 0, 1, None, _lib.dptr(b)) == 0, lib.bqb_last_error()
+            print(f"torus root bound={b[0]:.3f} incumbent={lib.Bab_LBGet():.0f} "
+                  f"wall={time.perf_counter() - t0:.3f} s bundle_iterations={lib.bqb_bundle_iterations(1)}",
+                  flush=True)
+        return
     if args.case in ("ipm", "ipm-torus"):
         A = instances.torus3d(args.n, 1) if args.case == "ipm-torus" else instances.gnp_pm1(args.n, 0.5, seed=1)
         nv = A.shape[0]
@@ -862,12 +880,13 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-nodes-per-step", type=int, default=256,
                     help="subproblems per step of the reference arm (bounded CPU sample)")
-    ap.add_argument("--case", choices=["ipm", "ipm-torus", "fused"], default=None,
+    ap.add_argument("--case", choices=["ipm", "ipm-torus", "fused", "torus-root"], default=None,
                     help="run one small profiling case instead of the benchmark")
     ap.add_argument("--n", type=int, default=100, help="--case: vertices (ipm-torus: the side)")
     ap.add_argument("--repeats", type=int, default=3, help="--case ipm/ipm-torus: calls")
     ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
     ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
+    ap.add_argument("--hyperplanes", type=int, default=4096, help="--case torus-root: GW hyperplanes per round")
     args = ap.parse_args()
     faulthandler.enable(all_threads=True)
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
