@@ -285,7 +285,7 @@ TRAIN_C5 = [(80, 1), (80, 2), (100, 3), (100, 4), (120, 5), (120, 6), (150, 7), 
 
 
 # held-out instances of the same family (seeds disjoint from TRAIN_C5's)
-EVAL_C5 = [(150, 901), (150, 902), (100, 903), (100, 904)]
+EVAL_C5 = [(100, 903), (100, 904), (150, 901)]
 
 
 def main(argv):
@@ -294,8 +294,9 @@ def main(argv):
     parent's final cuts) and train (the shipped model's recipe; recording
     order across engines is not deterministic, so a new model is close to,
     not identical with, the shipped one).
-    python -m parallel_biqbin_maxcut_b200.warm evaluate <model.json> <out.json>:
-    plain against warm-started B&B on the held-out instances."""
+    python -m parallel_biqbin_maxcut_b200.warm evaluate <model.json> <out.json> [seconds]:
+    plain against warm-started B&B on the held-out instances (each run to
+    optimality or the time limit, 120 s by default)."""
     if len(argv) < 2 or argv[0] not in ("train", "evaluate"):
         print(main.__doc__)
         return 2
@@ -303,7 +304,9 @@ def main(argv):
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
     if argv[0] == "evaluate":
         p, _ = load_model(argv[1])
-        res = {f"G({n},0.9) seed {sd}": evaluate_bab(lib, c5_instance(n, sd), p) for n, sd in EVAL_C5}
+        limit = int(argv[3]) if len(argv) > 3 else 120
+        res = {f"G({n},0.9) seed {sd}": evaluate_bab(lib, c5_instance(n, sd), p, time_limit=limit)
+               for n, sd in EVAL_C5}
         with open(argv[2], "w") as fh:
             json.dump(res, fh, indent=1)
         print(json.dumps(res, indent=1))
