@@ -122,4 +122,8 @@ def test_parallel_solve_optimum(lib, kind, nv, seed):
     par = _lib.solve(A, threads=8)
     assert par["best_value"] == serial["best_value"]
     assert O.evaluateSolution(O.build_SP_L(A), par["x"]) == par["best_value"]
-    assert par["root_bound"] == serial["root_bound"]
+    # the parallel solver bounds its root on an engine, whose heuristic and
+    # k-gonal separation draw from their own streams: the root bound is the
+    # serial one's only up to those streams, and above the optimum
+    assert par["root_bound"] >= par["best_value"]
+    assert abs(par["root_bound"] - serial["root_bound"]) <= 1e-3 * abs(serial["root_bound"])
