@@ -804,16 +804,27 @@ def run_case(args):
         nv = A.shape[0]
         _lib.set_params(lib, _lib.make_params())
         lib.process_adj_matrix(_lib.dptr(A.copy()), nv)
-        lib.bqb_set_gw_hyperplanes(args.hyperplanes)
+        lib.bqb_set_gw_hyperplanes(max(args.hyperplanes, 0))
+        glob = _lib.GlobalArrays(lib, nv)
+        sol = (C.c_int * _lib.NMAX)()
+        C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(sol)
+        SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
+        PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
         for _ in range(args.repeats):
             nodes = (_lib.BabNode * 1)()
             b = np.zeros(1)
             lib.bqb_reset_incumbent(0.0)
+            lib.bqb_bundle_iterations(1)
             t0 = time.perf_counter()
-            assert lib.bqb_bound_nodes(nodes, 1, 0, 1, None, _lib.dptr(b)) == 0, lib.bqb_last_error()
+            if args.hyperplanes < 0:   # the drop-in: Evaluate on the library's default engine
+                C.CDLL("libc.so.6").srand(2020)
+                b[0] = lib.Evaluate(C.byref(nodes[0]), SP, PP, 0)
+            else:
+                assert lib.bqb_bound_nodes(nodes, 1, 0, 1, None, _lib.dptr(b)) == 0, lib.bqb_last_error()
             print(f"torus root bound={b[0]:.3f} incumbent={lib.Bab_LBGet():.0f} "
                   f"wall={time.perf_counter() - t0:.3f} s bundle_iterations={lib.bqb_bundle_iterations(1)}",
                   flush=True)
+        del glob
         return
     if args.case in ("ipm", "ipm-torus"):
         A = instances.torus3d(args.n, 1) if args.case == "ipm-torus" else instances.gnp_pm1(args.n, 0.5, seed=1)
@@ -886,7 +897,9 @@ def main():
     ap.add_argument("--repeats", type=int, default=3, help="--case ipm/ipm-torus: calls")
     ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
     ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
-    ap.add_argument("--hyperplanes", type=int, default=4096, help="--case torus-root: GW hyperplanes per round")
+    ap.add_argument("--hyperplanes", type=int, default=4096,
+                    help="--case torus-root: GW hyperplanes per round on an engine (0: the reference's count; "
+                         "-1: the drop-in Evaluate instead of an engine)")
     args = ap.parse_args()
     faulthandler.enable(all_threads=True)
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")

@@ -183,8 +183,9 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
             pd = 0;
             d = 1.0;
         }
-        const double l = sqrt(d);
-        const double lpq = p == Q ? l : s[Q] / l;
+        const double rs = rsqrt(d);   // one reciprocal square root per pivot
+        const double l = d * rs;
+        const double lpq = p == Q ? l : s[Q] * rs;
         s[Q] = lpq;
 #pragma unroll
         for (int r = Q + 1; r < CB; ++r) {
@@ -337,11 +338,14 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
 }
 
 // The panel sweep of A (n x n).  FULL: A becomes inv(A); otherwise only the
-// trailing updates run, for the pivots.  Returns 1 (positive definite), 0
-// (a non-positive pivot; every CTA returns 0 at the same panel) or -1 (a
+// trailing updates run, for the pivots.  With Xm (FULL only), the final
+// phase also writes Mout = Fout = inv(A) .* Xm for its tiles (the next
+// inverse's input), saving a phase.  Returns 1 (positive definite), 0 (a
+// non-positive pivot; every CTA returns 0 at the same panel) or -1 (a
 // barrier gave up).
 template <bool FULL>
-__device__ int sweep(double* A, const CoopArgs& a, Smem& sm)
+__device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = nullptr, double* Mout = nullptr,
+                     double* Fout = nullptr)
 {
     const int n = a.n;
     const int T = (n + CB - 1) / CB;
@@ -376,7 +380,13 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm)
                 else if (fixJ) v = Wl[i + (size_t)(j - kp0) * n];
                 else if (fixI) v = Wl[j + (size_t)(i - kp0) * n];
                 else v = A[i + (size_t)j * n];
-                A[i + (size_t)j * n] = -v;
+                const size_t ij = i + (size_t)j * n;
+                A[ij] = -v;
+                if (Xm) {
+                    const double m = -v * Xm[ij];
+                    Mout[ij] = m;
+                    Fout[ij] = m;
+                }
             }
         }
         if (!grid_sync(a.bar, sm)) return -1;
@@ -578,7 +588,8 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             a.Zi[e] = i == j ? a.zd[i] : -L[e];
         }
         if (!(alive = grid_sync(a.bar, sm))) break;
-        int pd = sweep<true>(a.Zi, a, sm);
+        // (its last phase also writes M = Zi .* X and F = M)
+        int pd = sweep<true>(a.Zi, a, sm, X, a.M, a.F);
         if (pd < 0) {
             alive = false;
             break;
@@ -587,13 +598,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             status = IPM_Z_NOT_PD;
             break;
         }
-        // M = Zi .* X, F = inv(M); dy1 = F (-e)
-        for (size_t e = gtid; e < nn; e += gstride) {
-            const double m = a.Zi[e] * X[e];
-            a.M[e] = m;
-            a.F[e] = m;
-        }
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        // F = inv(M); dy1 = F (-e)
         pd = sweep<true>(a.F, a, sm);
         if (pd < 0) {
             alive = false;
