@@ -245,3 +245,38 @@ def test_gpu_features_match_oracle(lib):
     bad[1] = n   # index out of range: rejected before any device work
     assert lib.bqb_warm_features(_lib.dptr(_lib.colmajor(Xm)), _lib.dptr(_lib.colmajor(L)), n, _lib.iptr(bad),
                                  _lib.dptr(values), len(cuts), 0.9, 12.5, None, _lib.fptr(out)) == -1
+
+
+@pytest.mark.gpu
+def test_parent_cuts_reach_children(lib):
+    """B&B with the recorder on: every child node sees its parent's final
+    cuts, so some recorded first-list cuts carry the parent's multiplier
+    (feature 13 = 1), and the parent cuts the child's own separation did not
+    find join the list as candidates (their violation is evaluated at the
+    child's X).  Targets are the multipliers the cuts end with (>= 0)."""
+    feats, targets = warm.record_pairs_bab(lib, [(60, 911)], threads=4, time_limit=60)
+    assert len(targets) > 0 and feats.shape == (len(targets), W.F)
+    assert np.all(np.isfinite(feats)) and np.all(targets >= 0)
+    with_parent = feats[:, 13] > 0.5
+    assert with_parent.any() and (~with_parent).any()
+    assert np.all(feats[with_parent, 12] >= 0) and np.all(feats[~with_parent, 12] == 0)
+
+
+@pytest.mark.gpu
+def test_parent_informed_bab_reaches_reference_optimum(lib):
+    """The parallel B&B with the shipped model on (proposals and a shortlist
+    built from each child's parent cuts) reaches the optimum the reference's
+    serial B&B printed (tests/golden/bab_optima.json); every bound it uses
+    is a bound at some gamma >= 0, so the optimum cannot change."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bab_optima.json")) as fh:
+        case = next(c for c in json.load(fh) if c["kind"] == "int10" and c["nv"] == 80)
+    A = warm.c5_instance(case["nv"], case["seed"])
+    p, _ = warm.load_model(warm.MODEL_C5)
+    warm.use_model(lib, p)
+    try:
+        r = _lib.solve(A, threads=8)
+    finally:
+        warm.use_model(lib, None)
+    assert r["best_value"] == case["max_value"]
