@@ -802,7 +802,7 @@ def run_case(args):
         # the torus's root node on one engine (rank 0), batched GW rounding
         A = np.ascontiguousarray(instances.torus3d(7, 1))
         nv = A.shape[0]
-        _lib.set_params(lib, _lib.make_params())
+        _lib.set_params(lib, _lib.make_params(**({"include_Pent": 0, "include_Hepta": 0} if args.no_kgon else {})))
         lib.process_adj_matrix(_lib.dptr(A.copy()), nv)
         lib.bqb_set_gw_hyperplanes(max(args.hyperplanes, 0))
         glob = _lib.GlobalArrays(lib, nv)
@@ -897,6 +897,7 @@ def main():
     ap.add_argument("--repeats", type=int, default=3, help="--case ipm/ipm-torus: calls")
     ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
     ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
+    ap.add_argument("--no-kgon", action="store_true", help="--case torus-root: no pentagonal / heptagonal cuts")
     ap.add_argument("--hyperplanes", type=int, default=4096,
                     help="--case torus-root: GW hyperplanes per round on an engine (0: the reference's count; "
                          "-1: the drop-in Evaluate instead of an engine)")
