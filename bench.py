@@ -832,10 +832,17 @@ def run_case(args):
         Lc = _lib.colmajor(instances.root_matrix(A))
         X = np.zeros(nv * nv)
         phi = C.c_double()
+        if nv > 128 and args.coop_profile:
+            lib.bqb_ipm_coop_profile_enable(1)
         for _ in range(args.repeats):
             t0 = time.perf_counter()
             lib.ipm_mc_pk(_lib.dptr(Lc), nv, _lib.dptr(X), C.byref(phi), 0)
             print(f"n={nv} phi={phi.value:.6f} wall={1e3 * (time.perf_counter() - t0):.3f} ms", flush=True)
+            if nv > 128 and args.coop_profile:
+                pr = (C.c_double * 8)()
+                lib.bqb_ipm_coop_profile(pr, 1)
+                print("  parts (ms): barrier waits %.3f, panel factors %.3f, tile updates %.3f, products %.3f, "
+                      "call %.3f; %d barriers, %d sweep phases" % tuple(pr[:7]), flush=True)
         return
     nv, count = args.n, args.count
     A = np.ascontiguousarray(instances.gnp_pm1(nv, 0.5, seed=1))
@@ -898,6 +905,7 @@ def main():
     ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
     ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
     ap.add_argument("--no-kgon", action="store_true", help="--case torus-root: no pentagonal / heptagonal cuts")
+    ap.add_argument("--coop-profile", action="store_true", help="--case ipm/ipm-torus: time the multi-CTA IPM by parts")
     ap.add_argument("--hyperplanes", type=int, default=4096,
                     help="--case torus-root: GW hyperplanes per round on an engine (0: the reference's count; "
                          "-1: the drop-in Evaluate instead of an engine)")

@@ -69,7 +69,20 @@ struct CoopArgs {
     double *y, *zd, *dy, *dy1, *dy2, *r, *t;
     double* part;        // gridDim.x x 4 partial sums
     unsigned* bar;       // [0] arrivals, [1] generation, [2] error
+    unsigned long long* prof;   // (may be null) CTA 0's nanoseconds per part, COOP_PROF_* slots
     int n;
+};
+
+// Parts of the time CTA 0 spends in a call (bqb_ipm_coop_profile).
+enum CoopProf : int {
+    COOP_PROF_BARRIER,   // waiting at grid barriers
+    COOP_PROF_FACTOR,    // the panel factorisations (every CTA factors each panel block)
+    COOP_PROF_TILES,     // the sweeps' tile updates
+    COOP_PROF_GEMM,      // the two symmetric products
+    COOP_PROF_TOTAL,     // the whole call
+    COOP_PROF_BARRIERS,  // count of grid barriers
+    COOP_PROF_PHASES,    // count of sweep phases
+    COOP_PROF_WORDS = 8
 };
 
 struct Smem {
@@ -96,10 +109,11 @@ __device__ __forceinline__ unsigned long long global_ns()
 // Grid barrier with a bounded wait.  Returns false once any CTA has given up
 // (then nothing waits any more).  The fences around the arrival make every
 // write before the barrier visible to every read after it.
-__device__ bool grid_sync(unsigned* bar, Smem& sm)
+__device__ bool grid_sync(unsigned* bar, Smem& sm, unsigned long long* prof = nullptr)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
+        const unsigned long long tb = prof && blockIdx.x == 0 ? global_ns() : 0ull;
         volatile unsigned* vb = bar;
         int ok = vb[2] == 0u;
         if (ok) {
@@ -127,6 +141,10 @@ __device__ bool grid_sync(unsigned* bar, Smem& sm)
             __threadfence();
         }
         sm.ok = ok;
+        if (prof && blockIdx.x == 0) {
+            prof[COOP_PROF_BARRIER] += global_ns() - tb;
+            prof[COOP_PROF_BARRIERS] += 1;
+        }
     }
     __syncthreads();
     return sm.ok != 0;
@@ -351,7 +369,15 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
     const int T = (n + CB - 1) / CB;
     for (int K = 0; K < T; ++K) {
         const int k0 = K * CB, b = n - k0 < CB ? n - k0 : CB;
+        const bool rec = a.prof && blockIdx.x == 0 && threadIdx.x == 0;
+        unsigned long long tp = rec ? global_ns() : 0ull;
         if (!panel_factor(A, n, k0, b, sm)) return 0;
+        if (rec) {
+            const unsigned long long t = global_ns();
+            a.prof[COOP_PROF_FACTOR] += t - tp;
+            a.prof[COOP_PROF_PHASES] += 1;
+            tp = t;
+        }
         if (!FULL && K == T - 1) return 1;
         const double* Wprev = a.Wb + (size_t)((K + 1) & 1) * n * CB;
         const double* Dprev = a.Db + (size_t)((K + 1) & 1) * CB * CB;
@@ -361,7 +387,9 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
         const int Tt = T - t0;
         for (int q = blockIdx.x; q < Tt * Tt; q += gridDim.x)
             tile_step<FULL>(A, n, K, k0, b, t0 + q % Tt, t0 + q / Tt, Wprev, Dprev, Wcur, Dcur, sm);
-        if (!grid_sync(a.bar, sm)) return -1;
+        if (a.prof) __syncthreads();
+        if (rec) a.prof[COOP_PROF_TILES] += global_ns() - tp;
+        if (!grid_sync(a.bar, sm, a.prof)) return -1;
     }
     if (FULL) {
         // the last panel's fix, and A = -A
@@ -389,7 +417,7 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
                 }
             }
         }
-        if (!grid_sync(a.bar, sm)) return -1;
+        if (!grid_sync(a.bar, sm, a.prof)) return -1;
     }
     return 1;
 }
@@ -533,11 +561,11 @@ __device__ void warp_rows_rhs(const double* Zi, const double* dX1, const double*
 __device__ bool solve(const CoopArgs& a, const double* b, double* x, Smem& sm)
 {
     warp_rows_matvec(a.F, a.n, b, x);
-    if (!grid_sync(a.bar, sm)) return false;
+    if (!grid_sync(a.bar, sm, a.prof)) return false;
     warp_rows_resid(a.M, a.n, b, x, a.r);
-    if (!grid_sync(a.bar, sm)) return false;
+    if (!grid_sync(a.bar, sm, a.prof)) return false;
     warp_rows_refine(a.F, a.n, a.r, a.t, x);
-    return grid_sync(a.bar, sm);
+    return grid_sync(a.bar, sm, a.prof);
 }
 
 __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
@@ -549,6 +577,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
     const size_t gtid = (size_t)blockIdx.x * CT + threadIdx.x, gstride = (size_t)gridDim.x * CT;
     const double* __restrict__ L = a.L;
     double* X = a.Xbase + (a.xslot ? (size_t)(*a.xslot) * nn : 0);
+    const unsigned long long t_call = a.prof && blockIdx.x == 0 ? global_ns() : 0ull;
 
     // ---- initial point (src/ipm_mc_pk.c:65-99): y_c = sum_r |L_rc| + 1.1,
     // zd = y - diag(L), X = I; psi = trace(L), mu = sum(zd) / 2n, phi = sum(y)
@@ -569,7 +598,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         for (size_t e = gtid; e < nn; e += gstride) X[e] = (e % n == e / n) ? 1.0 : 0.0;
         block_partials(s0, s1, s2, 0.0, sm, a.part);
     }
-    bool alive = grid_sync(a.bar, sm);
+    bool alive = grid_sync(a.bar, sm, a.prof);
     grid_totals(a.part, sm);
     double psi = sm.tot[0];
     double mu = sm.tot[1] / (2.0 * n);
@@ -587,7 +616,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             const int i = (int)(e % n), j = (int)(e / n);
             a.Zi[e] = i == j ? a.zd[i] : -L[e];
         }
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         // (its last phase also writes M = Zi .* X and F = M)
         int pd = sweep<true>(a.Zi, a, sm, X, a.M, a.F);
         if (pd < 0) {
@@ -610,15 +639,21 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         }
         if (!(alive = solve(a, nullptr, a.dy1, sm))) break;
         // dX1 = sym(Zi (-Diag(dy1) X) - X)
+        unsigned long long tg = a.prof && blockIdx.x == 0 ? global_ns() : 0ull;
         gemm_sym(a.Zi, a.dy1, X, nullptr, nullptr, -1.0, X, 0.0, nullptr, n, a.dX1, sm);
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (a.prof) __syncthreads();
+        if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_GEMM] += global_ns() - tg;
+        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         // corrector: rhs = mu diag(Zi) - (Zi .* dX1) dy1; dy2 = F rhs
         warp_rows_rhs(a.Zi, a.dX1, a.dy1, mu, n, a.dy);
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         if (!(alive = solve(a, a.dy, a.dy2, sm))) break;
         // dX = sym(Zi (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1)
+        tg = a.prof && blockIdx.x == 0 ? global_ns() : 0ull;
         gemm_sym(a.Zi, a.dy2, X, a.dy1, a.dX1, 1.0, a.dX1, mu, a.Zi, n, a.dX, sm);
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (a.prof) __syncthreads();
+        if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_GEMM] += global_ns() - tg;
+        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         for (size_t c = gtid; c < (size_t)n; c += gstride) a.dy[c] = a.dy1[c] + a.dy2[c];
 
         // primal line search: X + ap dX positive definite.  Consecutive
@@ -632,7 +667,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         while (true) {
             double* Tt = (tr++ & 1) ? a.T2 : a.T;
             for (size_t e = gtid; e < nn; e += gstride) Tt[e] = fma(ap, a.dX[e], X[e]);
-            if (!(alive = grid_sync(a.bar, sm))) break;
+            if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
             pd = sweep<false>(Tt, a, sm);
             if (pd < 0) {
                 alive = false;
@@ -662,7 +697,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
                 const int i = (int)(e % n), j = (int)(e / n);
                 Tt[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
             }
-            if (!(alive = grid_sync(a.bar, sm))) break;
+            if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
             pd = sweep<false>(Tt, a, sm);
             if (pd < 0) {
                 alive = false;
@@ -712,7 +747,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             }
             block_partials(zx, lx, ys, 0.0, sm, a.part);
         }
-        if (!(alive = grid_sync(a.bar, sm))) break;
+        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         grid_totals(a.part, sm);
         mu = sm.tot[0] / (2.0 * n);
         if (ap + ad > 1.6) mu *= 0.5;
@@ -724,6 +759,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         // barriers, so no barrier is needed here)
     }
     if (!alive) status = IPM_SYNC;
+    if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_TOTAL] += global_ns() - t_call;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out[0] = phi;
         a.out[1] = (double)iter;
@@ -743,6 +779,22 @@ struct CoopConfig {
     int grid = 0;
     size_t smem = 0;
 };
+
+// Per-part timing of CTA 0 (off unless bqb_ipm_coop_profile_enable(1)).
+std::atomic<int> g_coop_prof_on{0};
+DevBuf<unsigned long long> g_coop_prof;
+std::mutex g_coop_prof_mu;
+
+unsigned long long* coop_prof_device()
+{
+    if (!g_coop_prof_on.load()) return nullptr;
+    std::lock_guard<std::mutex> lock(g_coop_prof_mu);
+    if (!g_coop_prof.p) {
+        g_coop_prof.ensure(COOP_PROF_WORDS);
+        BQB_CUDA(cudaMemset(g_coop_prof.p, 0, COOP_PROF_WORDS * sizeof(unsigned long long)));
+    }
+    return g_coop_prof.p;
+}
 
 // The per-size schedule: the grid (CTAs) to use for T = ceil(n / 32) tiles
 // per dimension, filled by the autotuner (bqb_ipm_autotune) or set by hand
@@ -802,6 +854,7 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
     a.xslot = xslot;
     a.out = dout;
     a.stats = ipm_stats_device();
+    a.prof = coop_prof_device();
     a.n = n;
     a.Zi = p;
     a.F = a.Zi + nn;
@@ -917,4 +970,23 @@ BQB_API int bqb_ipm_autotune(int n, int reps, int* best_grid, double* best_ms)
     if (best_grid) *best_grid = bg;
     if (best_ms) *best_ms = bms;
     return 0;
+}
+
+// Time the multi-CTA IPM spends per part (its CTA 0, summed over calls since
+// the last reset): enable (on != 0) or disable the timing; out[8] = {barrier
+// waits, panel factorisations, tile updates, products, whole calls (ms),
+// grid barriers, sweep phases, 0}; reset != 0 zeroes after reading.  For
+// profiling; no reference counterpart.
+BQB_API void bqb_ipm_coop_profile_enable(int on) { g_coop_prof_on.store(on != 0); }
+
+BQB_API void bqb_ipm_coop_profile(double* out, int reset)
+{
+    unsigned long long h[COOP_PROF_WORDS] = {};
+    std::lock_guard<std::mutex> lock(g_coop_prof_mu);
+    if (g_coop_prof.p) {
+        BQB_CUDA(cudaMemcpy(h, g_coop_prof.p, sizeof h, cudaMemcpyDeviceToHost));
+        if (reset) BQB_CUDA(cudaMemset(g_coop_prof.p, 0, sizeof h));
+    }
+    for (int i = 0; i < COOP_PROF_WORDS; ++i)
+        out[i] = i < COOP_PROF_BARRIERS ? 1e-6 * (double)h[i] : (double)h[i];
 }
