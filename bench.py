@@ -832,12 +832,18 @@ def run_case(args):
         Lc = _lib.colmajor(instances.root_matrix(A))
         X = np.zeros(nv * nv)
         phi = C.c_double()
+        lib.bqb_stats_reset()
+        lib.bqb_stats_enable(1)
         if nv > 128 and args.coop_profile:
             lib.bqb_ipm_coop_profile_enable(1)
         for _ in range(args.repeats):
             t0 = time.perf_counter()
             lib.ipm_mc_pk(_lib.dptr(Lc), nv, _lib.dptr(X), C.byref(phi), 0)
             print(f"n={nv} phi={phi.value:.6f} wall={1e3 * (time.perf_counter() - t0):.3f} ms", flush=True)
+            st = (C.c_double * 6)()
+            lib.bqb_ipm_stats(st)
+            lib.bqb_stats_reset()
+            print(f"  IPM iterations {int(st[2])}, line-search trials {int(st[3])}", flush=True)
             if nv > 128 and args.coop_profile:
                 pr = (C.c_double * 8)()
                 lib.bqb_ipm_coop_profile(pr, 1)
