@@ -17,6 +17,9 @@
  *     src/bab_functions.c:199-200.
  *
  * Usage: bqb_ref_bab <instance.rudy> <params>
+ * Environment: BQB_REF_SEED=<s> re-seeds rand() with s after Bab_Init's
+ * srand(2020) (src/bab_functions.c:82), before the root is evaluated, to
+ * sample the spread of the random parts (heuristic, k-gonal annealing).
  * Output: the reference's printFinalOutput block (src/bab_functions.c:351-371).
  */
 #include <stdio.h>
@@ -45,6 +48,9 @@ int main(int argc, char **argv)
     heap = Init_Heap(1000000);
     if (Bab_Init(argc, argv, 0))
         return 1;
+
+    const char *seed = getenv("BQB_REF_SEED");
+    if (seed) srand((unsigned)strtoul(seed, NULL, 10));
 
     TIME = MPI_Wtime();
 

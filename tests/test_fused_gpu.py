@@ -7,15 +7,11 @@ random numbers), a node's bound does not depend on the random streams, and
 the fused kernel runs the engine path's arithmetic (same IPM, lambda_eta,
 bundle step and cut-operator code at the same thread count, the same
 triangle list), so its bounds and fractional solutions must equal the serial
-drop-in SDPbound (src/bounding.c) up to floating-point contraction: the
-shared device bodies are compiled into two kernels, and the compiler may fuse
-a multiply and an add into an FMA in one and not in the other, a last-bit
-difference that the bundle iterations carry to about 1e-8 relative, and
-further when it tips a discrete step (a cut at the violation threshold, a
-serious-step test); most nodes agree bit for bit.  Tolerance: 1e-5 relative
-on bounds, and 1e-2 absolute on fractional solutions (the last column of the
-bundle's X, which the IPM determines only to its stopping gap of 1e-2).  With the random streams in play every bound must
-still be an upper bound of the node."""
+drop-in SDPbound (src/bounding.c) bit for bit.  The library is compiled
+without contraction of multiplies and adds into FMAs (-fmad=false), so the
+device bodies shared by the two kernels round identically in both.  With
+the random streams in play every bound must still be an upper bound of the
+node."""
 import ctypes as C
 
 import numpy as np
@@ -66,10 +62,9 @@ def test_fused_bounds_equal_serial(lib, solved, kmax, seed):
     got = np.zeros(len(nodes))
     assert lib.bqb_bound_nodes_fused(nodes, len(nodes), 1, _lib.dptr(got)) == 0
     assert lib.bqb_fused_fallbacks() == f0
-    np.testing.assert_allclose(got, want, rtol=1e-5, atol=0)
-    assert np.mean(got == want) >= 0.5
+    np.testing.assert_array_equal(got, want)
     for i in range(len(nodes)):
-        np.testing.assert_allclose(nodes[i].fracsol[: NV - 1], ser[i].fracsol[: NV - 1], rtol=0, atol=1e-2)
+        assert list(nodes[i].fracsol[: NV - 1]) == list(ser[i].fracsol[: NV - 1])
 
 
 @pytest.mark.gpu
