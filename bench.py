@@ -814,20 +814,34 @@ def run_case(args):
         C.c_void_p.in_dll(lib, "BabSol").value = C.addressof(sol)
         SP = C.cast(C.c_void_p.in_dll(lib, "SP").value, C.POINTER(_lib.Problem))
         PP = C.cast(C.c_void_p.in_dll(lib, "PP").value, C.POINTER(_lib.Problem))
-        for _ in range(args.repeats):
+        lib.bqb_set_root_effort(1 if args.root_effort else 0)
+        for rep in range(args.repeats):
+            seed = args.seed + rep
             nodes = (_lib.BabNode * 1)()
             b = np.zeros(1)
             lib.bqb_reset_incumbent(0.0)
             lib.bqb_bundle_iterations(1)
+            lib.bqb_bound_trace_enable(1)
             t0 = time.perf_counter()
             if args.hyperplanes < 0:   # the drop-in: Evaluate on the library's default engine
-                C.CDLL("libc.so.6").srand(2020)
+                C.CDLL("libc.so.6").srand(seed)
                 b[0] = lib.Evaluate(C.byref(nodes[0]), SP, PP, 0)
             else:
+                assert lib.bqb_seed_engines(seed) == 0
                 assert lib.bqb_bound_nodes(nodes, 1, 0, 1, None, _lib.dptr(b)) == 0, lib.bqb_last_error()
-            print(f"torus root bound={b[0]:.3f} incumbent={lib.Bab_LBGet():.0f} "
-                  f"wall={time.perf_counter() - t0:.3f} s bundle_iterations={lib.bqb_bundle_iterations(1)}",
-                  flush=True)
+            wall = time.perf_counter() - t0
+            rows = lib.bqb_bound_trace(None, 0)
+            tr = np.zeros(rows * 9)
+            lib.bqb_bound_trace(_lib.dptr(tr), rows)
+            lib.bqb_bound_trace_enable(0)
+            tr = tr.reshape(rows, 9)
+            print(f"torus root seed={seed} root_effort={int(args.root_effort)} bound={b[0]:.3f} "
+                  f"incumbent={lib.Bab_LBGet():.0f} wall={wall:.3f} s "
+                  f"bundle_iterations={lib.bqb_bundle_iterations(1)}", flush=True)
+            for r in tr:
+                print(f"  round {int(r[2]):2d} bound={r[3]:.1f} incumbent={r[4]:.0f} cuts={int(r[5])}/{int(r[6])}/"
+                      f"{int(r[7])} t={r[8]:.2f} s", flush=True)
+        lib.bqb_set_root_effort(0)
         del glob
         return
     if args.case in ("ipm", "ipm-torus"):
@@ -915,6 +929,10 @@ def main():
     ap.add_argument("--count", type=int, default=16, help="--case fused: subproblems")
     ap.add_argument("--kmax", type=int, default=20, help="--case fused: most fixed vertices")
     ap.add_argument("--no-kgon", action="store_true", help="--case torus-root: no pentagonal / heptagonal cuts")
+    ap.add_argument("--root-effort", action="store_true",
+                    help="--case torus-root: every outer round at the root unless pruned (no early give-up)")
+    ap.add_argument("--seed", type=int, default=2020,
+                    help="--case torus-root: srand seed of the drop-in, or the engines' seed base (+1 per repeat)")
     ap.add_argument("--coop-profile", action="store_true", help="--case ipm/ipm-torus: time the multi-CTA IPM by parts")
     ap.add_argument("--hyperplanes", type=int, default=4096,
                     help="--case torus-root: GW hyperplanes per round on an engine (0: the reference's count; "

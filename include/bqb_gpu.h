@@ -243,6 +243,27 @@ long long bqb_heuristic_runs(int reset);
  * counterpart. */
 long long bqb_bundle_iterations(int reset);
 
+/* Root effort: full != 0 makes SDPbound run its outer loop to
+ * max_outer_iter + extra_iter rounds at rank 0 (the root) unless the node is
+ * pruned, skipping the two early give-up tests (src/bounding.c:203-214).
+ * Nodes with rank != 0 keep the reference's rule.  Off by default.  No
+ * reference counterpart. */
+void bqb_set_root_effort(int full);
+
+/* Trace of SDPbound's outer loop (inspection): on != 0 clears the trace and
+ * starts recording; bqb_bound_trace copies up to max_rows rows of 9 values
+ * (node number, rank, round, bound, incumbent, triangle / pentagonal /
+ * heptagonal cuts after the round, seconds since the node's loop started)
+ * and returns the rows recorded.  No reference counterpart. */
+void bqb_bound_trace_enable(int on);
+
+/* Restart the engines' random streams: engine i draws from the stream
+ * srand(base + i) gives (base 2021 by default) and seeds its annealing
+ * chains from base + i.  Returns 1 (nothing changed) while an engine is
+ * leased, else 0.  No reference counterpart. */
+int bqb_seed_engines(unsigned base);
+int bqb_bound_trace(double *out, int max_rows);
+
 /* Tensor-core product D = A B^T (tcgen05.mma kind::tf32, FP32 accumulation
  * in tensor memory, operands staged by TMA): the kernel behind the batched
  * Goemans-Williamson projection S = Lf V of many hyperplanes at once (the

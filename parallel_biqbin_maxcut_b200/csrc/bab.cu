@@ -510,13 +510,15 @@ namespace {
 std::mutex g_pool_mu;
 std::vector<bqb::Engine*> g_pool;
 std::vector<char> g_pool_busy;
+unsigned g_pool_seed = 2021u;
 
 // k private engines leased to the caller alone (concurrent callers get
 // different engines; an engine and its buffers are never shared by two
 // bounding threads), sized for problems up to N x N.  The first free
 // engines are taken in creation order, so a single caller always gets
-// engines 0..k-1; engine i draws random numbers from the stream srand(2021 + i)
-// would give.  The lease ends when the returned object goes away.
+// engines 0..k-1; engine i draws random numbers from the stream srand(base + i)
+// would give (base 2021 unless bqb_seed_engines changed it).  The lease ends
+// when the returned object goes away.
 struct EngineLease {
     std::vector<bqb::Engine*> e;
     EngineLease(int k, int N)
@@ -528,7 +530,7 @@ struct EngineLease {
                 e.push_back(g_pool[i]);
             }
         while ((int)e.size() < k) {
-            g_pool.push_back(bqb::engine_create(2021u + (unsigned)g_pool.size()));
+            g_pool.push_back(bqb::engine_create(g_pool_seed + (unsigned)g_pool.size()));
             g_pool_busy.push_back(1);
             e.push_back(g_pool.back());
         }
@@ -545,6 +547,24 @@ struct EngineLease {
 };
 
 }  // namespace
+
+// Restart the engines' random streams: engine i (existing or created later)
+// draws from the stream srand(base + i) gives, and its annealing chains from
+// seeds derived from base + i.  Returns 1 while an engine is leased (nothing
+// changes), else 0.
+BQB_API int bqb_seed_engines(unsigned base)
+{
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    for (char b : g_pool_busy)
+        if (b) return 1;
+    g_pool_seed = base;
+    for (size_t i = 0; i < g_pool.size(); ++i) {
+        g_pool[i]->rng.seed(base + (unsigned)i);
+        g_pool[i]->sa_seed = (uint64_t)(base + (unsigned)i) << 32;
+        g_pool[i]->sa_calls = 0;
+    }
+    return 0;
+}
 
 // Bound `count` independent nodes of the problem in SP (set up by
 // process_adj_matrix) with `threads` concurrent engines; bounds[i] receives

@@ -13,6 +13,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <chrono>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -33,6 +35,21 @@ namespace bqb {
 std::atomic<bqb_heuristic_fn> g_heuristic_hook{nullptr};
 std::atomic<long long> g_heuristic_runs{0};
 std::atomic<long long> g_bundle_iters{0};
+
+// Root effort: with it on, a node bounded with rank 0 (the root) runs the
+// outer loop of SDPbound to max_outer_iter + extra_iter rounds unless it is
+// pruned, skipping the two early give-up tests of src/bounding.c:203-214.
+// The bound stays a valid bound (the loop only runs longer); the reference
+// has no such switch, so it is off unless the caller turns it on.
+std::atomic<int> g_root_effort{0};
+
+// Trace of SDPbound's outer loop: one row of BQB_TRACE_COLS values per
+// round while tracing is on (inspection only).
+constexpr int BQB_TRACE_COLS = 9;
+std::atomic<int> g_trace_on{0};
+std::mutex g_trace_mu;
+std::vector<double> g_trace;
+std::atomic<long long> g_trace_node{0};
 
 void upload_cuts(Engine& E, const HostState& H, const Problem* P)
 {
@@ -352,6 +369,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
 
     int count = 0;
     bool done = false, prune = false, giveup = false;
+    const bool root_effort = rank == 0 && g_root_effort.load() != 0;
+    const long long trace_id = g_trace_on.load() ? g_trace_node.fetch_add(1) : -1;
+    const auto trace_t0 = std::chrono::steady_clock::now();
     while (!done) {
         ++count;
         const double oldf = f;
@@ -363,10 +383,12 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             prune = bound < Bab_LBGet() + 1.0;
         }
         const double gap = bound - Bab_LBGet();
-        if (count == params.triag_iter + params.pent_iter + params.hept_iter)
-            if (gap - 1.0 > (oldf - f) * (params.max_outer_iter - count)) giveup = true;
-        if (count == params.max_outer_iter)
-            if (gap - 1.0 > (oldf - f) * params.extra_iter) giveup = true;
+        if (!root_effort) {
+            if (count == params.triag_iter + params.pent_iter + params.hept_iter)
+                if (gap - 1.0 > (oldf - f) * (params.max_outer_iter - count)) giveup = true;
+            if (count == params.max_outer_iter)
+                if (gap - 1.0 > (oldf - f) * params.extra_iter) giveup = true;
+        }
         if (count == params.max_outer_iter + params.extra_iter) giveup = true;
 
         if (!prune && !giveup) {
@@ -400,6 +422,14 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         // calls BLAS with m = 0 there, which is undefined); stop here
         done = prune || giveup || PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq == 0;
         store_fracsol();
+        if (trace_id >= 0) {
+            const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - trace_t0).count();
+            const double row[BQB_TRACE_COLS] = {(double)trace_id, (double)rank,  (double)count,
+                                                bound,            Bab_LBGet(),   (double)PP_->NIneq,
+                                                (double)PP_->NPentIneq, (double)PP_->NHeptaIneq, secs};
+            std::lock_guard<std::mutex> g(g_trace_mu);
+            g_trace.insert(g_trace.end(), row, row + BQB_TRACE_COLS);
+        }
 
         if (!done) {
             for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
@@ -482,6 +512,32 @@ BQB_API long long bqb_heuristic_runs(int reset)
 BQB_API long long bqb_bundle_iterations(int reset)
 {
     return reset ? g_bundle_iters.exchange(0) : g_bundle_iters.load();
+}
+
+// Root effort on (1) or off (0, the reference's give-up rule at every node).
+BQB_API void bqb_set_root_effort(int full) { g_root_effort.store(full ? 1 : 0); }
+
+// Tracing of SDPbound's outer loop on (1) / off (0); switching it on clears
+// the trace and restarts the node numbering.
+BQB_API void bqb_bound_trace_enable(int on)
+{
+    std::lock_guard<std::mutex> g(g_trace_mu);
+    g_trace.clear();
+    g_trace_node.store(0);
+    g_trace_on.store(on ? 1 : 0);
+}
+
+// Copies up to max_rows trace rows (node, rank, round, bound, incumbent,
+// triangle / pentagonal / heptagonal cuts after the round's separation,
+// seconds since the node's loop started) into out and returns the number
+// of rows recorded so far.
+BQB_API int bqb_bound_trace(double* out, int max_rows)
+{
+    std::lock_guard<std::mutex> g(g_trace_mu);
+    const int rows = (int)(g_trace.size() / BQB_TRACE_COLS);
+    const int k = rows < max_rows ? rows : max_rows;
+    if (out && k > 0) memcpy(out, g_trace.data(), (size_t)k * BQB_TRACE_COLS * sizeof(double));
+    return rows;
 }
 
 // SDPbound (src/bounding.c:24-342) in the default engine: the reference's
