@@ -84,7 +84,11 @@ LEG_CALLS = {
     "fused": "bqb_solve_fused (batches of 2 x SMs, 8 in flight), FP64",
     "fused_learned": "bqb_solve_fused (batches of 2 x SMs, 8 in flight) with the shipped warm-start model",
     "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply), "
-               "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32)",
+               "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32), root effort "
+               "(the root runs every outer round of SDPbound unless pruned)",
+    "engines_learned": "the engines leg with the shipped warm-start model (children start from the parent's "
+                       "multipliers where the model keeps them)",
+    "device_pool_root_effort": "bqb_solve_device with root effort (the root runs every outer round unless pruned)",
     "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
     "device_pool": "bqb_solve_device: the whole tree in one persistent launch, open-node pool on the device",
 }
@@ -446,13 +450,15 @@ def run_gpu(args):
         fused_kw = dict(fused_batch=2 * sms, fused_depth=8)
         cases = [("n100", TTO_NAME, tto_instance(),
                   [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w),
-                   ("device_pool", dict(device_pool=True), None)])]
+                   ("device_pool", dict(device_pool=True), None),
+                   ("device_pool_root_effort", dict(device_pool=True, root_effort=True), None)])]
         if args.tto_torus:
             # the multi-CTA IPM's per-size schedule for the torus's sizes
             # (n = 343 and its subproblems, the same panel count)
             tto_sched = _lib.autotune_ipm([343], reps=2)
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
-                          [("engines", dict(threads=16, gw_hyperplanes=4096), None)]))
+                          [("engines", dict(threads=16, gw_hyperplanes=4096, root_effort=True), None),
+                           ("engines_learned", dict(threads=16, gw_hyperplanes=4096, root_effort=True), p_w)]))
         tto = {}
         for key, name, A, legs in cases:
             e = {"instance": name}
@@ -866,7 +872,8 @@ def run_case(args):
                 pr = (C.c_double * 8)()
                 lib.bqb_ipm_coop_profile(pr, 1)
                 print("  parts (ms): barrier waits %.3f, panel factors %.3f, tile updates %.3f, products %.3f, "
-                      "call %.3f; %d barriers, %d sweep phases" % tuple(pr[:7]), flush=True)
+                      "call %.3f; %d barriers, %d sweep phases; panel block loads %.3f ms" % tuple(pr[:8]),
+                      flush=True)
         return
     nv, count = args.n, args.count
     A = np.ascontiguousarray(instances.gnp_pm1(nv, 0.5, seed=1))

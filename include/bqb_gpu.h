@@ -439,8 +439,9 @@ void bqb_ipm_schedule_set(int n, int grid);
 /* Timing of the multi-CTA IPM by parts (its first CTA, summed over calls;
  * off by default): out[8] = {ms waiting at grid barriers, ms in panel
  * factorisations, ms in tile updates, ms in the products, ms in whole
- * calls, grid barriers, sweep phases, 0}; reset != 0 zeroes after
- * reading.  For profiling; no reference counterpart. */
+ * calls, grid barriers, sweep phases, ms of the panel factorisations
+ * spent loading the panel block}; reset != 0 zeroes after reading.  For
+ * profiling; no reference counterpart. */
 void bqb_ipm_coop_profile_enable(int on);
 void bqb_ipm_coop_profile(double *out, int reset);
 int bqb_ipm_autotune(int n, int reps, int *best_grid, double *best_ms);

@@ -278,20 +278,30 @@ def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: 
 class GlobalArrays:
     """Allocates the reference-layout globals in a library (X, Z, X_test,
     dual_gamma, ..., cut arrays) and points the library's pointer globals at
-    them, as src/allocate_free.c:8-42 does.  Keeps the buffers alive."""
+    them, as src/allocate_free.c:8-42 does.  Keeps the buffers alive.
 
-    def __init__(self, cdll, N: int, bundle_cap: int = 64, mmax: int = 20000, list_cap: int = 20000):
+    Capacities follow the reference (src/biqbin.h:37-42): 50,000 cuts of
+    each kind and 150,000 entries in the multiplier vectors, which SDPbound
+    fills up to the current number of cuts (a 343-vertex torus root holds
+    about 21,000).  The host bundle arrays (X_bundle, G, lambda, F) are read
+    and written only by the drop-in bundle_method, for bundles of at most
+    ``bundle_cap`` elements over at most ``g_rows`` cuts; SDPbound keeps its
+    bundle on the device."""
+
+    def __init__(self, cdll, N: int, bundle_cap: int = 64, g_rows: int = 20000, list_cap: int = 20000,
+                 cut_cap: int = 50000):
         self.cdll = cdll
         self.N = N
+        mmax = 3 * cut_cap
         dbl = {"X": N * N, "Z": N * N, "X_test": N * N, "X_bundle": N * N * bundle_cap,
                "dual_gamma": mmax, "dgamma": mmax, "gamma_test": mmax, "eta": mmax, "g": mmax,
-               "lambda": bundle_cap, "F": bundle_cap, "G": mmax * bundle_cap}
+               "lambda": bundle_cap, "F": bundle_cap, "G": g_rows * bundle_cap}
         self.arr = {name: np.zeros(size) for name, size in dbl.items()}
-        self.cuts = (TriIneq * mmax)()
+        self.cuts = (TriIneq * cut_cap)()
         self.lst = (TriIneq * list_cap)()
-        self.pcuts = (PentIneq * mmax)()
+        self.pcuts = (PentIneq * cut_cap)()
         self.plst = (PentIneq * list_cap)()
-        self.hcuts = (HeptIneq * mmax)()
+        self.hcuts = (HeptIneq * cut_cap)()
         self.hlst = (HeptIneq * list_cap)()
         self.bind()
 

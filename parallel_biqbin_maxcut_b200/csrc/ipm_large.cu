@@ -82,6 +82,7 @@ enum CoopProf : int {
     COOP_PROF_TOTAL,     // the whole call
     COOP_PROF_BARRIERS,  // count of grid barriers
     COOP_PROF_PHASES,    // count of sweep phases
+    COOP_PROF_PF_LOAD,   // the part of the panel factorisations spent loading the panel block
     COOP_PROF_WORDS = 8
 };
 
@@ -191,9 +192,10 @@ __device__ void grid_totals(const double* part, Smem& sm)
 // update of the rows below.  Instantiated for every Q so that every index
 // into s[] is a constant and s[] stays in registers.  No early exit: after a
 // non-positive pivot (the same d in every lane) the steps go on with a unit
-// pivot and the caller discards the result.
+// pivot and the caller discards the result.  Lane Q keeps the pivot's
+// reciprocal square root, the reciprocal of its diagonal entry of the factor.
 template <int Q>
-__device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
+__device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd, double& rdiag)
 {
     if constexpr (Q < CB) {
         double d = __shfl_sync(0xffffffffu, s[Q], Q);
@@ -204,13 +206,17 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
         const double rs = rsqrt(d);   // one reciprocal square root per pivot
         const double l = d * rs;
         const double lpq = p == Q ? l : s[Q] * rs;
+        if (p == Q) rdiag = rs;
         s[Q] = lpq;
 #pragma unroll
         for (int r = Q + 1; r < CB; ++r) {
             const double lrq = __shfl_sync(0xffffffffu, lpq, r);
-            if (r <= p) s[r] = fma(-lpq, lrq, s[r]);
+            // lane r's own entry l_rq is lpq: its diagonal update (the next
+            // pivot, for r = Q + 1) does not wait for the shuffle
+            if (r < p) s[r] = fma(-lpq, lrq, s[r]);
+            else if (r == p) s[r] = fma(-lpq, lpq, s[r]);
         }
-        chol_step<Q + 1>(s, p, pd);
+        chol_step<Q + 1>(s, p, pd, rdiag);
     }
 }
 
@@ -218,15 +224,23 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd)
 // li[I] = (delta_It - sum_{k < I} D[I][k] li[k]) / D[I][I] (zero above the
 // diagonal, where every term is zero).  Instantiated for every I so that li[]
 // stays in registers; the D entries are shared-memory broadcasts that do not
-// depend on the chain.
+// depend on the chain.  The sum runs in four interleaved partial sums, so
+// the dependent chain per step is a quarter as long.
 template <int I>
 __device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int t)
 {
     if constexpr (I < CB) {
-        double acc = I == t ? 1.0 : 0.0;
+        double a0 = I == t ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
-        for (int k = 0; k < I; ++k) acc = fma(-sm.D[I][k], li[k], acc);
-        li[I] = acc * sm.R[I];
+        for (int k = 0; k + 3 < I; k += 4) {
+            a0 = fma(-sm.D[I][k], li[k], a0);
+            a1 = fma(-sm.D[I][k + 1], li[k + 1], a1);
+            a2 = fma(-sm.D[I][k + 2], li[k + 2], a2);
+            a3 = fma(-sm.D[I][k + 3], li[k + 3], a3);
+        }
+#pragma unroll
+        for (int k = I & ~3; k < I; ++k) a0 = fma(-sm.D[I][k], li[k], a0);
+        li[I] = ((a0 + a1) + (a2 + a3)) * sm.R[I];
         linv_step<I + 1>(li, sm, t);
     }
 }
@@ -236,28 +250,29 @@ __device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int 
 // block is padded to 32 x 32 with the identity), then lane t forms column t
 // of Li by forward substitution.  Returns false (in every thread) on a
 // non-positive pivot.
-__device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm)
+__device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, unsigned long long* load_ns)
 {
     const int tid = threadIdx.x;
+    const unsigned long long t0 = load_ns ? global_ns() : 0ull;
     for (int e = tid; e < CB * CB; e += CT) {
         const int p = e % CB, q = e / CB;
         sm.D[p][q] = p < b && q < b ? A[(k0 + p) + (size_t)(k0 + q) * n] : (p == q ? 1.0 : 0.0);
     }
     __syncthreads();
+    if (load_ns) *load_ns += global_ns() - t0;
     if (tid < 32) {
         const int p = tid;
         double s[CB];
 #pragma unroll
         for (int r = 0; r < CB; ++r) s[r] = sm.D[p][r];
         int pd = 1;
-        chol_step<0>(s, p, pd);
+        double rdiag = 1.0;
+        chol_step<0>(s, p, pd, rdiag);
         if (p == 0) sm.pd = pd;
         if (pd) {
 #pragma unroll
             for (int r = 0; r < CB; ++r) sm.D[p][r] = r <= p ? s[r] : 0.0;
-#pragma unroll
-            for (int r = 0; r < CB; ++r)
-                if (r == p) sm.R[p] = 1.0 / s[r];
+            sm.R[p] = rdiag;
         }
         __syncwarp();
         if (pd) {
@@ -371,7 +386,7 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
         const int k0 = K * CB, b = n - k0 < CB ? n - k0 : CB;
         const bool rec = a.prof && blockIdx.x == 0 && threadIdx.x == 0;
         unsigned long long tp = rec ? global_ns() : 0ull;
-        if (!panel_factor(A, n, k0, b, sm)) return 0;
+        if (!panel_factor(A, n, k0, b, sm, rec ? a.prof + COOP_PROF_PF_LOAD : nullptr)) return 0;
         if (rec) {
             const unsigned long long t = global_ns();
             a.prof[COOP_PROF_FACTOR] += t - tp;
@@ -975,7 +990,8 @@ BQB_API int bqb_ipm_autotune(int n, int reps, int* best_grid, double* best_ms)
 // Time the multi-CTA IPM spends per part (its CTA 0, summed over calls since
 // the last reset): enable (on != 0) or disable the timing; out[8] = {barrier
 // waits, panel factorisations, tile updates, products, whole calls (ms),
-// grid barriers, sweep phases, 0}; reset != 0 zeroes after reading.  For
+// grid barriers, sweep phases, the panel factorisations' block loads (ms)};
+// reset != 0 zeroes after reading.  For
 // profiling; no reference counterpart.
 BQB_API void bqb_ipm_coop_profile_enable(int on) { g_coop_prof_on.store(on != 0); }
 
@@ -988,5 +1004,5 @@ BQB_API void bqb_ipm_coop_profile(double* out, int reset)
         if (reset) BQB_CUDA(cudaMemset(g_coop_prof.p, 0, sizeof h));
     }
     for (int i = 0; i < COOP_PROF_WORDS; ++i)
-        out[i] = i < COOP_PROF_BARRIERS ? 1e-6 * (double)h[i] : (double)h[i];
+        out[i] = (i < COOP_PROF_BARRIERS || i == COOP_PROF_PF_LOAD) ? 1e-6 * (double)h[i] : (double)h[i];
 }
