@@ -86,6 +86,9 @@ LEG_CALLS = {
     "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply), "
                "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32), root effort "
                "(the root runs every outer round of SDPbound unless pruned)",
+    "engines_parent_start": "the engines leg with parent start (each child starts from its parent's final "
+                            "triangle, pentagonal and heptagonal cuts and multipliers when that start's dual "
+                            "value is lower)",
     "engines_learned": "the engines leg with the shipped warm-start model (children start from the parent's "
                        "multipliers where the model keeps them)",
     "device_pool_root_effort": "bqb_solve_device with root effort (the root runs every outer round unless pruned)",
@@ -458,6 +461,8 @@ def run_gpu(args):
             tto_sched = _lib.autotune_ipm([343], reps=2)
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
                           [("engines", dict(threads=16, gw_hyperplanes=4096, root_effort=True), None),
+                           ("engines_parent_start", dict(threads=16, gw_hyperplanes=4096, root_effort=True,
+                                                         parent_start=True), None),
                            ("engines_learned", dict(threads=16, gw_hyperplanes=4096, root_effort=True), p_w)]))
         tto = {}
         for key, name, A, legs in cases:

@@ -250,6 +250,17 @@ long long bqb_bundle_iterations(int reset);
  * reference counterpart. */
 void bqb_set_root_effort(int full);
 
+/* Parent start: on != 0 makes every node bounded by SDPbound export its
+ * final cuts (triangle, pentagonal, heptagonal) and multipliers, and makes
+ * bqb_solve_parallel start each child from its parent's: the parent's cuts
+ * that avoid the child's fixed vertices join the child's first cut list
+ * with the parent's multipliers; that start is evaluated once (one IPM) and
+ * kept when its dual value is below the plain start's.  Bounds stay valid
+ * (inherited cuts are valid for the child; any multipliers >= 0 bound).  A
+ * loaded warm-start model (bqb_warm_enable) takes precedence.  Off by
+ * default.  No reference counterpart. */
+void bqb_set_parent_start(int on);
+
 /* Trace of SDPbound's outer loop (inspection): on != 0 clears the trace and
  * starts recording; bqb_bound_trace copies up to max_rows rows of 9 values
  * (node number, rank, round, bound, incumbent, triangle / pentagonal /

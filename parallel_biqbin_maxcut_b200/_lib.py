@@ -147,6 +147,7 @@ SIGNATURES = {
     "bqb_heuristic_runs": (C.c_longlong, [C.c_int]),
     "bqb_bundle_iterations": (C.c_longlong, [C.c_int]),
     "bqb_set_root_effort": (None, [C.c_int]),
+    "bqb_set_parent_start": (None, [C.c_int]),
     "bqb_bound_trace_enable": (None, [C.c_int]),
     "bqb_bound_trace": (C.c_int, [D, C.c_int]),
     "bqb_seed_engines": (C.c_int, [C.c_uint]),
@@ -241,7 +242,7 @@ def make_params(**overrides) -> Params:
 
 def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: int = 4,
           gw_hyperplanes: int = 0, device_pool: bool = False, pool_nodes: int = 0, root_effort: bool = False,
-          **param_overrides) -> dict:
+          parent_start: bool = False, **param_overrides) -> dict:
     """Solve Max-Cut on ``adj`` to optimality (best-first B&B, GPU bounding;
     ``threads`` > 1 bounds that many nodes concurrently on engines;
     ``fused_batch`` > 0 bounds batches of up to that many nodes with the
@@ -249,10 +250,13 @@ def solve(adj: np.ndarray, threads: int = 1, fused_batch: int = 0, fused_depth: 
     > 0: the engines' GW rounds project that many hyperplanes at once on
     the tensor cores; ``device_pool``: the whole tree in one persistent
     launch with the open-node pool on the device); ``root_effort``: the
-    root runs every outer round of SDPbound unless pruned)."""
+    root runs every outer round of SDPbound unless pruned; ``parent_start``:
+    with ``threads`` > 1, each child starts from its parent's final cuts and
+    multipliers)."""
     lib = load()
     lib.bqb_set_gw_hyperplanes(int(gw_hyperplanes))
     lib.bqb_set_root_effort(1 if root_effort else 0)
+    lib.bqb_set_parent_start(1 if parent_start else 0)
     A = np.ascontiguousarray(adj, dtype=np.float64)
     p = make_params(**param_overrides)
     res = SolveResult()

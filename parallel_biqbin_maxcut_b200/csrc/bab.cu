@@ -652,8 +652,8 @@ BQB_API int bqb_solve_parallel(const double* adj, int num_vertices, const BiqBin
     std::condition_variable cv;
     int active = 0;
     bool stop = false;
-    // with the learned warm start or the recorder on, each child bounds with
-    // its parent's final cuts (bqb::Engine::parent)
+    // with the learned warm start, the recorder or the parent start on, each
+    // child bounds with its parent's final cuts (bqb::Engine::parent)
     std::unordered_map<BabNode*, std::shared_ptr<bqb::ParentCuts>> parent_of;
     auto branch = [&](BabNode* node, const std::shared_ptr<bqb::ParentCuts>& cuts = nullptr) {
         const int ic = getBranchingVariable(node);

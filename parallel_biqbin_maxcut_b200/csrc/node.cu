@@ -16,6 +16,7 @@
 #include <chrono>
 #include <mutex>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "internal.h"
@@ -42,6 +43,18 @@ std::atomic<long long> g_bundle_iters{0};
 // The bound stays a valid bound (the loop only runs longer); the reference
 // has no such switch, so it is off unless the caller turns it on.
 std::atomic<int> g_root_effort{0};
+
+// Parent start: with it on, every node exports its final cuts (triangle,
+// pentagonal, heptagonal; original vertex numbers) and multipliers, and a
+// node bounded with its parent's cuts (a B&B driver sets Engine::parent)
+// starts from them: the parent's cuts that avoid the child's fixed vertices
+// join the child's first cut list with the parent's multipliers, and that
+// start is evaluated once (one IPM) and kept when its dual value is below the
+// plain start's, as the learned warm start's proposal is.  Every cut of the
+// parent that avoids the fixed vertices is valid for the child, and any
+// multipliers >= 0 give a valid bound.  Off unless the caller turns it on; a
+// loaded warm-start model takes precedence.
+std::atomic<int> g_parent_start{0};
 
 // Trace of SDPbound's outer loop: one row of BQB_TRACE_COLS values per
 // round while tracing is on (inspection only).
@@ -233,12 +246,15 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     // say which of them the bundle keeps.
     const bool warm_on = warm_active();
     const bool warm_rec = warm_recording();
+    const bool pstart_on = g_parent_start.load() != 0;
+    const bool pstart = pstart_on && !warm_on && !warm_rec && E.parent != nullptr;
+    bool inherited = false;   // this node's list holds its parent's k-gonal cuts
     std::vector<float> warm_feats;
     std::vector<Triangle_Inequality> warm_first;
     double warm_scale = 1.0;
     std::vector<int> orig;   // subproblem vertex -> original vertex
     const int n_own = PP_->NIneq;
-    if (warm_on || warm_rec) {
+    if (warm_on || warm_rec || pstart_on) {
         orig.resize(n);
         int idx = 0;
         for (int i = 0; i < NB && idx < n - 1; ++i)
@@ -336,6 +352,94 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             upload_cuts(E, H, PP_);
         }
     }
+    if (pstart) {
+        const ParentCuts& PC = *E.parent;
+        std::vector<int> cidx(NB + 1, -1);
+        for (int q = 0; q < n; ++q) cidx[orig[q]] = q;
+        std::unordered_set<uint64_t> have;
+        have.reserve((size_t)n_own * 2 + 16);
+        std::vector<double> prop;
+        prop.reserve((size_t)n_own + PC.key.size() + PC.pent.size() + PC.hept.size());
+        for (int c = 0; c < n_own; ++c) {
+            const Triangle_Inequality& t = H.cuts[c];
+            have.insert(orig_cut_key(t.type, orig[t.i], orig[t.j], orig[t.k]));
+            prop.push_back(H.cuts[c].y);
+        }
+        int m = n_own;
+        for (size_t c = 0; c < PC.key.size() && m < BQB_MAX_TRI_INEQ; ++c) {
+            if (!(PC.gam[c] > 0.0) || have.count(PC.key[c])) continue;
+            const int a = cidx[(PC.key[c] >> 32) & 0xFFFF], bb = cidx[(PC.key[c] >> 16) & 0xFFFF],
+                      cc = cidx[PC.key[c] & 0xFFFF];
+            if (a < 0 || bb < 0 || cc < 0) continue;   // a vertex the child fixed
+            Triangle_Inequality& t = H.cuts[m++];
+            t.type = (int)(PC.key[c] >> 48);
+            t.i = a;
+            t.j = bb;
+            t.k = cc;
+            t.value = 0.0;
+            t.y = PC.gam[c];
+            prop.push_back(PC.gam[c]);
+        }
+        // k-gonal cuts: every vertex must survive in the child
+        auto map_kgon = [&](const ParentKgon& q, int k, int* perm) {
+            for (int a = 0; a < k; ++a) {
+                perm[a] = cidx[q.v[a]];
+                if (perm[a] < 0) return false;
+            }
+            return true;
+        };
+        int np = 0, nh = 0;
+        for (const ParentKgon& q : PC.pent) {
+            if (np >= BQB_MAX_PENT_INEQ) break;
+            Pentagonal_Inequality& c = H.pcuts[np];
+            if (!(q.gam > 0.0) || !map_kgon(q, 5, c.permutation)) continue;
+            c.type = q.type;
+            c.value = 0.0;
+            c.y = q.gam;
+            ++np;
+        }
+        for (const ParentKgon& q : PC.hept) {
+            if (nh >= BQB_MAX_HEPTA_INEQ) break;
+            Heptagonal_Inequality& c = H.hcuts[nh];
+            if (!(q.gam > 0.0) || !map_kgon(q, 7, c.permutation)) continue;
+            c.type = q.type;
+            c.value = 0.0;
+            c.y = q.gam;
+            ++nh;
+        }
+        for (int i = 0; i < np; ++i) prop.push_back(H.pcuts[i].y);
+        for (int i = 0; i < nh; ++i) prop.push_back(H.hcuts[i].y);
+        if (m > n_own || np > 0 || nh > 0) {
+            PP_->NIneq = m;
+            PP_->NPentIneq = np;
+            PP_->NHeptaIneq = nh;
+            upload_cuts(E, H, PP_);
+            const int mt = nd.cuts.m;
+            double* gp = nd.b.gam.p;
+            BQB_CUDA(cudaMemcpyAsync(gp, prop.data(), (size_t)mt * sizeof(double), cudaMemcpyHostToDevice, s));
+            BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            opBt_launch(nd.cuts, nd.L0.p, n, gp, s);
+            double* Xw = E.warm.X.ensure(nn);
+            ipm_device(E.ipm_ws, nd.L0.p, Xw, n, dout, s);
+            BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BQB_CUDA(cudaStreamSynchronize(s));
+            double fw = nd.hs.p[0];
+            for (int i = 0; i < mt; ++i) fw += prop[i];
+            const bool keep = (int)nd.hs.p[2] == IPM_OK && fw < f;
+            warm_count(keep);
+            if (keep) {
+                for (int i = 0; i < mt; ++i) H.dual_gamma[i] = prop[i];
+                BQB_CUDA(cudaMemcpyAsync(dX, Xw, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                f = fw;
+                inherited = true;
+            } else {
+                PP_->NIneq = n_own;   // back to the child's own cuts
+                PP_->NPentIneq = 0;
+                PP_->NHeptaIneq = 0;
+                upload_cuts(E, H, PP_);
+            }
+        }
+    }
     if (warm_rec) {
         // the features of the first list as it stands (own cuts, then the
         // shortlisted or, without a model, all parent candidates)
@@ -399,6 +503,16 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             BQB_CUDA(cudaStreamSynchronize(s));
             viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
             const bool do_pent = params.include_Pent && (count > params.triag_iter || viol3 < 0.2);
+            const bool do_hept = params.include_Hepta && ((count > params.triag_iter + params.pent_iter) ||
+                                                          (viol3 < 0.2 && (1 - viol5 < 0.4)));
+            if (inherited) {
+                // inherited k-gonal cuts carry the bundle's current
+                // multipliers into rounds that do not separate them
+                if (!do_pent)
+                    for (int i = 0; i < penta; ++i) H.pcuts[i].y = H.dual_gamma[triag + i];
+                if (!do_hept)
+                    for (int i = 0; i < PP_->NHeptaIneq; ++i) H.hcuts[i].y = H.dual_gamma[triag + penta + i];
+            }
             // the default engine anneals on the host from the rand() stream
             // (the reference's cuts); extra engines run the chains on the GPU
             if ((do_pent || params.include_Hepta) && E.is_default) {
@@ -408,8 +522,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             if (do_pent)
                 viol5 = E.is_default ? pent_update(H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag, E.rng)
                                      : pent_update_dev(E, H, PP_, H.dual_gamma, &pent_add, &pent_sub, triag);
-            if (params.include_Hepta &&
-                ((count > params.triag_iter + params.pent_iter) || (viol3 < 0.2 && (1 - viol5 < 0.4)))) {
+            if (do_hept) {
                 if (E.is_default)
                     hept_update(H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta, E.rng);
                 else
@@ -465,11 +578,11 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         bdl_iter += count % 2;
         bdl_iter = (bdl_iter < params.max_bundle_iter) ? bdl_iter : params.max_bundle_iter;
     }
-    if (warm_on || warm_rec) {
-        std::vector<double> fg(PP_->NIneq > 0 ? PP_->NIneq : 1);
-        if (PP_->NIneq > 0) {
-            BQB_CUDA(cudaMemcpyAsync(fg.data(), b.gam.p, (size_t)PP_->NIneq * sizeof(double), cudaMemcpyDeviceToHost,
-                                     s));
+    if (warm_on || warm_rec || pstart_on) {
+        const int mall = PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq;
+        std::vector<double> fg(mall > 0 ? mall : 1);
+        if (mall > 0) {
+            BQB_CUDA(cudaMemcpyAsync(fg.data(), b.gam.p, (size_t)mall * sizeof(double), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
         }
         if (warm_rec && !warm_first.empty())
@@ -485,6 +598,18 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             fc->key.push_back(key);
             fc->gam.push_back(fg[c]);
             fc->index[key] = fg[c];
+        }
+        if (pstart_on) {
+            for (int i = 0; i < PP_->NPentIneq; ++i) {
+                ParentKgon q{H.pcuts[i].type, {0, 0, 0, 0, 0, 0, 0}, fg[PP_->NIneq + i]};
+                for (int a = 0; a < 5; ++a) q.v[a] = orig[H.pcuts[i].permutation[a]];
+                fc->pent.push_back(q);
+            }
+            for (int i = 0; i < PP_->NHeptaIneq; ++i) {
+                ParentKgon q{H.hcuts[i].type, {0, 0, 0, 0, 0, 0, 0}, fg[PP_->NIneq + PP_->NPentIneq + i]};
+                for (int a = 0; a < 7; ++a) q.v[a] = orig[H.hcuts[i].permutation[a]];
+                fc->hept.push_back(q);
+            }
         }
         E.final_cuts = std::move(fc);
     }
@@ -513,6 +638,9 @@ BQB_API long long bqb_bundle_iterations(int reset)
 {
     return reset ? g_bundle_iters.exchange(0) : g_bundle_iters.load();
 }
+
+// Parent start on (1) or off (0, the reference's start at every node).
+BQB_API void bqb_set_parent_start(int on) { g_parent_start.store(on ? 1 : 0); }
 
 // Root effort on (1) or off (0, the reference's give-up rule at every node).
 BQB_API void bqb_set_root_effort(int full) { g_root_effort.store(full ? 1 : 0); }

@@ -61,10 +61,18 @@ struct WarmDev {
 // the multipliers they end with: what a child node inherits.  A triangle
 // keeps its orientation (i > j > k) and its type under this numbering, so
 // the same key names the same inequality in parent and child.
+// A node's final pentagonal / heptagonal cut in original vertex numbers
+// (v[0..k-1]) with its final multiplier.
+struct ParentKgon {
+    int type;
+    int v[7];
+    double gam;
+};
 struct ParentCuts {
-    std::vector<uint64_t> key;
-    std::vector<double> gam;
+    std::vector<uint64_t> key;     // triangle cuts (orig_cut_key) ...
+    std::vector<double> gam;       // ... and their final multipliers
     std::unordered_map<uint64_t, double> index;
+    std::vector<ParentKgon> pent, hept;
 };
 inline uint64_t orig_cut_key(int type, int a, int b, int c)
 {

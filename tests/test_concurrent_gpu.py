@@ -127,3 +127,31 @@ def test_parallel_solve_optimum(lib, kind, nv, seed):
     # serial one's only up to those streams, and above the optimum
     assert par["root_bound"] >= par["best_value"]
     assert abs(par["root_bound"] - serial["root_bound"]) <= 1e-3 * abs(serial["root_bound"])
+
+
+@pytest.mark.gpu
+def test_root_effort_and_parent_start(lib):
+    """Root effort (no early give-up at the root) and parent start (children
+    begin from their parent's final cuts and multipliers) change only how
+    fast the bound falls: the optimum is the serial solver's, the root bound
+    with root effort is no larger than without it for the same random
+    streams (the bundle's objective never rises, and the first rounds are
+    the same), and children keep some parent starts."""
+    A = instances.gnp_pm1(50, 0.5, 4)
+    serial = _lib.solve(A)
+    assert lib.bqb_seed_engines(2021) == 0
+    plain = _lib.solve(A, threads=8)
+    assert lib.bqb_seed_engines(2021) == 0
+    effort = _lib.solve(A, threads=8, root_effort=True)
+    assert effort["root_bound"] <= plain["root_bound"] + 1e-9 * abs(plain["root_bound"])
+    st = (C.c_longlong * 2)()
+    lib.bqb_warm_stats(st, 1)
+    assert lib.bqb_seed_engines(2021) == 0
+    ps = _lib.solve(A, threads=8, parent_start=True)
+    lib.bqb_warm_stats(st, 1)
+    lib.bqb_set_parent_start(0)
+    for r in (plain, effort, ps):
+        assert r["best_value"] == serial["best_value"]
+        assert O.evaluateSolution(O.build_SP_L(A), r["x"]) == r["best_value"]
+    if ps["nodes"] > 1:
+        assert st[0] + st[1] > 0 and st[0] > 0, list(st)
