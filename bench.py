@@ -91,7 +91,6 @@ LEG_CALLS = {
                             "value is lower)",
     "engines_learned": "the engines leg with the shipped warm-start model (children start from the parent's "
                        "multipliers where the model keeps them)",
-    "device_pool_root_effort": "bqb_solve_device with root effort (the root runs every outer round unless pruned)",
     "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
     "device_pool": "bqb_solve_device: the whole tree in one persistent launch, open-node pool on the device",
 }
@@ -453,8 +452,7 @@ def run_gpu(args):
         fused_kw = dict(fused_batch=2 * sms, fused_depth=8)
         cases = [("n100", TTO_NAME, tto_instance(),
                   [("fused", fused_kw, None), ("fused_learned", fused_kw, p_w),
-                   ("device_pool", dict(device_pool=True), None),
-                   ("device_pool_root_effort", dict(device_pool=True, root_effort=True), None)])]
+                   ("device_pool", dict(device_pool=True), None)])]
         if args.tto_torus:
             # the multi-CTA IPM's per-size schedule for the torus's sizes
             # (n = 343 and its subproblems, the same panel count)

@@ -87,13 +87,12 @@ enum CoopProf : int {
 };
 
 struct Smem {
-    double D[CB][LDS];    // panel block, then its Cholesky factor (lower)
+    double D[CB][LDS];    // the panel block
     double Li[CB][LDS];   // inverse of the factor (lower)
     double A1[CB][LDS];   // C_I, or a GEMM operand tile
     double A2[CB][LDS];   // C_J, or a GEMM operand tile
     double V1[CB][LDS];   // V_I, or a GEMM operand tile
     double V2[CB][LDS];   // V_J, or a GEMM operand tile
-    double R[CB];         // reciprocals of the factor's diagonal
     double red[CW * 4];
     double tot[4];
     int ok;
@@ -187,15 +186,21 @@ __device__ void grid_totals(const double* part, Smem& sm)
 
 // ---- the panel sweep ---------------------------------------------------------
 
-// Step Q of the register Cholesky of a 32 x 32 block held by one warp
-// (lane p holds row p in s[]): column Q of the factor, then the rank-1
-// update of the rows below.  Instantiated for every Q so that every index
-// into s[] is a constant and s[] stays in registers.  No early exit: after a
-// non-positive pivot (the same d in every lane) the steps go on with a unit
-// pivot and the caller discards the result.  Lane Q keeps the pivot's
-// reciprocal square root, the reciprocal of its diagonal entry of the factor.
+// Step Q of the register Cholesky of a 32 x 32 block held by one warp, and
+// of the inverse of its factor.  Lane p holds row p of the block in s[] and
+// row p of the inverse in li[] (initially row p of the identity).  Step Q:
+// column Q of the factor (l_pQ in lane p), the rank-1 update of the rows
+// below (the dependent chain from pivot to pivot), then row Q of the inverse
+// is final once scaled by 1 / l_QQ (the pivot's reciprocal square root) and
+// is eliminated from the rows below: li_p -= l_pQ li_Q, entries j <= Q
+// (forward substitution L Li = I, row by row).  The inverse's updates do not
+// feed the next pivot, so they fill the chain's idle issue slots.
+// Instantiated for every Q so that every index into s[] and li[] is a
+// constant and both stay in registers.  No early exit: after a non-positive
+// pivot (the same d in every lane) the steps go on with a unit pivot and the
+// caller discards the result.
 template <int Q>
-__device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd, double& rdiag)
+__device__ __forceinline__ void chol_inv_step(double (&s)[CB], double (&li)[CB], int p, int& pd)
 {
     if constexpr (Q < CB) {
         double d = __shfl_sync(0xffffffffu, s[Q], Q);
@@ -206,50 +211,29 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd, doubl
         const double rs = rsqrt(d);   // one reciprocal square root per pivot
         const double l = d * rs;
         const double lpq = p == Q ? l : s[Q] * rs;
-        if (p == Q) rdiag = rs;
         s[Q] = lpq;
 #pragma unroll
         for (int r = Q + 1; r < CB; ++r) {
             const double lrq = __shfl_sync(0xffffffffu, lpq, r);
-            // lane r's own entry l_rq is lpq: its diagonal update (the next
-            // pivot, for r = Q + 1) does not wait for the shuffle
-            if (r < p) s[r] = fma(-lpq, lrq, s[r]);
-            else if (r == p) s[r] = fma(-lpq, lpq, s[r]);
+            if (r <= p) s[r] = fma(-lpq, lrq, s[r]);
         }
-        chol_step<Q + 1>(s, p, pd, rdiag);
+        if (p == Q) {
+#pragma unroll
+            for (int j = 0; j <= Q; ++j) li[j] *= rs;
+        }
+#pragma unroll
+        for (int j = 0; j <= Q; ++j) {
+            const double v = __shfl_sync(0xffffffffu, li[j], Q);
+            if (p > Q) li[j] = fma(-lpq, v, li[j]);
+        }
+        chol_inv_step<Q + 1>(s, li, p, pd);
     }
 }
 
-// Step I of the inverse of the lower factor for the calling lane's column t:
-// li[I] = (delta_It - sum_{k < I} D[I][k] li[k]) / D[I][I] (zero above the
-// diagonal, where every term is zero).  Instantiated for every I so that li[]
-// stays in registers; the D entries are shared-memory broadcasts that do not
-// depend on the chain.  The sum runs in four interleaved partial sums, so
-// the dependent chain per step is a quarter as long.
-template <int I>
-__device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int t)
-{
-    if constexpr (I < CB) {
-        double a0 = I == t ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll
-        for (int k = 0; k + 3 < I; k += 4) {
-            a0 = fma(-sm.D[I][k], li[k], a0);
-            a1 = fma(-sm.D[I][k + 1], li[k + 1], a1);
-            a2 = fma(-sm.D[I][k + 2], li[k + 2], a2);
-            a3 = fma(-sm.D[I][k + 3], li[k + 3], a3);
-        }
-#pragma unroll
-        for (int k = I & ~3; k < I; ++k) a0 = fma(-sm.D[I][k], li[k], a0);
-        li[I] = ((a0 + a1) + (a2 + a3)) * sm.R[I];
-        linv_step<I + 1>(li, sm, t);
-    }
-}
-
-// Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
-// in shared memory.  Warp 0 factors in registers (lane p holds row p; the
-// block is padded to 32 x 32 with the identity), then lane t forms column t
-// of Li by forward substitution.  Returns false (in every thread) on a
-// non-positive pivot.
+// Every CTA: the inverse Li = Ld^{-1} of the Cholesky factor of
+// D = A[K, K] (b x b) in shared memory.  Warp 0 factors and inverts in
+// registers (the block padded to 32 x 32 with the identity).  Returns false
+// (in every thread) on a non-positive pivot.
 __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, unsigned long long* load_ns)
 {
     const int tid = threadIdx.x;
@@ -262,24 +246,18 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, un
     if (load_ns) *load_ns += global_ns() - t0;
     if (tid < 32) {
         const int p = tid;
-        double s[CB];
+        double s[CB], li[CB];
 #pragma unroll
-        for (int r = 0; r < CB; ++r) s[r] = sm.D[p][r];
+        for (int r = 0; r < CB; ++r) {
+            s[r] = sm.D[p][r];
+            li[r] = r == p ? 1.0 : 0.0;
+        }
         int pd = 1;
-        double rdiag = 1.0;
-        chol_step<0>(s, p, pd, rdiag);
+        chol_inv_step<0>(s, li, p, pd);
         if (p == 0) sm.pd = pd;
         if (pd) {
 #pragma unroll
-            for (int r = 0; r < CB; ++r) sm.D[p][r] = r <= p ? s[r] : 0.0;
-            sm.R[p] = rdiag;
-        }
-        __syncwarp();
-        if (pd) {
-            double li[CB];
-            linv_step<0>(li, sm, p);
-#pragma unroll
-            for (int i = 0; i < CB; ++i) sm.Li[i][p] = li[i];
+            for (int j = 0; j < CB; ++j) sm.Li[p][j] = j <= p ? li[j] : 0.0;
         }
     }
     __syncthreads();
