@@ -253,8 +253,12 @@ def test_parent_cuts_reach_children(lib):
     cuts, so some recorded first-list cuts carry the parent's multiplier
     (feature 13 = 1), and the parent cuts the child's own separation did not
     find join the list as candidates (their violation is evaluated at the
-    child's X).  Targets are the multipliers the cuts end with (>= 0)."""
-    feats, targets = warm.record_pairs_bab(lib, [(60, 911)], threads=4, time_limit=60)
+    child's X).  Targets are the multipliers the cuts end with (>= 0).
+    The instance's tree has dozens of nodes (39 in the reference's serial
+    B&B), so children that run the cutting-plane loop exist whatever the
+    engines' random streams do."""
+    assert lib.bqb_seed_engines(2021) == 0
+    feats, targets = warm.record_pairs_bab(lib, [(80, 913)], threads=4, time_limit=60)
     assert len(targets) > 0 and feats.shape == (len(targets), W.F)
     assert np.all(np.isfinite(feats)) and np.all(targets >= 0)
     with_parent = feats[:, 13] > 0.5
