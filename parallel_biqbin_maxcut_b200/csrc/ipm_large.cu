@@ -56,6 +56,7 @@ constexpr int CB = 32;          // panel and tile width
 constexpr int CT = 256;         // threads per CTA
 constexpr int CW = CT / 32;     // warps per CTA
 constexpr int LDS = CB + 1;     // padded shared-memory row
+static_assert(CT == CW * 32 && CB == 32 && 4 * CW == CB, "a CTA's threads cover a tile as 32 rows x 8 columns, 4 times");
 constexpr unsigned long long BAR_TIMEOUT_NS = 2000000000ull;
 
 struct CoopArgs {
@@ -87,12 +88,15 @@ enum CoopProf : int {
 };
 
 struct Smem {
+    double Lc[CB][CB];    // the panel's factor by columns (row Q = column Q)
+    double Lr[CB][CB + 2];   // the panel's factor by rows (rows 16-byte aligned)
     double D[CB][LDS];    // the panel block
     double Li[CB][LDS];   // inverse of the factor (lower)
     double A1[CB][LDS];   // C_I, or a GEMM operand tile
     double A2[CB][LDS];   // C_J, or a GEMM operand tile
     double V1[CB][LDS];   // V_I, or a GEMM operand tile
     double V2[CB][LDS];   // V_J, or a GEMM operand tile
+    double R[CB];         // reciprocals of the factor's diagonal
     double red[CW * 4];
     double tot[4];
     int ok;
@@ -186,21 +190,18 @@ __device__ void grid_totals(const double* part, Smem& sm)
 
 // ---- the panel sweep ---------------------------------------------------------
 
-// Step Q of the register Cholesky of a 32 x 32 block held by one warp, and
-// of the inverse of its factor.  Lane p holds row p of the block in s[] and
-// row p of the inverse in li[] (initially row p of the identity).  Step Q:
-// column Q of the factor (l_pQ in lane p), the rank-1 update of the rows
-// below (the dependent chain from pivot to pivot), then row Q of the inverse
-// is final once scaled by 1 / l_QQ (the pivot's reciprocal square root) and
-// is eliminated from the rows below: li_p -= l_pQ li_Q, entries j <= Q
-// (forward substitution L Li = I, row by row).  The inverse's updates do not
-// feed the next pivot, so they fill the chain's idle issue slots.
-// Instantiated for every Q so that every index into s[] and li[] is a
-// constant and both stay in registers.  No early exit: after a non-positive
-// pivot (the same d in every lane) the steps go on with a unit pivot and the
-// caller discards the result.
+// Step Q of the register Cholesky of a 32 x 32 block held by one warp
+// (lane p holds row p in s[]): column Q of the factor, then the rank-1
+// update of the rows below.  The column goes to the warp through shared
+// memory (one store per lane, then broadcast reads of two entries at a
+// time), which costs fewer issue slots than a shuffle per entry.
+// Instantiated for every Q so that every index into s[] is a constant and
+// s[] stays in registers.  No early exit: after a non-positive pivot (the
+// same d in every lane) the steps go on with a unit pivot and the caller
+// discards the result.  Lane Q keeps the pivot's reciprocal square root, the
+// reciprocal of its diagonal entry of the factor.
 template <int Q>
-__device__ __forceinline__ void chol_inv_step(double (&s)[CB], double (&li)[CB], int p, int& pd)
+__device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd, double& rdiag, double (*Lc)[CB])
 {
     if constexpr (Q < CB) {
         double d = __shfl_sync(0xffffffffu, s[Q], Q);
@@ -208,32 +209,57 @@ __device__ __forceinline__ void chol_inv_step(double (&s)[CB], double (&li)[CB],
             pd = 0;
             d = 1.0;
         }
-        const double rs = rsqrt(d);   // one reciprocal square root per pivot
+        const double rs = rsqrt(d);
         const double l = d * rs;
         const double lpq = p == Q ? l : s[Q] * rs;
+        if (p == Q) rdiag = rs;
         s[Q] = lpq;
+        Lc[Q][p] = lpq;
+        __syncwarp();
+        constexpr int r0 = (Q + 1) & ~1;
 #pragma unroll
-        for (int r = Q + 1; r < CB; ++r) {
-            const double lrq = __shfl_sync(0xffffffffu, lpq, r);
-            if (r <= p) s[r] = fma(-lpq, lrq, s[r]);
+        for (int r = r0; r < CB; r += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(&Lc[Q][r]);
+            if (r > Q && r <= p) s[r] = fma(-lpq, v.x, s[r]);
+            if (r + 1 <= p) s[r + 1] = fma(-lpq, v.y, s[r + 1]);
         }
-        if (p == Q) {
-#pragma unroll
-            for (int j = 0; j <= Q; ++j) li[j] *= rs;
-        }
-#pragma unroll
-        for (int j = 0; j <= Q; ++j) {
-            const double v = __shfl_sync(0xffffffffu, li[j], Q);
-            if (p > Q) li[j] = fma(-lpq, v, li[j]);
-        }
-        chol_inv_step<Q + 1>(s, li, p, pd);
+        chol_step<Q + 1>(s, p, pd, rdiag, Lc);
     }
 }
 
-// Every CTA: the inverse Li = Ld^{-1} of the Cholesky factor of
-// D = A[K, K] (b x b) in shared memory.  Warp 0 factors and inverts in
-// registers (the block padded to 32 x 32 with the identity).  Returns false
-// (in every thread) on a non-positive pivot.
+// Step I of the inverse of the lower factor for the calling lane's column t:
+// li[I] = (delta_It - sum_{k < I} Lr[I][k] li[k]) / Lr[I][I] (zero above the
+// diagonal, where every term is zero).  Instantiated for every I so that li[]
+// stays in registers; the factor's entries are shared-memory broadcasts read
+// two at a time that do not depend on the chain.  The sum runs in four
+// interleaved partial sums, so the dependent chain per step is a quarter as
+// long.
+template <int I>
+__device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int t)
+{
+    if constexpr (I < CB) {
+        double a0 = I == t ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+        for (int k = 0; k + 3 < I; k += 4) {
+            const double2 u = *reinterpret_cast<const double2*>(&sm.Lr[I][k]);
+            const double2 w = *reinterpret_cast<const double2*>(&sm.Lr[I][k + 2]);
+            a0 = fma(-u.x, li[k], a0);
+            a1 = fma(-u.y, li[k + 1], a1);
+            a2 = fma(-w.x, li[k + 2], a2);
+            a3 = fma(-w.y, li[k + 3], a3);
+        }
+#pragma unroll
+        for (int k = I & ~3; k < I; ++k) a0 = fma(-sm.Lr[I][k], li[k], a0);
+        li[I] = ((a0 + a1) + (a2 + a3)) * sm.R[I];
+        linv_step<I + 1>(li, sm, t);
+    }
+}
+
+// Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
+// in shared memory.  Warp 0 factors in registers (lane p holds row p; the
+// block is padded to 32 x 32 with the identity), then lane t forms column t
+// of Li by forward substitution.  Returns false (in every thread) on a
+// non-positive pivot.
 __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, unsigned long long* load_ns)
 {
     const int tid = threadIdx.x;
@@ -246,18 +272,25 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, un
     if (load_ns) *load_ns += global_ns() - t0;
     if (tid < 32) {
         const int p = tid;
-        double s[CB], li[CB];
+        double s[CB];
 #pragma unroll
-        for (int r = 0; r < CB; ++r) {
-            s[r] = sm.D[p][r];
-            li[r] = r == p ? 1.0 : 0.0;
-        }
+        for (int r = 0; r < CB; ++r) s[r] = sm.D[p][r];
         int pd = 1;
-        chol_inv_step<0>(s, li, p, pd);
+        double rdiag = 1.0;
+        chol_step<0>(s, p, pd, rdiag, sm.Lc);
         if (p == 0) sm.pd = pd;
         if (pd) {
 #pragma unroll
-            for (int j = 0; j < CB; ++j) sm.Li[p][j] = j <= p ? li[j] : 0.0;
+            for (int r = 0; r < CB; r += 2)
+                *reinterpret_cast<double2*>(&sm.Lr[p][r]) = make_double2(r <= p ? s[r] : 0.0, r + 1 <= p ? s[r + 1] : 0.0);
+            sm.R[p] = rdiag;
+        }
+        __syncwarp();
+        if (pd) {
+            double li[CB];
+            linv_step<0>(li, sm, p);
+#pragma unroll
+            for (int i = 0; i < CB; ++i) sm.Li[i][p] = li[i];
         }
     }
     __syncthreads();
@@ -267,8 +300,9 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, un
 // C rows of tile block I (32 x b): the panel columns of A for rows I, or, for
 // the row block of the previous panel (whose entries still wait for their
 // fix), W_{K-1} transposed.  Then V = C Ld^{-T}: V(r, q) = sum_{p <= q}
-// C(r, p) Li(q, p).
-__device__ void load_v(const double* A, int n, int I, int k0, int b, const double* Wprev, bool from_w,
+// C(r, p) Li(q, p).  Not inlined: its registers are then allocated apart
+// from the panel factorisation's, and the kernel needs no spill slots.
+__device__ __noinline__ void load_v(const double* A, int n, int I, int k0, int b, const double* Wprev, bool from_w,
                        double (*Cs)[LDS], double (*Vs)[LDS], Smem& sm)
 {
     const int i0 = I * CB;
@@ -280,11 +314,19 @@ __device__ void load_v(const double* A, int n, int I, int k0, int b, const doubl
         Cs[r][p] = v;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < CB * CB; e += CT) {
-        const int r = e % CB, q = e / CB;
-        double v = 0.0;
-        for (int p = 0; p <= q; ++p) v = fma(Cs[r][p], sm.Li[q][p], v);
-        Vs[r][q] = q < b ? v : 0.0;
+    // thread (r, c0) forms V(r, c0 + 8 j), j = 0..3, reading C(r, p) once for
+    // all four; Li(q, p) = 0 for p > q, so running p to the largest q adds
+    // exact zeros to the smaller ones
+    {
+        const int r = threadIdx.x % CB, c0 = threadIdx.x / CB;
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int p = 0; p <= c0 + 3 * CW; ++p) {
+            const double cp = Cs[r][p];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = fma(cp, sm.Li[c0 + CW * j][p], v[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) Vs[r][c0 + CW * j] = c0 + CW * j < b ? v[j] : 0.0;
     }
     __syncthreads();
 }
@@ -307,9 +349,20 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
     }
     double (*VJ)[LDS] = J != I ? sm.V2 : sm.V1;
     const int i0 = I * CB, j0 = J * CB, kp0 = (K - 1) * CB;
+    // thread (r, c0) owns the entries (r, c0 + 8 j), j = 0..3, of the tile
+    // and reads V1(r, q) once for all four
+    const int r = threadIdx.x % CB, c0 = threadIdx.x / CB;
     if (upd || fixI || fixJ) {
-        for (int e = threadIdx.x; e < CB * CB; e += CT) {
-            const int r = e % CB, c = e / CB;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (upd)
+            for (int q = 0; q < b; ++q) {
+                const double a = sm.V1[r][q];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) acc[jj] = fma(a, VJ[c0 + CW * jj][q], acc[jj]);
+            }
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int c = c0 + CW * jj;
             const int i = i0 + r, j = j0 + c;
             if (i >= n || j >= n) continue;
             double v;
@@ -317,23 +370,24 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
             else if (fixJ) v = Wprev[i + (size_t)(j - kp0) * n];
             else if (fixI) v = Wprev[j + (size_t)(i - kp0) * n];
             else v = A[i + (size_t)j * n];
-            if (upd) {
-                double acc = 0.0;
-                for (int q = 0; q < b; ++q) acc = fma(sm.V1[r][q], VJ[c][q], acc);
-                v -= acc;
-            }
+            if (upd) v -= acc[jj];
             A[i + (size_t)j * n] = v;
         }
     }
     if (FULL && upd && I == J) {
-        // W_K(i, q) = sum_{p >= q} V(i, p) Li(p, q)
-        for (int e = threadIdx.x; e < CB * CB; e += CT) {
-            const int r = e % CB, q = e / CB;
-            const int i = i0 + r;
-            if (i >= n || q >= b) continue;
-            double w = 0.0;
-            for (int p = q; p < b; ++p) w = fma(sm.V1[r][p], sm.Li[p][q], w);
-            Wcur[i + (size_t)q * n] = w;
+        // W_K(i, q) = sum_{p >= q} V(i, p) Li(p, q); Li(p, q) = 0 for p < q,
+        // so starting p at the smallest q adds exact zeros to the others
+        double w[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int p = c0; p < b; ++p) {
+            const double vp = sm.V1[r][p];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) w[jj] = fma(vp, sm.Li[p][c0 + CW * jj], w[jj]);
+        }
+        const int i = i0 + r;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const int q = c0 + CW * jj;
+            if (i < n && q < b) Wcur[i + (size_t)q * n] = w[jj];
         }
     }
     if (FULL && I == K && J == K) {
