@@ -385,6 +385,15 @@ void bqb_fused_profile(double *out);
 /* Calls per phase of the fused kernel since the last reset, the phases of
  * bqb_fused_profile (out[11]; out[2] = heuristic runs). */
 void bqb_fused_phase_calls(long long *out);
+/* Seconds per phase of SDPbound on the engines (bqb_bound_nodes, the
+ * parallel and serial solvers, the drop-in), summed over engines and calls
+ * since the last reset: out[9] = {IPM, lambda_eta, L - B^T(gamma), op_B of
+ * the new bundle element + bundle step, heuristic, triangle separation,
+ * pentagonal / heptagonal separation, cut upload and the rest, whole
+ * calls}.  Off by default; with it on every phase boundary synchronises
+ * the engine's stream.  For profiling; no reference counterpart. */
+void bqb_engine_profile_enable(int on);
+void bqb_engine_profile(double *out, int reset);
 /* Device milliseconds each node of the last bqb_bound_nodes_fused call took
  * (node order of that call); writes at most `count`, returns how many. */
 int bqb_fused_node_times(double *out, int count);

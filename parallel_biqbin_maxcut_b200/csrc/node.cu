@@ -64,6 +64,59 @@ std::mutex g_trace_mu;
 std::vector<double> g_trace;
 std::atomic<long long> g_trace_node{0};
 
+// Time by phase of sdp_bound on every engine (off by default; for
+// profiling).  With it on, each phase boundary synchronises the engine's
+// stream and adds the host time since the previous boundary to the phase
+// that ended, so the parts sum to the bounding time (the synchronisations
+// make it a little slower than without).
+enum EngPhase : int {
+    EP_IPM,          // the IPM calls (basic bound, fct_eval's, proposals)
+    EP_LAMBDA,       // lambda_eta
+    EP_OPBT,         // L0 = L - B^T(gamma)
+    EP_BUNDLE,       // op_B of the new element, the bundle step and X combination
+    EP_HEUR,         // the heuristic
+    EP_TRI,          // triangle separation and cut-list update
+    EP_KGON,         // pentagonal and heptagonal separation (X copy included)
+    EP_REBUILD,      // cut upload, subgradient rebuild, state reads
+    EP_TOTAL,        // whole sdp_bound calls
+    EP_WORDS
+};
+std::atomic<int> g_eprof_on{0};
+std::atomic<long long> g_eprof_ns[EP_WORDS];
+
+struct PhaseClock {
+    cudaStream_t s;
+    bool on;
+    std::chrono::steady_clock::time_point t;
+    explicit PhaseClock(cudaStream_t st) : s(st), on(g_eprof_on.load() != 0), t(std::chrono::steady_clock::now()) {}
+    void mark(int phase)
+    {
+        if (!on) return;
+        BQB_CUDA(cudaStreamSynchronize(s));
+        const auto now = std::chrono::steady_clock::now();
+        g_eprof_ns[phase].fetch_add(std::chrono::duration_cast<std::chrono::nanoseconds>(now - t).count());
+        t = now;
+    }
+    // restart the clock without charging the time since the last boundary
+    void skip()
+    {
+        if (on) t = std::chrono::steady_clock::now();
+    }
+};
+
+// Adds a whole call's time on return (with profiling on).
+struct CallClock {
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    CallClock() : on(g_eprof_on.load() != 0), t0(std::chrono::steady_clock::now()) {}
+    ~CallClock()
+    {
+        if (on)
+            g_eprof_ns[EP_TOTAL].fetch_add(
+                std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
 void upload_cuts(Engine& E, const HostState& H, const Problem* P)
 {
     std::vector<CutRec> rec = pack_cuts(H.cuts, P->NIneq, H.pcuts, P->NPentIneq, H.hcuts, P->NHeptaIneq);
@@ -115,17 +168,24 @@ double bundle_iterations(Engine& E, int bdl_iter, double* t)
     nd.hs.p[0] = *t;
     BQB_CUDA(cudaMemcpyAsync(b.dstate.p + BD_T, nd.hs.p, sizeof(double), cudaMemcpyHostToDevice, s));
     g_bundle_iters.fetch_add(bdl_iter);
+    PhaseClock pc(s);
+    pc.mark(EP_REBUILD);
     for (int it = 0; it < bdl_iter; ++it) {
         lambda_eta_launch(b, nullptr, s);
+        pc.mark(EP_LAMBDA);
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, nd.L.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
         if (nd.cuts.m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gtest.p, s);
+        pc.mark(EP_OPBT);
         ipm_device(E.ipm_ws, nd.L0.p, b.Xb.p, n, nd.out.p, s, b.istate.p + BI_NEXT);
+        pc.mark(EP_IPM);
         if (nd.cuts.m > 0)
             opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
         bundle_step_launch(b, nd.out.p, nd.L.p, s);
         bundle_xcomb_launch(b, nd.X.p, s);
+        pc.mark(EP_BUNDLE);
     }
     fetch_state(nd, s);
+    pc.mark(EP_REBUILD);
     *t = nd.hs.p[BD_T];
     return nd.hs.p[BD_F];
 }
@@ -137,6 +197,8 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     NodeDev& nd = E.nd;
     HostState H = E.host();
     const int n = PP_->n;
+    CallClock call_clock;
+    PhaseClock pc(s);
     E.final_cuts.reset();
     const int N0 = SP_->n;
     const int NB = N0 - 1;   // BabPbSize
@@ -174,6 +236,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     };
     std::vector<double> hostL;
     auto heuristic = [&]() {
+        pc.mark(EP_REBUILD);
         for (int i = 0; i < NB; ++i) x[i] = node->xfixed[i] ? node->sol.X[i] : 0;
         g_heuristic_runs.fetch_add(1);
         bqb_heuristic_fn hook = g_heuristic_hook.load();
@@ -191,6 +254,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
                              E.is_default ? 0 : gw_hyperplanes());
         }
         updateSolution(x.data());
+        pc.mark(EP_HEUR);
     };
 
     int bdl_iter = params.init_bundle_iter;
@@ -203,9 +267,11 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     double& f = *H.f;
 
     // basic SDP relaxation
+    pc.mark(EP_REBUILD);
     ipm_device(E.ipm_ws, dL, dX, n, dout, s);
     BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaStreamSynchronize(s));
+    pc.mark(EP_IPM);
     check_ipm_status_host(nd.hs.p);
     f = nd.hs.p[0];
     const double basic_bound = f + fixedvalue;
@@ -216,7 +282,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     if (bound < Bab_LBGet() + 1.0) return bound;
     if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) return bound;
 
+    pc.mark(EP_REBUILD);
     viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
+    pc.mark(EP_TRI);
     // No violated triangle inequality (X is a cut matrix up to the
     // tolerance): the bundle would start from t = .../0 with no cuts, where
     // the reference's BLAS calls reject m = 0 (src/bounding.c:122-131,
@@ -328,9 +396,11 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
         opBt_launch(nd.cuts, nd.L0.p, n, E.warm.gam.p, s);
         double* Xw = E.warm.X.ensure(nn);
+        pc.mark(EP_REBUILD);
         ipm_device(E.ipm_ws, nd.L0.p, Xw, n, dout, s);
         BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
         BQB_CUDA(cudaStreamSynchronize(s));
+        pc.mark(EP_IPM);
         double fw = nd.hs.p[0];
         for (int i = 0; i < m; ++i) fw += prop[i];
         const bool keep = (int)nd.hs.p[2] == IPM_OK && fw < f;
@@ -420,9 +490,11 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
             opBt_launch(nd.cuts, nd.L0.p, n, gp, s);
             double* Xw = E.warm.X.ensure(nn);
+            pc.mark(EP_REBUILD);
             ipm_device(E.ipm_ws, nd.L0.p, Xw, n, dout, s);
             BQB_CUDA(cudaMemcpyAsync(nd.hs.p, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
+            pc.mark(EP_IPM);
             double fw = nd.hs.p[0];
             for (int i = 0; i < mt; ++i) fw += prop[i];
             const bool keep = (int)nd.hs.p[2] == IPM_OK && fw < f;
@@ -479,7 +551,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     while (!done) {
         ++count;
         const double oldf = f;
+        pc.mark(EP_REBUILD);
         f = bundle_iterations(E, bdl_iter, &t);
+        pc.skip();
         bound = f + fixedvalue;
         prune = bound < Bab_LBGet() + 1.0;
         if (!prune) {
@@ -501,7 +575,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             const int m = PP_->NIneq + PP_->NPentIneq + PP_->NHeptaIneq;
             BQB_CUDA(cudaMemcpyAsync(H.dual_gamma, b.gam.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
+            pc.mark(EP_REBUILD);
             viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
+            pc.mark(EP_TRI);
             const bool do_pent = params.include_Pent && (count > params.triag_iter || viol3 < 0.2);
             const bool do_hept = params.include_Hepta && ((count > params.triag_iter + params.pent_iter) ||
                                                           (viol3 < 0.2 && (1 - viol5 < 0.4)));
@@ -528,6 +604,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
                 else
                     hept_update_dev(E, H, PP_, H.dual_gamma, &hept_add, &hept_sub, triag + penta);
             }
+            pc.mark(EP_KGON);
         } else {
             tri_add = tri_sub = pent_add = pent_sub = hept_add = hept_sub = 0;
         }
@@ -562,7 +639,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             // fct_eval(PP, dual_gamma, X_test, g) into the free slot
             BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
             if (m > 0) opBt_launch(nd.cuts, nd.L0.p, n, b.gam.p, s);
+            pc.mark(EP_REBUILD);
             ipm_device(E.ipm_ws, nd.L0.p, b.Xb.p, n, dout, s, b.istate.p + BI_NEXT);
+            pc.mark(EP_IPM);
             // G(:, i) = 1 - B(X_bundle(i)) for the bundle, then g for the new element
             opB_launch(nd.cuts, b.Xb.p, nn, b.slot.p, k, n, b.G.p, b.ldg, true, s);
             opB_launch(nd.cuts, b.Xb.p, nn, b.istate.p + BI_NEXT, 1, n, b.G.p, b.ldg, true, s);
@@ -615,6 +694,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     }
     bound = f + fixedvalue;
     if (rank == 0) diff = basic_bound - bound;
+    pc.mark(EP_REBUILD);
     return bound;
 }
 
@@ -637,6 +717,21 @@ BQB_API long long bqb_heuristic_runs(int reset)
 BQB_API long long bqb_bundle_iterations(int reset)
 {
     return reset ? g_bundle_iters.exchange(0) : g_bundle_iters.load();
+}
+
+// Time by phase of the engines' SDPbound (seconds, summed over engines and
+// calls): out[9] = {IPM, lambda_eta, L - B^T(gamma), op_B + bundle step,
+// heuristic, triangle separation, pentagonal / heptagonal separation, cut
+// upload and the rest, whole calls}.  Profiling only: with it on, every
+// phase boundary synchronises the engine's stream.  reset != 0 zeroes the
+// sums after reading.  No reference counterpart.
+BQB_API void bqb_engine_profile_enable(int on) { g_eprof_on.store(on ? 1 : 0); }
+BQB_API void bqb_engine_profile(double* out, int reset)
+{
+    for (int i = 0; i < EP_WORDS; ++i) {
+        const long long v = reset ? g_eprof_ns[i].exchange(0) : g_eprof_ns[i].load();
+        if (out) out[i] = 1e-9 * (double)v;
+    }
 }
 
 // Parent start on (1) or off (0, the reference's start at every node).
