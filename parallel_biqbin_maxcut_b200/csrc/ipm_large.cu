@@ -405,12 +405,13 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
 // The panel sweep of A (n x n).  FULL: A becomes inv(A); otherwise only the
 // trailing updates run, for the pivots.  With Xm (FULL only), the final
 // phase also writes Mout = Fout = inv(A) .* Xm for its tiles (the next
-// inverse's input), saving a phase.  Returns 1 (positive definite), 0 (a
-// non-positive pivot; every CTA returns 0 at the same panel) or -1 (a
-// barrier gave up).
+// inverse's input), saving a phase; with dXm as well, Xm + ap dXm (rounded
+// as the step's update rounds it) takes the place of Xm.  Returns 1
+// (positive definite), 0 (a non-positive pivot; every CTA returns 0 at the
+// same panel) or -1 (a barrier gave up).
 template <bool FULL>
 __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = nullptr, double* Mout = nullptr,
-                     double* Fout = nullptr)
+                     double* Fout = nullptr, const double* dXm = nullptr, double ap = 0.0)
 {
     const int n = a.n;
     const int T = (n + CB - 1) / CB;
@@ -458,7 +459,8 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
                 const size_t ij = i + (size_t)j * n;
                 A[ij] = -v;
                 if (Xm) {
-                    const double m = -v * Xm[ij];
+                    const double xm = dXm ? fma(ap, dXm[ij], Xm[ij]) : Xm[ij];
+                    const double m = -v * xm;
                     Mout[ij] = m;
                     Fout[ij] = m;
                 }
@@ -605,13 +607,13 @@ __device__ void warp_rows_rhs(const double* Zi, const double* dX1, const double*
 
 // x = M^{-1} b (b null: -e): x = F b, then one refinement step.  Three
 // phases; returns false when a barrier gave up.
-__device__ bool solve(const CoopArgs& a, const double* b, double* x, Smem& sm)
+__device__ bool solve(const CoopArgs& a, const double* F, const double* b, double* x, Smem& sm)
 {
-    warp_rows_matvec(a.F, a.n, b, x);
+    warp_rows_matvec(F, a.n, b, x);
     if (!grid_sync(a.bar, sm, a.prof)) return false;
     warp_rows_resid(a.M, a.n, b, x, a.r);
     if (!grid_sync(a.bar, sm, a.prof)) return false;
-    warp_rows_refine(a.F, a.n, a.r, a.t, x);
+    warp_rows_refine(F, a.n, a.r, a.t, x);
     return grid_sync(a.bar, sm, a.prof);
 }
 
@@ -652,30 +654,42 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
     double phi = sm.tot[2];
     double gap = fabs(phi - psi);
     int iter = 0, ls_total = 0, status = IPM_OK;
+    // Zi and F trade buffers: the dual line search sweeps its trials in
+    // full, alternating between the two, so a first trial that passes leaves
+    // inv(Z) of the new point (the same matrix, with the same arithmetic, as
+    // the sweep of the next iteration would) and M = F = inv(Z) .* X of the
+    // new X in the other buffer.
+    double* Zi = a.Zi;
+    double* F = a.F;
+    bool have_zi = false;
 
     while (alive && gap > 1e-2) {
         if (++iter > IPM_MAX_ITERS) {
             status = IPM_MAXITER;
             break;
         }
-        // Zi = inv(Z), Z = Diag(zd) - L off the diagonal
-        for (size_t e = gtid; e < nn; e += gstride) {
-            const int i = (int)(e % n), j = (int)(e / n);
-            a.Zi[e] = i == j ? a.zd[i] : -L[e];
+        int pd = 1;
+        if (!have_zi) {
+            // Zi = inv(Z), Z = Diag(zd) - L off the diagonal
+            for (size_t e = gtid; e < nn; e += gstride) {
+                const int i = (int)(e % n), j = (int)(e / n);
+                Zi[e] = i == j ? a.zd[i] : -L[e];
+            }
+            if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
+            // (its last phase also writes M = Zi .* X and F = M)
+            pd = sweep<true>(Zi, a, sm, X, a.M, F);
+            if (pd < 0) {
+                alive = false;
+                break;
+            }
+            if (!pd) {
+                status = IPM_Z_NOT_PD;
+                break;
+            }
         }
-        if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-        // (its last phase also writes M = Zi .* X and F = M)
-        int pd = sweep<true>(a.Zi, a, sm, X, a.M, a.F);
-        if (pd < 0) {
-            alive = false;
-            break;
-        }
-        if (!pd) {
-            status = IPM_Z_NOT_PD;
-            break;
-        }
+        have_zi = false;
         // F = inv(M); dy1 = F (-e)
-        pd = sweep<true>(a.F, a, sm);
+        pd = sweep<true>(F, a, sm);
         if (pd < 0) {
             alive = false;
             break;
@@ -684,20 +698,20 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             status = IPM_M_NOT_PD;
             break;
         }
-        if (!(alive = solve(a, nullptr, a.dy1, sm))) break;
+        if (!(alive = solve(a, F, nullptr, a.dy1, sm))) break;
         // dX1 = sym(Zi (-Diag(dy1) X) - X)
         unsigned long long tg = a.prof && blockIdx.x == 0 ? global_ns() : 0ull;
-        gemm_sym(a.Zi, a.dy1, X, nullptr, nullptr, -1.0, X, 0.0, nullptr, n, a.dX1, sm);
+        gemm_sym(Zi, a.dy1, X, nullptr, nullptr, -1.0, X, 0.0, nullptr, n, a.dX1, sm);
         if (a.prof) __syncthreads();
         if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_GEMM] += global_ns() - tg;
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         // corrector: rhs = mu diag(Zi) - (Zi .* dX1) dy1; dy2 = F rhs
-        warp_rows_rhs(a.Zi, a.dX1, a.dy1, mu, n, a.dy);
+        warp_rows_rhs(Zi, a.dX1, a.dy1, mu, n, a.dy);
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-        if (!(alive = solve(a, a.dy, a.dy2, sm))) break;
+        if (!(alive = solve(a, F, a.dy, a.dy2, sm))) break;
         // dX = sym(Zi (-Diag(dy2) X - Diag(dy1) dX1) + mu Zi + dX1)
         tg = a.prof && blockIdx.x == 0 ? global_ns() : 0ull;
-        gemm_sym(a.Zi, a.dy2, X, a.dy1, a.dX1, 1.0, a.dX1, mu, a.Zi, n, a.dX, sm);
+        gemm_sym(Zi, a.dy2, X, a.dy1, a.dX1, 1.0, a.dX1, mu, Zi, n, a.dX, sm);
         if (a.prof) __syncthreads();
         if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_GEMM] += global_ns() - tg;
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
@@ -734,24 +748,44 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             break;
         }
         if (ap < 1.0) ap *= 0.95;
-        // dual line search: Z + ad Diag(dy) positive definite
+        // dual line search: Z + ad Diag(dy) positive definite.  The trials
+        // are full sweeps (the same pivots as the trailing ones), alternating
+        // between Zi and F, both free by now (the primal trials used T and
+        // T2, so no CTA still reads these); the final phase of the one that
+        // passes forms M = F = inv(Z + ad Diag(dy)) .* (X + ap dX) in the
+        // other buffer.  When the first trial (ad = 1, the step itself)
+        // passes, the next iteration starts from these.
         double ad = 1.0;
         trials = 0;
         ok = false;
+        int dt = 0;
         while (true) {
-            double* Tt = (tr++ & 1) ? a.T2 : a.T;
+            double* Tt = (dt & 1) ? F : Zi;
+            double* Fo = (dt & 1) ? Zi : F;
+            ++dt;
             for (size_t e = gtid; e < nn; e += gstride) {
                 const int i = (int)(e % n), j = (int)(e / n);
                 Tt[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
             }
             if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-            pd = sweep<false>(Tt, a, sm);
+            // (only the first trial can be the step: later ones test the
+            // pivots alone)
+            pd = trials == 0 ? sweep<true>(Tt, a, sm, X, a.M, Fo, a.dX, ap) : sweep<false>(Tt, a, sm);
             if (pd < 0) {
                 alive = false;
                 break;
             }
             if (pd) {
                 ok = true;
+                // the step is the trial's only when the first trial passed
+                // (after a failed trial it is 0.95 ad, another point)
+                if (trials == 0) {
+                    if (Tt != Zi) {
+                        F = Zi;
+                        Zi = Tt;
+                    }
+                    have_zi = true;
+                }
                 break;
             }
             if (++trials >= IPM_MAX_TRIALS) break;
