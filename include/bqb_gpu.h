@@ -394,6 +394,11 @@ void bqb_fused_phase_calls(long long *out);
  * the engine's stream.  For profiling; no reference counterpart. */
 void bqb_engine_profile_enable(int on);
 void bqb_engine_profile(double *out, int reset);
+/* With the engines' profile on: out[6] = {lambda_eta calls, rounds of its
+ * lambda / eta alternation, sum of the bundle sizes, SM cycles in the QP,
+ * SM cycles in the calls, sum of the cut counts}.  No reference
+ * counterpart. */
+void bqb_lambda_eta_profile(double *out, int reset);
 /* Device milliseconds each node of the last bqb_bound_nodes_fused call took
  * (node order of that call); writes at most `count`, returns how many. */
 int bqb_fused_node_times(double *out, int count);

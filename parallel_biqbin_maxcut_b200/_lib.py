@@ -128,6 +128,7 @@ SIGNATURES = {
     "bqb_ipm_schedule_set": (None, [C.c_int, C.c_int]),
     "bqb_engine_profile_enable": (None, [C.c_int]),
     "bqb_engine_profile": (None, [C.POINTER(C.c_double), C.c_int]),
+    "bqb_lambda_eta_profile": (None, [C.POINTER(C.c_double), C.c_int]),
     "bqb_ipm_coop_profile_enable": (None, [C.c_int]),
     "bqb_ipm_coop_profile": (None, [C.POINTER(C.c_double), C.c_int]),
     "bqb_ipm_autotune": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),

@@ -15,7 +15,10 @@
 // bundle_xcomb_kernel: X = X_bundle * lambda after a serious step.
 #include <math.h>
 
+#include <mutex>
+
 #include "bundle_body.cuh"
+#include "globals.h"
 
 namespace bqb {
 
@@ -99,6 +102,24 @@ void BundleDev::ensure_m(int m_, cudaStream_t s)
     (void)s;
 }
 
+extern std::atomic<int> g_eprof_on;
+
+// lambda_eta counters of the engines (with the engines' phase profile on):
+// calls, rounds, sum of k, cycles in the QP, cycles, sum of m.
+DevBuf<unsigned long long> g_le_prof;
+std::mutex g_le_prof_mu;
+
+static unsigned long long* le_prof_device()
+{
+    if (!g_eprof_on.load()) return nullptr;
+    std::lock_guard<std::mutex> lock(g_le_prof_mu);
+    if (!g_le_prof.p) {
+        g_le_prof.ensure(8);
+        BQB_CUDA(cudaMemset(g_le_prof.p, 0, 8 * sizeof(unsigned long long)));
+    }
+    return g_le_prof.p;
+}
+
 void lambda_eta_launch(BundleDev& b, const double* zeta_in, cudaStream_t s)
 {
     // k is only known on the device: size shared memory for any k <= cap.
@@ -108,6 +129,7 @@ void lambda_eta_launch(BundleDev& b, const double* zeta_in, cudaStream_t s)
     BQB_SMEM_LIMIT(lambda_eta_kernel, bytes);
     LeArgs a{b.G.p, b.ldg, b.slot.p, b.m, zeta_in, b.Fv.p, b.gam.p, b.lam.p, b.eta.p, b.dgam.p,
              b.gtest.p, b.dstate.p, b.istate.p, b.qp_ws.p, -1};
+    a.prof = le_prof_device();
     lambda_eta_kernel<<<1, LE_THREADS, bytes, s>>>(a);
     BQB_COUNT_LAUNCH();
     check_launch("lambda_eta_kernel");
@@ -116,9 +138,9 @@ void lambda_eta_launch(BundleDev& b, const double* zeta_in, cudaStream_t s)
 void solve_lambda_launch(int k, const double* Q, const double* c, double* lambda, int* err, cudaStream_t s)
 {
     static DevBuf<double> ws;
-    double* w = ws.ensure((size_t)2 * k * k + 8 * (size_t)k + 8);
+    double* w = ws.ensure((size_t)k * k + qp_a_doubles(k) + 8 * (size_t)k + 8);
     size_t bytes = 2 * (size_t)k * sizeof(double);
-    if (k <= QP_SMEM_K) bytes += ((size_t)k * k + 6 * (size_t)k) * sizeof(double);
+    if (k <= QP_SMEM_K) bytes += (qp_a_doubles(k) + 6 * (size_t)k) * sizeof(double);
     BQB_SMEM_LIMIT(solve_lambda_kernel, bytes);
     solve_lambda_kernel<<<1, 32, bytes, s>>>(k, Q, c, lambda, err, w);
     BQB_COUNT_LAUNCH();
@@ -159,3 +181,23 @@ void bundle_fval_launch(BundleDev& b, const double* L, const int* slot_ptr, cons
 }
 
 }  // namespace bqb
+
+using namespace bqb;
+
+// The engines' lambda_eta counters (with bqb_engine_profile_enable(1)):
+// out[6] = {calls, rounds of the lambda / eta alternation, sum of the bundle
+// sizes k, SM cycles in the QP, SM cycles in the calls, sum of the cut
+// counts m}; reset != 0 zeroes them after reading.  For profiling; no
+// reference counterpart.
+BQB_API void bqb_lambda_eta_profile(double* out, int reset)
+{
+    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    std::lock_guard<std::mutex> lock(g_le_prof_mu);
+    if (g_le_prof.p) {
+        BQB_CUDA(cudaDeviceSynchronize());
+        BQB_CUDA(cudaMemcpy(h, g_le_prof.p, sizeof(h), cudaMemcpyDeviceToHost));
+        if (reset) BQB_CUDA(cudaMemset(g_le_prof.p, 0, sizeof(h)));
+    }
+    for (int i = 0; i < 6; ++i)
+        if (out) out[i] = (double)h[i];
+}

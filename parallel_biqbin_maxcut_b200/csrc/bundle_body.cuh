@@ -19,11 +19,211 @@ __device__ __forceinline__ double Qat(const double* Q, int k, int a, int b)
     return a >= b ? Q[a + (size_t)b * k] : Q[b + (size_t)a * k];
 }
 
+// Doubles of the QP workspace's matrix region for bundle size k: the
+// register form (k <= 32) uses a 32 x 32 broadcast buffer.
+__host__ __device__ constexpr size_t qp_a_doubles(int k) { return k <= 32 ? 1024 : (size_t)k * k; }
+
+// Step J of the Cholesky factorisation of the QP's matrix A = Q + Diag(z ./
+// lambda) held in registers (lane p < KP holds row p in s[], columns <= p;
+// rows and columns from k to KP - 1 are the identity's).  The same
+// operations in the same order as the shared-memory form below: the pivot's
+// reciprocal square root rj, the column scaled by it, then every entry
+// (p, r), J < r <= p, less l_pJ l_rJ (a rounded product, then a rounded
+// difference).  Column J goes to the warp through Lc (one store per lane,
+// then broadcast reads).  Instantiated for every J so that s[] stays in
+// registers.  After a non-positive pivot the steps go on with a unit pivot
+// and pd is false.
+template <int KP, int J>
+__device__ __forceinline__ void qp_chol_step(double (&s)[KP], int p, bool& pd, double& rdiag, double* Lc)
+{
+    if constexpr (J < KP) {
+        double d = __shfl_sync(0xffffffffu, s[J], J);
+        if (!(d > 0.0)) {
+            pd = false;
+            d = 1.0;
+        }
+        const double rj = rsqrt(d);
+        const double l = p == J ? __dmul_rn(d, rj) : __dmul_rn(s[J], rj);
+        if (p == J) rdiag = rj;
+        s[J] = l;
+        if (p < KP) Lc[J * KP + p] = l;
+        __syncwarp();
+#pragma unroll
+        for (int r = J + 1; r < KP; ++r)
+            if (r <= p) s[r] = __dsub_rn(s[r], __dmul_rn(l, Lc[J * KP + r]));
+        __syncwarp();
+        qp_chol_step<KP, J + 1>(s, p, pd, rdiag, Lc);
+    }
+}
+
+// Forward substitution step J for u and w together (lane p holds u_p, w_p
+// and row p of the factor): u_J *= 1/L_JJ, then u_p -= L_pJ u_J below.
+template <int KP, int J>
+__device__ __forceinline__ void qp_fwd_step(const double (&s)[KP], int p, double rdiag, double& u, double& w)
+{
+    if constexpr (J < KP) {
+        const double rj = __shfl_sync(0xffffffffu, rdiag, J);
+        const double uj = __dmul_rn(__shfl_sync(0xffffffffu, u, J), rj);
+        const double wj = __dmul_rn(__shfl_sync(0xffffffffu, w, J), rj);
+        if (p == J) {
+            u = uj;
+            w = wj;
+        } else if (p > J) {
+            u = __dsub_rn(u, __dmul_rn(s[J], uj));
+            w = __dsub_rn(w, __dmul_rn(s[J], wj));
+        }
+        qp_fwd_step<KP, J + 1>(s, p, rdiag, u, w);
+    }
+}
+
+// Backward substitution step J (from KP - 1 down): u_J *= 1/L_JJ, then
+// u_p -= L_Jp u_J above; Lr holds the factor by rows.
+template <int KP, int J>
+__device__ __forceinline__ void qp_bwd_step(const double* Lr, int p, double rdiag, double& u, double& w)
+{
+    if constexpr (J >= 0) {
+        const double rj = __shfl_sync(0xffffffffu, rdiag, J);
+        const double uj = __dmul_rn(__shfl_sync(0xffffffffu, u, J), rj);
+        const double wj = __dmul_rn(__shfl_sync(0xffffffffu, w, J), rj);
+        if (p == J) {
+            u = uj;
+            w = wj;
+        } else if (p < J) {
+            const double l = Lr[J * KP + p];
+            u = __dsub_rn(u, __dmul_rn(l, uj));
+            w = __dsub_rn(w, __dmul_rn(l, wj));
+        }
+        qp_bwd_step<KP, J - 1>(Lr, p, rdiag, u, w);
+    }
+}
+
+// warp_qp for k <= KP (16 or 32): lane a < k keeps the QP's entry a of
+// lambda, z, Q lambda, c, u, w and row a of A = Q + Diag(z ./ lambda) in
+// registers; ws holds the factor's column broadcasts, then its rows (KP x KP
+// doubles).  The arithmetic is warp_qp's below, operation for operation
+// (the same sums in the same order, the same warp reductions), so both
+// forms return the same bits; this one has no shared-memory loop per row.
+template <int KP>
+__device__ __noinline__ bool warp_qp_reg(int k, const double* Q, const double* c, double* lam, double* ws)
+{
+    const int lane = threadIdx.x & 31;
+    const bool own = lane < k;
+    double la = 1.0 / k;
+    if (own) lam[lane] = la;
+    __syncwarp();
+    double qla = 0.0, ca = 0.0, za = 0.0;
+    if (own) {
+        ca = c[lane];
+        double acc = 0.0;
+        for (int b = 0; b < k; ++b) acc += Qat(Q, k, lane, b) * lam[b];
+        qla = acc;
+        za = acc + ca;
+    }
+    double mintmp = own ? za : BQB_BUNDLE_BIG;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mintmp = fmin(mintmp, __shfl_xor_sync(0xffffffffu, mintmp, o));
+    double y;
+    if (mintmp > 1) {
+        y = 0.0;
+    } else {
+        y = mintmp - 1.0;
+        if (own) za = za - y;
+    }
+    // (each lane's partial starts at 0.0, as the loop form's does)
+    double s1 = own ? 0.0 + za * la : 0.0, s2 = own ? 0.0 + la : 0.0;
+    double s3 = own ? 0.0 + la * qla : 0.0, s4 = own ? 0.0 + la * ca : 0.0;
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    s3 = warp_sum(s3);
+    s4 = warp_sum(s4);
+    double mu = 0.5 * (s1 / k);
+    double res_p = 1.0 - s2;
+    double gap = (s4 + 0.5 * s3) - (y - 0.5 * s3);
+    int cnt = 0;
+    double* L = ws;   // KP x KP
+    while (fabs(gap) > 1e-5) {
+        ++cnt;
+        // A = Q + Diag(z ./ lambda) (lower, padded with the identity), r = c - y + Qlam
+        // (an own lane's entries b <= lane are Q's lower triangle: Q[lane + b k])
+        double a[KP];
+        const double dg = own ? za / la : 0.0;
+#pragma unroll
+        for (int b = 0; b < KP; ++b) {
+            double v = b == lane ? 1.0 : 0.0;
+            if (own && b <= lane) {
+                v = Q[lane + (size_t)b * k];
+                if (b == lane) v += dg;
+            }
+            a[b] = v;
+        }
+        double u = own ? 1.0 : 0.0;
+        double w = own ? c[lane] - y + qla : 0.0;
+        bool pd = true;
+        double rdiag = 1.0;
+        qp_chol_step<KP, 0>(a, lane, pd, rdiag, L);
+        if (!pd) return false;
+        if (lane < KP) {
+#pragma unroll
+            for (int r = 0; r < KP; ++r) L[lane * KP + r] = r <= lane ? a[r] : 0.0;
+        }
+        __syncwarp();
+        qp_fwd_step<KP, 0>(a, lane, rdiag, u, w);
+        qp_bwd_step<KP, KP - 1>(L, lane, rdiag, u, w);
+        const double su = warp_sum(own ? 0.0 + u : 0.0), sw = warp_sum(own ? 0.0 + w : 0.0);
+        const double dy = (res_p + sw) / su;
+        double ap = -BQB_BUNDLE_BIG, ad = -BQB_BUNDLE_BIG;
+        double dl = 0.0, dz = 0.0;
+        if (own) {
+            dl = u * dy - w;
+            dz = 1.0 / la * (mu - la * za - za * dl);
+            ap = -dl / la;
+            ad = -dz / za;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ap = fmax(ap, __shfl_xor_sync(0xffffffffu, ap, o));
+            ad = fmax(ad, __shfl_xor_sync(0xffffffffu, ad, o));
+        }
+        ap = (ap > 0) ? ((0.99 / ap < 1.0) ? 0.99 / ap : 1.0) : 1.0;
+        ad = (ad > 0) ? ((0.99 / ad < 1.0) ? 0.99 / ad : 1.0) : 1.0;
+        y += ad * dy;
+        if (own) {
+            la = fma(ap, dl, la);
+            za = fma(ad, dz, za);
+            lam[lane] = la;
+        }
+        __syncwarp();
+        double t1 = 0.0, t2 = 0.0, t3 = 0.0, t4 = 0.0;
+        if (own) {
+            double acc = 0.0;
+            for (int b = 0; b < k; ++b) acc += Qat(Q, k, lane, b) * lam[b];
+            qla = acc;
+            t1 = 0.0 + la;
+            t2 = 0.0 + la * za;
+            t3 = 0.0 + la * acc;
+            t4 = 0.0 + la * ca;
+        }
+        t1 = warp_sum(t1);
+        t2 = warp_sum(t2);
+        t3 = warp_sum(t3);
+        t4 = warp_sum(t4);
+        __syncwarp();
+        res_p = 1 - t1;
+        mu = (t2 / k) * 0.4;
+        if (ap + ad > 1.8) mu *= 0.2;
+        gap = (t4 + 0.5 * t3) - (y - 0.5 * t3);
+        if (cnt > 30) break;
+    }
+    return true;
+}
+
 // One warp.  Q: k x k (lower triangle read), c: k, lam: k (out).
 // ws: A[k*k], then six k-vectors (Q lambda, z, dlambda, u, w, and the
 // reciprocals of the factor's diagonal).  Returns false on a non-PD A.
+// Bundles of up to 16 go to the register form above (same results).
 __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* lam, double* ws)
 {
+    if (k <= 16) return warp_qp_reg<16>(k, Q, c, lam, ws);
     const int lane = threadIdx.x & 31;
     double* A = ws;
     double* Qlam = A + (size_t)k * k;
@@ -207,6 +407,7 @@ struct LeArgs {
     int* istate;
     double* qp_ws_global;
     int k_fixed;   // >= 0: use this k instead of istate[BI_K]
+    unsigned long long* prof = nullptr;   // (profiling) calls, rounds, sum of k, QP cycles, cycles, sum of m
 };
 
 // sm: dynamic shared memory of le_smem_bytes(min(k, QP_SMEM_K)) bytes (at
@@ -257,6 +458,8 @@ __device__ inline void lambda_eta_body(const LeArgs& a, double* sm)
 
     double dir_prev = 0.0;
     int cnt = 0;
+    const long long c_start = a.prof ? clock64() : 0;
+    long long c_qp = 0;
     while (true) {
         ++cnt;
         for (int b = warp; b < k; b += nw) {
@@ -267,11 +470,13 @@ __device__ inline void lambda_eta_body(const LeArgs& a, double* sm)
             if (lane == 0) c[b] = zeta[b] + (-t) * acc;
         }
         __syncthreads();
+        const long long c0 = a.prof ? clock64() : 0;
         if (warp == 0) {
             const bool ok = warp_qp(k, Q, c, lam, qpws);
             if (!ok && lane == 0) flag = 1;
         }
         __syncthreads();
+        if (a.prof) c_qp += clock64() - c0;
         if (flag) break;
         double acc2 = 0.0;
         for (int i = tid; i < m; i += blockDim.x) {
@@ -296,6 +501,14 @@ __device__ inline void lambda_eta_body(const LeArgs& a, double* sm)
     if (flag) {
         if (tid == 0) atomicOr(&a.istate[BI_ERR], 2);
         return;
+    }
+    if (a.prof && tid == 0) {
+        atomicAdd(a.prof + 0, 1ull);
+        atomicAdd(a.prof + 1, (unsigned long long)cnt);
+        atomicAdd(a.prof + 2, (unsigned long long)k);
+        atomicAdd(a.prof + 3, (unsigned long long)c_qp);
+        atomicAdd(a.prof + 4, (unsigned long long)(clock64() - c_start));
+        atomicAdd(a.prof + 5, (unsigned long long)m);
     }
     for (int b = tid; b < k; b += blockDim.x) a.lam[b] = lam[b];
     if (a.gtest)
@@ -501,7 +714,7 @@ __device__ inline void bundle_append_body(int* __restrict__ slot, int* __restric
 __host__ __device__ inline size_t le_smem_bytes(int k)
 {
     const size_t base = 3 * (size_t)k;
-    if (k <= QP_SMEM_K) return (base + (size_t)k * k + (size_t)k * k + 6 * (size_t)k) * sizeof(double);
+    if (k <= QP_SMEM_K) return (base + (size_t)k * k + qp_a_doubles(k) + 6 * (size_t)k) * sizeof(double);
     return base * sizeof(double);
 }
 
