@@ -1,14 +1,13 @@
-// Annealing chains of the k-gonal separation, one chain per thread
-// (src/qap_simulated_annealing.c:12-190 restated per chain).
+// Annealing chains of the k-gonal separation, one chain per warp
+// (src/qap_simulated_annealing.c:12-190 restated per chain; the warp
+// evaluates the moves of its chain speculatively, kgon_chain_warp).
 //
 // Layout: the chains of a CTA share the matrix X, staged in shared memory
-// when it fits (n <= 158 for 64 chains), and keep their permutations in
-// shared memory interleaved by chain (perm entry i of chain t at
-// i * SA_CHAINS_PER_CTA + t) so that the threads of a warp touching the same
-// position hit different banks.  The sum that sets the starting temperature
-// is taken by one thread in the reference's order, so every chain's
-// arithmetic is the sequential arithmetic of the restatement it is checked
-// against (IEEE double, no reassociation).
+// when it fits, and each warp keeps its chain's permutation in shared
+// memory.  The sum that sets the starting temperature is taken by one thread
+// in the reference's order, so every chain's arithmetic is the sequential
+// arithmetic of the restatement it is checked against (IEEE double, no
+// reassociation).
 #include <math.h>
 
 #include "kgon_sa.cuh"
@@ -17,25 +16,27 @@ namespace bqb {
 
 namespace {
 
-__global__ void __launch_bounds__(SA_CHAINS_PER_CTA)
+constexpr int SA_WARPS = 8;   // chains per CTA
+
+__global__ void __launch_bounds__(SA_WARPS * 32)
 kgon_sa_kernel(const double* __restrict__ X, int n, int K, int types, int chains, unsigned long long seed,
                int x_in_smem, double* __restrict__ cost_out, int* __restrict__ perm_out, int* __restrict__ status)
 {
     extern __shared__ __align__(16) double sa_smem[];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, w = tid >> 5;
     const size_t nn = (size_t)n * n;
     double* sX = sa_smem;
     double* sT = sa_smem + (x_in_smem ? nn : 0);
-    unsigned short* P = (unsigned short*)(sT + 2);
+    unsigned short* P = (unsigned short*)(sT + 2) + (size_t)w * n;
     if (x_in_smem)
         for (size_t e = tid; e < nn; e += blockDim.x) sX[e] = X[e];
     __syncthreads();
     const double* Xs = x_in_smem ? sX : X;
     if (tid == 0) sT[0] = kgon_temperature(Xs, n, K);
     __syncthreads();
-    const int c = blockIdx.x * SA_CHAINS_PER_CTA + tid;
+    const int c = blockIdx.x * SA_WARPS + w;
     if (c >= chains) return;
-    kgon_chain(Xs, n, K, types, c, seed, sT[0], P, SA_CHAINS_PER_CTA, tid, cost_out, perm_out, status);
+    kgon_chain_warp(Xs, n, K, types, c, seed, sT[0], P, cost_out, perm_out, status);
 }
 
 }  // namespace
@@ -50,15 +51,15 @@ void kgon_sa_device(KgonSaState& st, const double* dX, int n, int k, int types, 
     st.hcost.ensure(chains);
     st.hperm.ensure((size_t)chains * 7);
     st.hstat.ensure(1);
-    const size_t perm_bytes = (size_t)n * SA_CHAINS_PER_CTA * sizeof(unsigned short);
+    const size_t perm_bytes = (size_t)n * SA_WARPS * sizeof(unsigned short);
     const size_t fixed = 2 * sizeof(double) + perm_bytes;
     const size_t xbytes = (size_t)n * n * sizeof(double);
     const int x_in_smem = fixed + xbytes <= rt().smem_optin ? 1 : 0;
     const size_t bytes = fixed + (x_in_smem ? xbytes : 0);
     BQB_SMEM_LIMIT(kgon_sa_kernel, bytes);
     BQB_CUDA(cudaMemsetAsync(st.status.p, 0, sizeof(int), s));
-    const int grid = (chains + SA_CHAINS_PER_CTA - 1) / SA_CHAINS_PER_CTA;
-    kgon_sa_kernel<<<grid, SA_CHAINS_PER_CTA, bytes, s>>>(dX, n, k, types, chains, (unsigned long long)seed,
+    const int grid = (chains + SA_WARPS - 1) / SA_WARPS;
+    kgon_sa_kernel<<<grid, SA_WARPS * 32, bytes, s>>>(dX, n, k, types, chains, (unsigned long long)seed,
                                                          x_in_smem, st.cost.p, st.perm.p, st.status.p);
     BQB_COUNT_LAUNCH();
     check_launch("kgon_sa_kernel");

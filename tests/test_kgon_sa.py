@@ -5,9 +5,11 @@ built with the reference's flags and drawing from rand(), returns the
 reference build's qap_simulated_annealing value, permutation and rand()
 state (src/qap_simulated_annealing.c) -- this pins the restatement.
 
-GPU: the chains of bqb_kgon_sa (one thread per chain, SplitMix64 streams)
-equal the oracle's chains with the same streams bit for bit: the same best
-values, permutations and round-limit flag."""
+GPU: the chains of bqb_kgon_sa (one warp per chain evaluating its moves
+speculatively, SplitMix64 streams) equal the oracle's one-move-at-a-time
+chains with the same streams bit for bit: the same best values,
+permutations and round-limit flag, with X in shared memory (n <= 127) and
+in global memory (n = 200, 343)."""
 import ctypes as C
 
 import numpy as np
@@ -70,7 +72,7 @@ def test_oracle_chain_values_are_inequality_values():
 @pytest.mark.gpu
 @port
 @pytest.mark.parametrize("k,types,nv,seed", [(5, 3, 30, 1), (7, 4, 30, 2), (5, 3, 100, 3), (7, 4, 100, 4),
-                                             (5, 3, 64, 5), (7, 4, 127, 6)])
+                                             (5, 3, 64, 5), (7, 4, 127, 6), (5, 3, 200, 7), (7, 4, 343, 8)])
 def test_gpu_chains_equal_oracle(lib, k, types, nv, seed):
     X = _X(nv, seed)
     chains = 60 * types if nv <= 64 else 50 * types
