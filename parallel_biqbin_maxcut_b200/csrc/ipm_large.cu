@@ -87,20 +87,29 @@ enum CoopProf : int {
     COOP_PROF_WORDS = 8
 };
 
-struct Smem {
-    double Lc[CB][CB];    // the panel's factor by columns (row Q = column Q)
+// Trial sweeps a line-search round runs together (each with its own panel
+// factor in shared memory).
+constexpr int NTRIAL = 4;
+
+// One panel's factorisation.
+struct PanelF {
+    double Lc[CB][CB];       // the panel's factor by columns (row Q = column Q)
     double Lr[CB][CB + 2];   // the panel's factor by rows (rows 16-byte aligned)
-    double D[CB][LDS];    // the panel block
-    double Li[CB][LDS];   // inverse of the factor (lower)
+    double D[CB][LDS];       // the panel block
+    double Li[CB][LDS];      // inverse of the factor (lower)
+    double R[CB];            // reciprocals of the factor's diagonal
+};
+
+struct Smem {
+    PanelF pf[NTRIAL];
     double A1[CB][LDS];   // C_I, or a GEMM operand tile
     double A2[CB][LDS];   // C_J, or a GEMM operand tile
     double V1[CB][LDS];   // V_I, or a GEMM operand tile
     double V2[CB][LDS];   // V_J, or a GEMM operand tile
-    double R[CB];         // reciprocals of the factor's diagonal
     double red[CW * 4];
     double tot[4];
     int ok;
-    int pd;
+    int pd[NTRIAL];
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -235,7 +244,7 @@ __device__ __forceinline__ void chol_step(double (&s)[CB], int p, int& pd, doubl
 // interleaved partial sums, so the dependent chain per step is a quarter as
 // long.
 template <int I>
-__device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int t)
+__device__ __forceinline__ void linv_step(double (&li)[CB], const PanelF& sm, int t)
 {
     if constexpr (I < CB) {
         double a0 = I == t ? 1.0 : 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
@@ -255,30 +264,30 @@ __device__ __forceinline__ void linv_step(double (&li)[CB], const Smem& sm, int 
     }
 }
 
-// Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
-// in shared memory.  Warp 0 factors in registers (lane p holds row p; the
-// block is padded to 32 x 32 with the identity), then lane t forms column t
-// of Li by forward substitution.  Returns false (in every thread) on a
-// non-positive pivot.
-__device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, unsigned long long* load_ns)
+// The panel block D = A[K, K] (b x b, padded to 32 x 32 with the identity)
+// into f.D; every thread of the CTA takes part (no barrier).
+__device__ __forceinline__ void panel_load(const double* A, int n, int k0, int b, PanelF& f)
 {
-    const int tid = threadIdx.x;
-    const unsigned long long t0 = load_ns ? global_ns() : 0ull;
-    for (int e = tid; e < CB * CB; e += CT) {
+    for (int e = threadIdx.x; e < CB * CB; e += CT) {
         const int p = e % CB, q = e / CB;
-        sm.D[p][q] = p < b && q < b ? A[(k0 + p) + (size_t)(k0 + q) * n] : (p == q ? 1.0 : 0.0);
+        f.D[p][q] = p < b && q < b ? A[(k0 + p) + (size_t)(k0 + q) * n] : (p == q ? 1.0 : 0.0);
     }
-    __syncthreads();
-    if (load_ns) *load_ns += global_ns() - t0;
-    if (tid < 32) {
-        const int p = tid;
+}
+
+// One warp: the Cholesky factor Ld of f.D and Li = Ld^{-1} in f (lane p
+// holds row p in registers), then lane t forms column t of Li by forward
+// substitution.  *pd_out = 0 on a non-positive pivot (then f is partial).
+__device__ void panel_chol(PanelF& sm, int* pd_out)
+{
+    {
+        const int p = threadIdx.x & 31;
         double s[CB];
 #pragma unroll
         for (int r = 0; r < CB; ++r) s[r] = sm.D[p][r];
         int pd = 1;
         double rdiag = 1.0;
         chol_step<0>(s, p, pd, rdiag, sm.Lc);
-        if (p == 0) sm.pd = pd;
+        if (p == 0) *pd_out = pd;
         if (pd) {
 #pragma unroll
             for (int r = 0; r < CB; r += 2)
@@ -293,8 +302,20 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, un
             for (int i = 0; i < CB; ++i) sm.Li[i][p] = li[i];
         }
     }
+}
+
+// Every CTA: the Cholesky factor Ld of D = A[K, K] (b x b) and Li = Ld^{-1}
+// in sm.pf[0] (warp 0 factors).  Returns false (in every thread) on a
+// non-positive pivot.
+__device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, unsigned long long* load_ns)
+{
+    const unsigned long long t0 = load_ns ? global_ns() : 0ull;
+    panel_load(A, n, k0, b, sm.pf[0]);
     __syncthreads();
-    return sm.pd != 0;
+    if (load_ns) *load_ns += global_ns() - t0;
+    if (threadIdx.x < 32) panel_chol(sm.pf[0], &sm.pd[0]);
+    __syncthreads();
+    return sm.pd[0] != 0;
 }
 
 // C rows of tile block I (32 x b): the panel columns of A for rows I, or, for
@@ -303,7 +324,7 @@ __device__ bool panel_factor(const double* A, int n, int k0, int b, Smem& sm, un
 // C(r, p) Li(q, p).  Not inlined: its registers are then allocated apart
 // from the panel factorisation's, and the kernel needs no spill slots.
 __device__ __noinline__ void load_v(const double* A, int n, int I, int k0, int b, const double* Wprev, bool from_w,
-                       double (*Cs)[LDS], double (*Vs)[LDS], Smem& sm)
+                       double (*Cs)[LDS], double (*Vs)[LDS], const PanelF& f)
 {
     const int i0 = I * CB;
     for (int e = threadIdx.x; e < CB * CB; e += CT) {
@@ -323,7 +344,7 @@ __device__ __noinline__ void load_v(const double* A, int n, int I, int k0, int b
         for (int p = 0; p <= c0 + 3 * CW; ++p) {
             const double cp = Cs[r][p];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) v[j] = fma(cp, sm.Li[c0 + CW * j][p], v[j]);
+            for (int j = 0; j < 4; ++j) v[j] = fma(cp, f.Li[c0 + CW * j][p], v[j]);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) Vs[r][c0 + CW * j] = c0 + CW * j < b ? v[j] : 0.0;
@@ -337,15 +358,15 @@ __device__ __noinline__ void load_v(const double* A, int n, int I, int k0, int b
 // the update.
 template <bool FULL>
 __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, const double* Wprev,
-                          const double* Dprev, double* Wcur, double* Dcur, Smem& sm)
+                          const double* Dprev, double* Wcur, double* Dcur, Smem& sm, const PanelF& f)
 {
     const bool fixI = FULL && K > 0 && I == K - 1;
     const bool fixJ = FULL && K > 0 && J == K - 1;
     const bool upd = I != K && J != K;
     if (!upd && !fixI && !fixJ && !(FULL && I == K && J == K)) return;
     if (upd) {
-        load_v(A, n, I, k0, b, Wprev, fixI, sm.A1, sm.V1, sm);
-        if (J != I) load_v(A, n, J, k0, b, Wprev, fixJ, sm.A2, sm.V2, sm);
+        load_v(A, n, I, k0, b, Wprev, fixI, sm.A1, sm.V1, f);
+        if (J != I) load_v(A, n, J, k0, b, Wprev, fixJ, sm.A2, sm.V2, f);
     }
     double (*VJ)[LDS] = J != I ? sm.V2 : sm.V1;
     const int i0 = I * CB, j0 = J * CB, kp0 = (K - 1) * CB;
@@ -381,7 +402,7 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
         for (int p = c0; p < b; ++p) {
             const double vp = sm.V1[r][p];
 #pragma unroll
-            for (int jj = 0; jj < 4; ++jj) w[jj] = fma(vp, sm.Li[p][c0 + CW * jj], w[jj]);
+            for (int jj = 0; jj < 4; ++jj) w[jj] = fma(vp, f.Li[p][c0 + CW * jj], w[jj]);
         }
         const int i = i0 + r;
 #pragma unroll
@@ -395,11 +416,48 @@ __device__ void tile_step(double* A, int n, int K, int k0, int b, int I, int J, 
         for (int e = threadIdx.x; e < CB * CB; e += CT) {
             const int p = e % CB, q = e / CB;
             double acc = 0.0;
-            for (int k = p > q ? p : q; k < b; ++k) acc = fma(sm.Li[k][p], sm.Li[k][q], acc);
+            for (int k = p > q ? p : q; k < b; ++k) acc = fma(f.Li[k][p], f.Li[k][q], acc);
             Dcur[p + (size_t)q * CB] = acc;
         }
     }
     __syncthreads();
+}
+
+// The final phase of a full sweep: the fix of the last panel's row and
+// column blocks, and A = -A; with Xm, also Mout = Fout = A .* Xm (Xm + ap dXm
+// with dXm).  No barrier.
+__device__ void sweep_final(double* A, const CoopArgs& a, const double* Xm, double* Mout, double* Fout,
+                            const double* dXm, double ap)
+{
+    const int n = a.n;
+    const int T = (n + CB - 1) / CB;
+    {
+        const int K = T;
+        const double* Wl = a.Wb + (size_t)((K + 1) & 1) * n * CB;
+        const double* Dl = a.Db + (size_t)((K + 1) & 1) * CB * CB;
+        const int kp0 = (K - 1) * CB;
+        for (int q = blockIdx.x; q < T * T; q += gridDim.x) {
+            const int I = q % T, J = q / T;
+            const bool fixI = I == K - 1, fixJ = J == K - 1;
+            for (int e = threadIdx.x; e < CB * CB; e += CT) {
+                const int i = I * CB + e % CB, j = J * CB + e / CB;
+                if (i >= n || j >= n) continue;
+                double v;
+                if (fixI && fixJ) v = -Dl[(i - kp0) + (size_t)(j - kp0) * CB];
+                else if (fixJ) v = Wl[i + (size_t)(j - kp0) * n];
+                else if (fixI) v = Wl[j + (size_t)(i - kp0) * n];
+                else v = A[i + (size_t)j * n];
+                const size_t ij = i + (size_t)j * n;
+                A[ij] = -v;
+                if (Xm) {
+                    const double xm = dXm ? fma(ap, dXm[ij], Xm[ij]) : Xm[ij];
+                    const double m = -v * xm;
+                    Mout[ij] = m;
+                    Fout[ij] = m;
+                }
+            }
+        }
+    }
 }
 
 // The panel sweep of A (n x n).  FULL: A becomes inv(A); otherwise only the
@@ -434,41 +492,107 @@ __device__ int sweep(double* A, const CoopArgs& a, Smem& sm, const double* Xm = 
         const int t0 = FULL ? 0 : K + 1;
         const int Tt = T - t0;
         for (int q = blockIdx.x; q < Tt * Tt; q += gridDim.x)
-            tile_step<FULL>(A, n, K, k0, b, t0 + q % Tt, t0 + q / Tt, Wprev, Dprev, Wcur, Dcur, sm);
+            tile_step<FULL>(A, n, K, k0, b, t0 + q % Tt, t0 + q / Tt, Wprev, Dprev, Wcur, Dcur, sm, sm.pf[0]);
         if (a.prof) __syncthreads();
         if (rec) a.prof[COOP_PROF_TILES] += global_ns() - tp;
         if (!grid_sync(a.bar, sm, a.prof)) return -1;
     }
     if (FULL) {
         // the last panel's fix, and A = -A
-        const int K = T;
-        const double* Wl = a.Wb + (size_t)((K + 1) & 1) * n * CB;
-        const double* Dl = a.Db + (size_t)((K + 1) & 1) * CB * CB;
-        const int kp0 = (K - 1) * CB;
-        for (int q = blockIdx.x; q < T * T; q += gridDim.x) {
-            const int I = q % T, J = q / T;
-            const bool fixI = I == K - 1, fixJ = J == K - 1;
-            for (int e = threadIdx.x; e < CB * CB; e += CT) {
-                const int i = I * CB + e % CB, j = J * CB + e / CB;
-                if (i >= n || j >= n) continue;
-                double v;
-                if (fixI && fixJ) v = -Dl[(i - kp0) + (size_t)(j - kp0) * CB];
-                else if (fixJ) v = Wl[i + (size_t)(j - kp0) * n];
-                else if (fixI) v = Wl[j + (size_t)(i - kp0) * n];
-                else v = A[i + (size_t)j * n];
-                const size_t ij = i + (size_t)j * n;
-                A[ij] = -v;
-                if (Xm) {
-                    const double xm = dXm ? fma(ap, dXm[ij], Xm[ij]) : Xm[ij];
-                    const double m = -v * xm;
-                    Mout[ij] = m;
-                    Fout[ij] = m;
-                }
-            }
-        }
+        sweep_final(A, a, Xm, Mout, Fout, dXm, ap);
         if (!grid_sync(a.bar, sm, a.prof)) return -1;
     }
     return 1;
+}
+
+// Trial sweeps run together: nt matrices, each the trailing sweep (its
+// pivots) or, for at most one, the full sweep (its inverse).  state[t]
+// becomes 1 (positive definite) or -1 (a non-positive pivot); every CTA takes
+// the same decisions.
+struct TrialSet {
+    double* A[NTRIAL];
+    int full[NTRIAL];
+    int state[NTRIAL];
+    int nt;
+};
+
+// In each phase every running trial's panel block is factored by its own
+// warp (warp t for trial t) and the tiles of all running trials are spread
+// over the CTAs; a trial drops out at its first non-positive pivot, a
+// trailing sweep is done at its last panel's factorisation, a full sweep
+// after its final phase.  Returns false when a barrier gave up.  The last
+// phase has no barrier when no full sweep runs on (the caller's next fill
+// goes to other matrices or follows a barrier).
+__device__ bool msweep(TrialSet& ts, const CoopArgs& a, Smem& sm)
+{
+    const int n = a.n;
+    const int T = (n + CB - 1) / CB;
+    const bool rec = a.prof && blockIdx.x == 0 && threadIdx.x == 0;
+    for (int t = 0; t < ts.nt; ++t) ts.state[t] = 0;
+    for (int K = 0; K < T; ++K) {
+        const int k0 = K * CB, b = n - k0 < CB ? n - k0 : CB;
+        unsigned long long tp = rec ? global_ns() : 0ull;
+        for (int t = 0; t < ts.nt; ++t)
+            if (ts.state[t] == 0) panel_load(ts.A[t], n, k0, b, sm.pf[t]);
+        __syncthreads();
+        {
+            const int w = threadIdx.x >> 5;
+            if (w < ts.nt && ts.state[w] == 0) panel_chol(sm.pf[w], &sm.pd[w]);
+        }
+        __syncthreads();
+        bool running = false;
+        int tiles[NTRIAL];
+        int total = 0;
+        for (int t = 0; t < ts.nt; ++t) {
+            tiles[t] = 0;
+            if (ts.state[t] != 0) continue;
+            if (!sm.pd[t]) {
+                ts.state[t] = -1;
+            } else if (!ts.full[t] && K == T - 1) {
+                ts.state[t] = 1;
+            } else {
+                running = true;
+                const int tt = ts.full[t] ? T : T - K - 1;
+                tiles[t] = tt * tt;
+                total += tiles[t];
+            }
+        }
+        if (rec) {
+            const unsigned long long tn = global_ns();
+            a.prof[COOP_PROF_FACTOR] += tn - tp;
+            a.prof[COOP_PROF_PHASES] += 1;
+            tp = tn;
+        }
+        if (!running) return true;
+        const double* Wprev = a.Wb + (size_t)((K + 1) & 1) * n * CB;
+        const double* Dprev = a.Db + (size_t)((K + 1) & 1) * CB * CB;
+        double* Wcur = a.Wb + (size_t)(K & 1) * n * CB;
+        double* Dcur = a.Db + (size_t)(K & 1) * CB * CB;
+        for (int q = blockIdx.x; q < total; q += gridDim.x) {
+            int t = 0, r = q;
+            while (r >= tiles[t]) {
+                r -= tiles[t];
+                ++t;
+            }
+            if (ts.full[t]) {
+                tile_step<true>(ts.A[t], n, K, k0, b, r % T, r / T, Wprev, Dprev, Wcur, Dcur, sm, sm.pf[t]);
+            } else {
+                const int tt = T - K - 1;
+                tile_step<false>(ts.A[t], n, K, k0, b, K + 1 + r % tt, K + 1 + r / tt, Wprev, Dprev, Wcur, Dcur, sm,
+                                 sm.pf[t]);
+            }
+        }
+        if (a.prof) __syncthreads();
+        if (rec) a.prof[COOP_PROF_TILES] += global_ns() - tp;
+        if (!grid_sync(a.bar, sm, a.prof)) return false;
+    }
+    for (int t = 0; t < ts.nt; ++t)
+        if (ts.state[t] == 0 && ts.full[t]) {
+            sweep_final(ts.A[t], a, nullptr, nullptr, nullptr, nullptr, 0.0);
+            if (!grid_sync(a.bar, sm, a.prof)) return false;
+            ts.state[t] = 1;
+        }
+    return true;
 }
 
 // ---- products ------------------------------------------------------------------
@@ -654,13 +778,12 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
     double phi = sm.tot[2];
     double gap = fabs(phi - psi);
     int iter = 0, ls_total = 0, status = IPM_OK;
-    // Zi and F trade buffers: the dual line search sweeps its trials in
-    // full, alternating between the two, so a first trial that passes leaves
-    // inv(Z) of the new point (the same matrix, with the same arithmetic, as
-    // the sweep of the next iteration would) and M = F = inv(Z) .* X of the
-    // new X in the other buffer.
-    double* Zi = a.Zi;
-    double* F = a.F;
+    // When the dual line search's first trial (ad = 1) passes, its full sweep
+    // leaves inv(Z) of the new point in Zi (the same matrix, with the same
+    // arithmetic, as this iteration's own sweep would), and the next
+    // iteration only forms M = F = Zi .* X.
+    double* const Zi = a.Zi;
+    double* const F = a.F;
     bool have_zi = false;
 
     while (alive && gap > 1e-2) {
@@ -686,6 +809,13 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
                 status = IPM_Z_NOT_PD;
                 break;
             }
+        } else {
+            for (size_t e = gtid; e < nn; e += gstride) {
+                const double m = Zi[e] * X[e];
+                a.M[e] = m;
+                F[e] = m;
+            }
+            if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         }
         have_zi = false;
         // F = inv(M); dy1 = F (-e)
@@ -717,86 +847,84 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         for (size_t c = gtid; c < (size_t)n; c += gstride) a.dy[c] = a.dy1[c] + a.dy2[c];
 
-        // primal line search: X + ap dX positive definite.  Consecutive
-        // trials (primal, then dual) alternate between T and T2: a CTA may
-        // still read the last panel block of one trial while the others fill
-        // the next, so no barrier is needed after a trial's sweep.
-        int tr = 0;
-        double ap = 1.0;
-        int trials = 0;
-        bool ok = false;
-        while (true) {
-            double* Tt = (tr++ & 1) ? a.T2 : a.T;
-            for (size_t e = gtid; e < nn; e += gstride) Tt[e] = fma(ap, a.dX[e], X[e]);
-            if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-            pd = sweep<false>(Tt, a, sm);
-            if (pd < 0) {
-                alive = false;
-                break;
+        // line searches (src/ipm_mc_pk.c:281-309): the primal search
+        // (X + ap dX positive definite) and the dual search (Z + ad Diag(dy)
+        // positive definite) each try 1, 0.8, 0.64, ... and keep the first
+        // step that passes.  Here a round sweeps the next two trials of each
+        // unfinished search together (primal in T, T2; dual in Zi, F, all free
+        // by now); every trial's pivots are those of its own sweep, so the
+        // steps kept are the one-at-a-time searches' steps.  The dual's first
+        // trial (ad = 1, the step itself when it passes) is a full sweep whose
+        // inverse starts the next iteration.
+        double ap = 1.0, ad = 1.0;   // the next trial step of each search
+        int pi = 0, di = 0;          // its trial index
+        int pres = 0, dres = 0;      // 1 found, -1 gave up
+        double ap_ok = 1.0, ad_ok = 1.0;
+        int rounds = 0;
+        while (pres == 0 || dres == 0) {
+            // a CTA may still read the last round's panel blocks
+            if (rounds++ > 0 && !(alive = grid_sync(a.bar, sm, a.prof))) break;
+            TrialSet ts;
+            double alpha[NTRIAL];
+            int dual[NTRIAL];
+            ts.nt = 0;
+            auto add = [&](double* buf, double al, bool du, bool full) {
+                ts.A[ts.nt] = buf;
+                ts.full[ts.nt] = full ? 1 : 0;
+                alpha[ts.nt] = al;
+                dual[ts.nt] = du ? 1 : 0;
+                ++ts.nt;
+            };
+            const int np0 = ts.nt;
+            if (pres == 0) {
+                add(a.T, ap, false, false);
+                if (pi + 1 < IPM_MAX_TRIALS) add(a.T2, ap * 0.8, false, false);
             }
-            if (pd) {
-                ok = true;
-                break;
+            const int nd0 = ts.nt;
+            if (dres == 0) {
+                add(Zi, ad, true, di == 0);
+                if (di + 1 < IPM_MAX_TRIALS) add(F, ad * 0.8, true, false);
             }
-            if (++trials >= IPM_MAX_TRIALS) break;
-            ap *= 0.8;
-        }
-        if (!alive) break;
-        ls_total += trials + 1;
-        if (!ok) {
-            status = IPM_LINESEARCH;
-            break;
-        }
-        if (ap < 1.0) ap *= 0.95;
-        // dual line search: Z + ad Diag(dy) positive definite.  The trials
-        // are full sweeps (the same pivots as the trailing ones), alternating
-        // between Zi and F, both free by now (the primal trials used T and
-        // T2, so no CTA still reads these); the final phase of the one that
-        // passes forms M = F = inv(Z + ad Diag(dy)) .* (X + ap dX) in the
-        // other buffer.  When the first trial (ad = 1, the step itself)
-        // passes, the next iteration starts from these.
-        double ad = 1.0;
-        trials = 0;
-        ok = false;
-        int dt = 0;
-        while (true) {
-            double* Tt = (dt & 1) ? F : Zi;
-            double* Fo = (dt & 1) ? Zi : F;
-            ++dt;
+            // (dy_i = dy1_i + dy2_i is formed here: a.dy was written just now by
+            // the thread that owns i, with no barrier since)
             for (size_t e = gtid; e < nn; e += gstride) {
                 const int i = (int)(e % n), j = (int)(e / n);
-                Tt[e] = i == j ? fma(ad, a.dy[i], a.zd[i]) : -L[e];
+                for (int t = 0; t < ts.nt; ++t)
+                    ts.A[t][e] = dual[t] ? (i == j ? fma(alpha[t], a.dy1[i] + a.dy2[i], a.zd[i]) : -L[e])
+                                         : fma(alpha[t], a.dX[e], X[e]);
             }
             if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-            // (only the first trial can be the step: later ones test the
-            // pivots alone)
-            pd = trials == 0 ? sweep<true>(Tt, a, sm, X, a.M, Fo, a.dX, ap) : sweep<false>(Tt, a, sm);
-            if (pd < 0) {
-                alive = false;
-                break;
-            }
-            if (pd) {
-                ok = true;
-                // the step is the trial's only when the first trial passed
-                // (after a failed trial it is 0.95 ad, another point)
-                if (trials == 0) {
-                    if (Tt != Zi) {
-                        F = Zi;
-                        Zi = Tt;
+            if (!(alive = msweep(ts, a, sm))) break;
+            // each search: the first of its trials that passed, in order
+            auto decide = [&](int t0, int t1, int& res, int& idx, double& step, double& ok_step) {
+                for (int t = t0; t < t1; ++t) {
+                    if (ts.state[t] == 1) {
+                        res = 1;
+                        ok_step = alpha[t];
+                        ls_total += idx + (t - t0) + 1;
+                        return t - t0;
                     }
-                    have_zi = true;
                 }
-                break;
+                idx += t1 - t0;
+                step = alpha[t1 - 1] * 0.8;
+                if (idx >= IPM_MAX_TRIALS) res = -1;
+                return -1;
+            };
+            if (pres == 0) decide(np0, nd0, pres, pi, ap, ap_ok);
+            if (dres == 0) {
+                const bool first = di == 0;
+                if (decide(nd0, ts.nt, dres, di, ad, ad_ok) == 0 && first) have_zi = true;
             }
-            if (++trials >= IPM_MAX_TRIALS) break;
-            ad *= 0.8;
+            if (pres < 0 || dres < 0) break;
         }
         if (!alive) break;
-        ls_total += trials + 1;
-        if (!ok) {
+        if (pres < 0 || dres < 0) {
             status = IPM_LINESEARCH;
             break;
         }
+        ap = ap_ok;
+        ad = ad_ok;
+        if (ap < 1.0) ap *= 0.95;
         if (ad < 1.0) ad *= 0.95;
 
         // update (src/ipm_mc_pk.c:313-334): X += ap dX, y += ad dy,
