@@ -1,6 +1,7 @@
 // Internal (non-exported) device-level API shared by the C entry points
 // and the device-resident bounding driver.
 #pragma once
+#include <atomic>
 #include <vector>
 
 #include "bqb_common.cuh"
@@ -26,6 +27,9 @@ constexpr int IPM_REG_NMAX = 128;
 // (csrc/ipm_large.cu); same arguments and results as ipm_device.
 void ipm_large(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
                const int* xslot);
+// Engines bounding nodes with n > IPM_REG_NMAX at the moment: ipm_large
+// divides the co-resident CTAs among them (csrc/ipm_large.cu).
+extern std::atomic<int> g_large_share;
 
 // Raise the reference's fatal error for a non-zero IPM status word.
 void check_ipm_status_host(const double* out);

@@ -163,8 +163,14 @@ __device__ bool grid_sync(unsigned* bar, Smem& sm, unsigned long long* prof = nu
     return sm.ok != 0;
 }
 
-// Block-reduce four partial sums into part[blockIdx.x * 4 + k].
-__device__ void block_partials(double a, double b, double c, double d, Smem& sm, double* part)
+// The sums over all entries (the starting point's, the step's) are taken
+// over a fixed partition into VCTA parts, one block of CT threads each with
+// the entries of a CTA of a VCTA-CTA grid; a CTA of a smaller grid takes
+// several parts in turn.  The totals are then the same bits for any grid.
+constexpr int VCTA = 148;
+
+// Block-reduce four partial sums into part[v * 4 + k] (the CTA's part v).
+__device__ void block_partials(double a, double b, double c, double d, Smem& sm, double* part, int v)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     a = warp_sum(a);
@@ -181,17 +187,18 @@ __device__ void block_partials(double a, double b, double c, double d, Smem& sm,
     if (threadIdx.x < 4) {
         double s = 0.0;
         for (int q = 0; q < CW; ++q) s += sm.red[q * 4 + threadIdx.x];
-        part[blockIdx.x * 4 + threadIdx.x] = s;
+        part[v * 4 + threadIdx.x] = s;
     }
+    __syncthreads();   // sm.red is reused by the CTA's next part
 }
 
-// The totals of the partial sums (after a barrier), in CTA order: the same
+// The totals of the partial sums (after a barrier), in part order: the same
 // value in every CTA.
 __device__ void grid_totals(const double* part, Smem& sm)
 {
     if (threadIdx.x < 4) {
         double s = 0.0;
-        for (int g = 0; g < (int)gridDim.x; ++g) s += part[g * 4 + threadIdx.x];
+        for (int g = 0; g < VCTA; ++g) s += part[g * 4 + threadIdx.x];
         sm.tot[threadIdx.x] = s;
     }
     __syncthreads();
@@ -754,9 +761,11 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
 
     // ---- initial point (src/ipm_mc_pk.c:65-99): y_c = sum_r |L_rc| + 1.1,
     // zd = y - diag(L), X = I; psi = trace(L), mu = sum(zd) / 2n, phi = sum(y)
-    {
+    const size_t vstride = (size_t)VCTA * CT;
+    for (int v = blockIdx.x; v < VCTA; v += gridDim.x) {
+        const size_t vt = (size_t)v * CT + threadIdx.x;
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        for (size_t c = gtid; c < (size_t)n; c += gstride) {
+        for (size_t c = vt; c < (size_t)n; c += vstride) {
             double acc = 0.0;
             const double* Lc = L + c * n;
             for (int r = 0; r < n; ++r) acc += fabs(Lc[r]);
@@ -768,9 +777,9 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
             s1 += zc;
             s2 += yc;
         }
-        for (size_t e = gtid; e < nn; e += gstride) X[e] = (e % n == e / n) ? 1.0 : 0.0;
-        block_partials(s0, s1, s2, 0.0, sm, a.part);
+        block_partials(s0, s1, s2, 0.0, sm, a.part, v);
     }
+    for (size_t e = gtid; e < nn; e += gstride) X[e] = (e % n == e / n) ? 1.0 : 0.0;
     bool alive = grid_sync(a.bar, sm, a.prof);
     grid_totals(a.part, sm);
     double psi = sm.tot[0];
@@ -845,7 +854,6 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         if (a.prof) __syncthreads();
         if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_GEMM] += global_ns() - tg;
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
-        for (size_t c = gtid; c < (size_t)n; c += gstride) a.dy[c] = a.dy1[c] + a.dy2[c];
 
         // line searches (src/ipm_mc_pk.c:281-309): the primal search
         // (X + ap dX positive definite) and the dual search (Z + ad Diag(dy)
@@ -885,8 +893,7 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
                 add(Zi, ad, true, di == 0);
                 if (di + 1 < IPM_MAX_TRIALS) add(F, ad * 0.8, true, false);
             }
-            // (dy_i = dy1_i + dy2_i is formed here: a.dy was written just now by
-            // the thread that owns i, with no barrier since)
+            // (dy_i = dy1_i + dy2_i)
             for (size_t e = gtid; e < nn; e += gstride) {
                 const int i = (int)(e % n), j = (int)(e / n);
                 for (int t = 0; t < ts.nt; ++t)
@@ -928,12 +935,13 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         if (ad < 1.0) ad *= 0.95;
 
         // update (src/ipm_mc_pk.c:313-334): X += ap dX, y += ad dy,
-        // zd += ad dy, and the sums zx = <Z, X>, lx = <L, X>, sum(y) of the
-        // new point.  The diagonal of X goes with the vectors (the thread
-        // that moves zd_i also moves X_ii).
-        {
+        // zd += ad dy (dy = dy1 + dy2), and the sums zx = <Z, X>, lx = <L, X>,
+        // sum(y) of the new point.  The diagonal of X goes with the vectors
+        // (the thread that moves zd_i also moves X_ii).
+        for (int v = blockIdx.x; v < VCTA; v += gridDim.x) {
+            const size_t vt = (size_t)v * CT + threadIdx.x;
             double zx = 0.0, lx = 0.0, ys = 0.0;
-            for (size_t e = gtid; e < nn; e += gstride) {
+            for (size_t e = vt; e < nn; e += vstride) {
                 const int i = (int)(e % n), j = (int)(e / n);
                 if (i == j) continue;
                 const double xv = fma(ap, a.dX[e], X[e]);
@@ -942,19 +950,20 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
                 lx = fma(lv, xv, lx);
                 zx = fma(-lv, xv, zx);
             }
-            for (size_t c = gtid; c < (size_t)n; c += gstride) {
+            for (size_t c = vt; c < (size_t)n; c += vstride) {
                 const size_t e = c * n + c;
                 const double xv = fma(ap, a.dX[e], X[e]);
                 X[e] = xv;
-                const double yv = fma(ad, a.dy[c], a.y[c]);
-                const double zv = fma(ad, a.dy[c], a.zd[c]);
+                const double dyc = a.dy1[c] + a.dy2[c];
+                const double yv = fma(ad, dyc, a.y[c]);
+                const double zv = fma(ad, dyc, a.zd[c]);
                 a.y[c] = yv;
                 a.zd[c] = zv;
                 lx = fma(L[e], xv, lx);
                 zx = fma(zv, xv, zx);
                 ys += yv;
             }
-            block_partials(zx, lx, ys, 0.0, sm, a.part);
+            block_partials(zx, lx, ys, 0.0, sm, a.part, v);
         }
         if (!(alive = grid_sync(a.bar, sm, a.prof))) break;
         grid_totals(a.part, sm);
@@ -1011,9 +1020,20 @@ unsigned long long* coop_prof_device()
 std::mutex g_sched_mu;
 std::map<int, int> g_sched;
 
+}  // namespace
+
+// Engines bounding nodes above IPM_REG_NMAX right now (node.cu counts them):
+// each multi-CTA IPM launch then takes its share of the co-resident CTAs, so
+// the IPMs of concurrent engines run side by side instead of one after
+// another.  The IPM's result does not depend on its grid.
+std::atomic<int> g_large_share{0};
+
+namespace {
+
 // Grid size for n: the schedule's entry for its tile count, else one CTA
 // per 32 x 32 tile of the sweep; at most as many as can be co-resident (one
-// per SM at this register count).
+// per SM at this register count), divided by the number of engines bounding
+// large nodes at the time.
 CoopConfig coop_config(int n)
 {
     static int max_blocks = -1;
@@ -1034,7 +1054,9 @@ CoopConfig coop_config(int n)
         auto it = g_sched.find(T);
         if (it != g_sched.end()) g = it->second;
     }
-    if (g > max_blocks) g = max_blocks;
+    const int share = g_large_share.load();
+    const int cap = share > 1 ? max_blocks / share : max_blocks;
+    if (g > cap) g = cap;
     if (g < 1) g = 1;
     c.grid = g;
     return c;

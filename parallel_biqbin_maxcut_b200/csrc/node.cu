@@ -199,6 +199,18 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     const int n = PP_->n;
     CallClock call_clock;
     PhaseClock pc(s);
+    // (counted while it runs: concurrent large nodes share the GPU's CTAs)
+    struct LargeShare {
+        bool on;
+        explicit LargeShare(bool o) : on(o)
+        {
+            if (on) g_large_share.fetch_add(1);
+        }
+        ~LargeShare()
+        {
+            if (on) g_large_share.fetch_sub(1);
+        }
+    } large_share(n > IPM_REG_NMAX);
     E.final_cuts.reset();
     const int N0 = SP_->n;
     const int NB = N0 - 1;   // BabPbSize
