@@ -387,11 +387,12 @@ void bqb_fused_profile(double *out);
 void bqb_fused_phase_calls(long long *out);
 /* Seconds per phase of SDPbound on the engines (bqb_bound_nodes, the
  * parallel and serial solvers, the drop-in), summed over engines and calls
- * since the last reset: out[9] = {IPM, lambda_eta, L - B^T(gamma), op_B of
+ * since the last reset: out[12] = {IPM, lambda_eta, L - B^T(gamma), op_B of
  * the new bundle element + bundle step, heuristic, triangle separation,
- * pentagonal / heptagonal separation, cut upload and the rest, whole
- * calls}.  Off by default; with it on every phase boundary synchronises
- * the engine's stream.  For profiling; no reference counterpart. */
+ * pentagonal / heptagonal separation, the rest, whole calls, cut upload,
+ * fracsol, bundle growth}.  Off by default; with it on every phase boundary
+ * synchronises the engine's stream.  For profiling; no reference
+ * counterpart. */
 void bqb_engine_profile_enable(int on);
 void bqb_engine_profile(double *out, int reset);
 /* With the engines' profile on: out[6] = {lambda_eta calls, rounds of its

@@ -79,6 +79,9 @@ enum EngPhase : int {
     EP_KGON,         // pentagonal and heptagonal separation (X copy included)
     EP_REBUILD,      // cut upload, subgradient rebuild, state reads
     EP_TOTAL,        // whole sdp_bound calls
+    EP_UPLOAD,       // (part of the rest) cut upload: records, op_B^T index, buffer sizes
+    EP_FRAC,         // (part of the rest) X's last column for fracsol
+    EP_ALLOC,        // (part of the rest) bundle capacity growth
     EP_WORDS
 };
 std::atomic<int> g_eprof_on{0};
@@ -156,19 +159,21 @@ double bundle_iterations(Engine& E, int bdl_iter, double* t)
     cudaStream_t s = E.stream;
     const int n = nd.n;
     const size_t nn = (size_t)n * n;
+    PhaseClock pc(s);
     nd.hs.ensure(8);
     nd.hi.ensure(8);
     // k grows by at most one per iteration
     BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
     BQB_CUDA(cudaStreamSynchronize(s));
     const int k = nd.hi.p[BI_K];
+    pc.mark(EP_REBUILD);
     b.ensure_cap(k + bdl_iter + 2, n, s);
+    pc.mark(EP_ALLOC);
     nd.hi.p[BI_CAP] = b.cap;
     BQB_CUDA(cudaMemcpyAsync(b.istate.p + BI_CAP, nd.hi.p + BI_CAP, sizeof(int), cudaMemcpyHostToDevice, s));
     nd.hs.p[0] = *t;
     BQB_CUDA(cudaMemcpyAsync(b.dstate.p + BD_T, nd.hs.p, sizeof(double), cudaMemcpyHostToDevice, s));
     g_bundle_iters.fetch_add(bdl_iter);
-    PhaseClock pc(s);
     pc.mark(EP_REBUILD);
     for (int it = 0; it < bdl_iter; ++it) {
         lambda_eta_launch(b, nullptr, s);
@@ -233,9 +238,15 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         nd.P0N = N0;
         nd.P0L_gen = gen;
     }
+    auto upload = [&]() {
+        pc.mark(EP_REBUILD);
+        upload_cuts(E, H, PP_);
+        pc.mark(EP_UPLOAD);
+    };
     std::vector<int> x(NB > 0 ? NB : 1);
     std::vector<double> col(n);
     auto store_fracsol = [&]() {
+        pc.mark(EP_REBUILD);
         BQB_CUDA(cudaMemcpyAsync(col.data(), dX + (size_t)(n - 1) * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
         BQB_CUDA(cudaStreamSynchronize(s));
         int index = 0;
@@ -245,6 +256,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             else
                 node->fracsol[i] = 0.5 * (col[index++] + 1.0);
         }
+        pc.mark(EP_FRAC);
     };
     std::vector<double> hostL;
     auto heuristic = [&]() {
@@ -307,7 +319,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     double t = 0.5 * (bound - Bab_LBGet()) / (PP_->NIneq * viol3 * viol3);
 
     // bundle init: X_bundle(0) = X, G(:,0) = 1 - B(X), F(0) = <L,X>, bundle = 1
-    upload_cuts(E, H, PP_);
+    upload();
 
     // Learned warm start (off unless a model is loaded and switched on):
     // evaluate the proposed multipliers once (L0 = L - B^T(gamma_w), one
@@ -403,7 +415,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
                 ++m;
             }
         PP_->NIneq = m;
-        upload_cuts(E, H, PP_);
+        upload();
         BQB_CUDA(cudaMemcpyAsync(E.warm.gam.p, prop.data(), (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
         BQB_CUDA(cudaMemcpyAsync(nd.L0.p, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
         opBt_launch(nd.cuts, nd.L0.p, n, E.warm.gam.p, s);
@@ -424,14 +436,14 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         } else if (m != n_own) {
             PP_->NIneq = n_own;   // back to the child's own cuts
             rows.resize(n_own);
-            upload_cuts(E, H, PP_);
+            upload();
         }
         if (!keep)
             for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = 0.0;
     } else {
         if (PP_->NIneq != n_own) {
             for (int i = n_own; i < PP_->NIneq; ++i) H.dual_gamma[i] = 0.0;
-            upload_cuts(E, H, PP_);
+            upload();
         }
     }
     if (pstart) {
@@ -495,7 +507,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             PP_->NIneq = m;
             PP_->NPentIneq = np;
             PP_->NHeptaIneq = nh;
-            upload_cuts(E, H, PP_);
+            upload();
             const int mt = nd.cuts.m;
             double* gp = nd.b.gam.p;
             BQB_CUDA(cudaMemcpyAsync(gp, prop.data(), (size_t)mt * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -520,7 +532,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
                 PP_->NIneq = n_own;   // back to the child's own cuts
                 PP_->NPentIneq = 0;
                 PP_->NHeptaIneq = 0;
-                upload_cuts(E, H, PP_);
+                upload();
             }
         }
     }
@@ -533,7 +545,9 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         warm_first.assign(H.cuts, H.cuts + PP_->NIneq);
     }
     BundleDev& b = nd.b;
+    pc.mark(EP_REBUILD);
     b.ensure_cap(1 + bdl_iter + 2, n, s);
+    pc.mark(EP_ALLOC);
     const int m0 = nd.cuts.m;
     BQB_CUDA(cudaMemcpyAsync(b.gam.p, H.dual_gamma, (size_t)m0 * sizeof(double), cudaMemcpyHostToDevice, s));
     BQB_CUDA(cudaMemcpyAsync(b.Xb.p, dX, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -638,14 +652,16 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
             for (int i = 0; i < PP_->NPentIneq; ++i) H.dual_gamma[i + PP_->NIneq] = H.pcuts[i].y;
             for (int i = 0; i < PP_->NHeptaIneq; ++i)
                 H.dual_gamma[i + PP_->NIneq + PP_->NPentIneq] = H.hcuts[i].y;
-            upload_cuts(E, H, PP_);
+            upload();
             const int m = nd.cuts.m;
             BQB_CUDA(cudaMemcpyAsync(b.gam.p, H.dual_gamma, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, s));
             // current bundle size (host copy) for capacity and the G rebuild
             BQB_CUDA(cudaMemcpyAsync(nd.hi.p, b.istate.p, BI_WORDS * sizeof(int), cudaMemcpyDeviceToHost, s));
             BQB_CUDA(cudaStreamSynchronize(s));
             const int k = nd.hi.p[BI_K];
+            pc.mark(EP_REBUILD);
             b.ensure_cap(k + 2 + bdl_iter + 2, n, s);
+            pc.mark(EP_ALLOC);
             nd.hi.p[BI_CAP] = b.cap;
             BQB_CUDA(cudaMemcpyAsync(b.istate.p + BI_CAP, nd.hi.p + BI_CAP, sizeof(int), cudaMemcpyHostToDevice, s));
             // fct_eval(PP, dual_gamma, X_test, g) into the free slot
@@ -732,9 +748,9 @@ BQB_API long long bqb_bundle_iterations(int reset)
 }
 
 // Time by phase of the engines' SDPbound (seconds, summed over engines and
-// calls): out[9] = {IPM, lambda_eta, L - B^T(gamma), op_B + bundle step,
-// heuristic, triangle separation, pentagonal / heptagonal separation, cut
-// upload and the rest, whole calls}.  Profiling only: with it on, every
+// calls): out[12] = {IPM, lambda_eta, L - B^T(gamma), op_B + bundle step,
+// heuristic, triangle separation, pentagonal / heptagonal separation, the
+// rest, whole calls, cut upload, fracsol, bundle growth}.  Profiling only: with it on, every
 // phase boundary synchronises the engine's stream.  reset != 0 zeroes the
 // sums after reading.  No reference counterpart.
 BQB_API void bqb_engine_profile_enable(int on) { g_eprof_on.store(on ? 1 : 0); }
