@@ -428,6 +428,27 @@ def run_gpu(args):
         eng = {"value": ne / (e0.elapsed_time(e1) / 1e3), "unit": "nodes/s", "engines": T, "nodes": ne,
                "call": "bqb_bound_nodes, host nodes, one step (after one warm-up step)"}
 
+    # ---- FP64 certificates of node bounds (engines; one more IPM and a
+    # Cholesky factorisation per node, after the timed region) ----
+    cert = None
+    if T > 0 and args.cert_nodes > 0:
+        nc = min(args.cert_nodes, B)
+        st = np.zeros(6)
+        lib.bqb_certify_stats(_lib.dptr(st), 1)
+        lib.bqb_certify_enable(1)
+        lib.bqb_reset_incumbent(arm.lb)
+        try:
+            arm.bound_e2e(b0[:nc], min(T, 16))
+        finally:
+            lib.bqb_certify_enable(0)
+        lib.bqb_certify_stats(_lib.dptr(st), 1)
+        cert = {"nodes": int(st[0]), "max_rel_excess": float(st[1]), "mean_rel_excess": float(st[2]),
+                "failed": int(st[3]), "max_shift": float(st[4]), "max_rerun_mismatch": float(st[5]),
+                "call": "bqb_certify_enable(1) + bqb_bound_nodes on 16 engines, the first nodes of a timed batch",
+                "meaning": "per node: (certified bound - node bound) / max(1, |node bound|); the certified bound is "
+                           "sum(y) + n max(0, -lambda_lb(Diag(y) - L + B^T gamma)) + sum(gamma) + fixed value, "
+                           "lambda_lb an FP64 lower bound from a completed Cholesky factorisation and its backward error"}
+
     # ---- the plain drop-in (one node at a time, library stream) ----
     drop = None
     if args.dropin_nodes > 0:
@@ -607,6 +628,7 @@ def run_gpu(args):
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e / args.steps,
                     "call": "bqb_fused_submit/collect with host node structs"},
             "engines": eng,
+            "certificate": cert,
             "dropin_serial": drop,
             "time_to_optimality": tto,
             "learned_warm_start": learned,
@@ -925,6 +947,8 @@ def main():
                     help="also time the plain drop-in solver on the learned leg's instance")
     ap.add_argument("--engine-nodes", type=int, default=128,
                     help="nodes timed through the concurrent engines (0: skip)")
+    ap.add_argument("--cert-nodes", type=int, default=64,
+                    help="nodes whose bounds are certified in FP64 after the timed region (0: none)")
     ap.add_argument("--dropin-nodes", type=int, default=16,
                     help="nodes timed through the serial drop-in Evaluate (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

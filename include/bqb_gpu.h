@@ -472,6 +472,32 @@ void bqb_ipm_coop_profile_enable(int on);
 void bqb_ipm_coop_profile(double *out, int reset);
 int bqb_ipm_autotune(int n, int reps, int *best_grid, double *best_ms);
 
+/* FP64 certificate of a basic SDP bound (csrc/certificate.cu).  L: n x n
+ * column-major, y: any dual vector (host).  out[0] = an upper bound on
+ * max <L, X> over diag(X) = e, X psd that holds for every y: the sum of y
+ * plus n times an FP64 lower bound on -lambda_min(Diag(y) - L) when that
+ * minimum is negative, every rounding error bounded (a completed Cholesky
+ * factorisation of Diag(y) - L + tI and its backward error); out[1] = the
+ * lower bound on lambda_min; out[2] = the shift t the factorisation needed
+ * (0 when Diag(y) - L factors as it is); out[3] = 0, or 1 when no shift
+ * worked.  Returns 0, or 1 on bad arguments.  No reference counterpart (the
+ * reference's bound is the IPM's dual value, src/ipm_mc_pk.c:313-334). */
+int bqb_sdp_certificate(const double *L, const double *y, int n, double *out);
+/* ipm_mc_pk (src/ipm_mc_pk.c:28-359) that also returns the dual vector y of
+ * the last iterate (host, n doubles; phi is its sum): out[4] = {phi,
+ * iterations, status, <L, X>}; X may be NULL.  Returns 0, or 1 on bad
+ * arguments.  No reference counterpart. */
+int bqb_ipm_dual(const double *L, int n, double *X, double *y, double *out);
+/* Certificates of the engines' node bounds on (1) / off (0, default): each
+ * node's final bound is certified by one more IPM at its final multipliers
+ * and bqb_sdp_certificate.  bqb_certify_stats: out[6] = {nodes, largest and
+ * mean excess of the certified bound over the node's bound, relative to
+ * max(1, |bound|), nodes whose certificate failed, largest shift, largest
+ * relative difference between the rerun IPM's value and the bundle's};
+ * reset != 0 zeroes them.  No reference counterpart. */
+void bqb_certify_enable(int on);
+void bqb_certify_stats(double *out, int reset);
+
 /* Basic SDP bound of one problem without any device allocation.  No
  * counterpart in the reference: it exists for callers that may not call
  * cudaMalloc while they run (e.g. inside a host application whose memory

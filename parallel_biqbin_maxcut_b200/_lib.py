@@ -126,6 +126,11 @@ SIGNATURES = {
     "bqb_reset_incumbent": (None, [C.c_double]),
     "bqb_set_gw_hyperplanes": (None, [C.c_int]),
     "bqb_ipm_schedule_set": (None, [C.c_int, C.c_int]),
+    "bqb_sdp_certificate": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
+    "bqb_ipm_dual": (C.c_int, [C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_double)]),
+    "bqb_certify_enable": (None, [C.c_int]),
+    "bqb_certify_stats": (None, [C.POINTER(C.c_double), C.c_int]),
     "bqb_engine_profile_enable": (None, [C.c_int]),
     "bqb_engine_profile": (None, [C.POINTER(C.c_double), C.c_int]),
     "bqb_lambda_eta_profile": (None, [C.POINTER(C.c_double), C.c_int]),

@@ -63,16 +63,16 @@ void check_ipm_status_host(const double* out)
 // Device-level basic SDP bound for one problem (used by every caller).
 // xslot (optional, device): write X into dX + (*xslot) * n * n.
 void ipm_device(DevBuf<double>& wsbuf, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
-                const int* xslot)
+                const int* xslot, double* yout)
 {
     if (n > IPM_REG_NMAX) {
-        ipm_large(wsbuf, dL, dX, n, dout, s, xslot);
+        ipm_large(wsbuf, dL, dX, n, dout, s, xslot, yout);
         return;
     }
     size_t bytes = 0;
     const int place = ipm_place(n, rt().smem_optin, &bytes);
     double* ws = wsbuf.ensure(ipm_ws_doubles(n, place));
-    IpmDesc d{dL, dX, ws, dout, xslot, n, 0};
+    IpmDesc d{dL, dX, ws, dout, xslot, n, 0, yout};
     ipm_launch_one(d, s);
 }
 

@@ -62,6 +62,7 @@ struct Engine {
     uint64_t sa_seed = 0;    // its chains' seed base ...
     uint64_t sa_calls = 0;   // ... and the separation calls made so far
     DevBuf<double> ipm_ws;
+    DevBuf<double> cert_ws, cert_v;   // the bound certificate's factor (n x n) and vectors
     WarmDev warm;            // learned warm start of the bundle multipliers
     // set by a B&B driver before sdp_bound: the parent node's final cuts
     // (null: none); sdp_bound leaves the node's own final cuts in

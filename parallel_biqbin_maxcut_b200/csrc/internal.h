@@ -15,9 +15,9 @@ namespace bqb {
 // Basic SDP bound of one n x n problem already on the device (one launch).
 // ws: the caller's IPM scratch (grown as needed).  dout: 4 doubles (phi,
 // iterations, status, <L,X>).  xslot (optional, device): write X into
-// dX + (*xslot) * n * n.
+// dX + (*xslot) * n * n.  yout (optional, device): y of the last iterate.
 void ipm_device(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
-                const int* xslot = nullptr);
+                const int* xslot = nullptr, double* yout = nullptr);
 
 // Largest n of the register-resident IPM body (RM_NMAX in reg_linalg.cuh);
 // ipm_device hands larger problems to ipm_large.
@@ -26,10 +26,15 @@ constexpr int IPM_REG_NMAX = 128;
 // ipm_mc_pk for n > IPM_REG_NMAX as one cooperative multi-CTA launch
 // (csrc/ipm_large.cu); same arguments and results as ipm_device.
 void ipm_large(DevBuf<double>& ws, const double* dL, double* dX, int n, double* dout, cudaStream_t s,
-               const int* xslot);
+               const int* xslot, double* yout = nullptr);
 // Engines bounding nodes with n > IPM_REG_NMAX at the moment: ipm_large
 // divides the co-resident CTAs among them (csrc/ipm_large.cu).
 extern std::atomic<int> g_large_share;
+
+// FP64 certificate of the basic SDP bound of dL from the dual vector dy (both
+// device): dout[0..3] = certified bound, lower bound on lambda_min(Diag(y) -
+// L), shift used, status (csrc/certificate.cu).  ws: n x n scratch.
+void sdp_certificate(DevBuf<double>& ws, const double* dL, const double* dy, int n, double* dout, cudaStream_t s);
 
 // Raise the reference's fatal error for a non-zero IPM status word.
 void check_ipm_status_host(const double* out);

@@ -22,7 +22,8 @@ enum IpmStatus : int {
 // One problem.  L: n x n column-major (ld = n), read only.  X: n x n output.
 // ws: per-problem scratch of ipm_ws_doubles(n, place) doubles.
 // out[0] = phi (dual value e'y), out[1] = iterations, out[2] = status,
-// out[3] = final primal value <L,X>.  xslot (optional, device): the output
+// out[3] = final primal value <L,X>; yout (optional): y (phi = sum of y, in
+// the IPM's order).  xslot (optional, device): the output
 // matrix is X + (*xslot) * n * n, so a bundle can direct the result into a
 // free slot chosen on the device.
 struct IpmDesc {
@@ -33,6 +34,7 @@ struct IpmDesc {
     const int* xslot;
     int n;
     int pad_;
+    double* yout = nullptr;   // (optional) the dual vector y of the last iterate, n doubles
 };
 
 // Shared-memory placement flags chosen on the host from the largest n of a

@@ -71,6 +71,7 @@ struct CoopArgs {
     double* part;        // gridDim.x x 4 partial sums
     unsigned* bar;       // [0] arrivals, [1] generation, [2] error
     unsigned long long* prof;   // (may be null) CTA 0's nanoseconds per part, COOP_PROF_* slots
+    double* yout;        // (may be null) y of the last iterate
     int n;
 };
 
@@ -977,6 +978,9 @@ __global__ void __launch_bounds__(CT, 1) ipm_coop_kernel(CoopArgs a)
         // barriers, so no barrier is needed here)
     }
     if (!alive) status = IPM_SYNC;
+    // (y's last writes came before the update's barrier)
+    if (a.yout)
+        for (size_t c = gtid; c < (size_t)n; c += gstride) a.yout[c] = a.y[c];
     if (a.prof && blockIdx.x == 0 && threadIdx.x == 0) a.prof[COOP_PROF_TOTAL] += global_ns() - t_call;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out[0] = phi;
@@ -1075,7 +1079,7 @@ size_t ipm_large_ws_doubles(int n)
 // Xbase + (*xslot) * n * n.  Results in dout[0..3] (phi, iterations, status,
 // psi); status IPM_SYNC when a grid barrier gave up waiting.
 void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, double* dout, cudaStream_t s,
-               const int* xslot)
+               const int* xslot, double* yout)
 {
     const size_t nn = (size_t)n * n;
     double* p = wsbuf.ensure(ipm_large_ws_doubles(n));
@@ -1086,6 +1090,7 @@ void ipm_large(DevBuf<double>& wsbuf, const double* L, double* Xbase, int n, dou
     a.out = dout;
     a.stats = ipm_stats_device();
     a.prof = coop_prof_device();
+    a.yout = yout;
     a.n = n;
     a.Zi = p;
     a.F = a.Zi + nn;

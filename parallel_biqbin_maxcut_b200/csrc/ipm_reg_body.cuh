@@ -235,6 +235,8 @@ __device__ inline void ipm_body_reg(const IpmDesc& d, double* smem, int zi_in_sm
         gap = fabs(phi - psi);
     }
 
+    if (d.yout)
+        for (int i = tid; i < n; i += nt) d.yout[i] = y[i];
     if (tid == 0) {
         d.out[0] = phi;
         d.out[1] = (double)iter;

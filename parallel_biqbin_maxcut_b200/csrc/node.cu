@@ -56,6 +56,18 @@ std::atomic<int> g_root_effort{0};
 // loaded warm-start model takes precedence.
 std::atomic<int> g_parent_start{0};
 
+// Bound certificates (off by default): with them on, every node's final
+// bound B = F(gamma) + fixed value is certified in FP64 -- one more IPM at
+// the final multipliers gamma gives y, and sdp_certificate an upper bound
+// on the basic SDP value of L - B^T(gamma) from it -- and the excess of the
+// certified bound over B is recorded (B itself is what the node returns).
+std::atomic<int> g_cert_on{0};
+std::mutex g_cert_mu;
+struct CertStats {
+    long long nodes = 0, failed = 0;
+    double max_rel = 0.0, sum_rel = 0.0, max_mismatch = 0.0, max_shift = 0.0;
+} g_cert;
+
 // Trace of SDPbound's outer loop: one row of BQB_TRACE_COLS values per
 // round while tracing is on (inspection only).
 constexpr int BQB_TRACE_COLS = 9;
@@ -243,6 +255,47 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         upload_cuts(E, H, PP_);
         pc.mark(EP_UPLOAD);
     };
+    // the certificate of the bound B = fval + fixed value at the current
+    // multipliers (none: the basic bound)
+    auto certify = [&](bool with_cuts, double fval, double fixed) {
+        if (!g_cert_on.load()) return;
+        const int m = with_cuts ? nd.cuts.m : 0;
+        double* L0 = nd.L0.ensure(nn);
+        BQB_CUDA(cudaMemcpyAsync(L0, dL, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        std::vector<double> g(m > 0 ? m : 1);
+        if (m > 0) {
+            opBt_launch(nd.cuts, L0, n, nd.b.gam.p, s);
+            BQB_CUDA(cudaMemcpyAsync(g.data(), nd.b.gam.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        double* v = E.cert_v.ensure((size_t)n + 8);
+        ipm_device(E.ipm_ws, L0, E.warm.X.ensure(nn), n, v + n, s, nullptr, v);
+        sdp_certificate(E.cert_ws, L0, v, n, v + n + 4, s);
+        double h[8];
+        BQB_CUDA(cudaMemcpyAsync(h, v + n, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        BQB_CUDA(cudaStreamSynchronize(s));
+        // sum of the multipliers, with its rounding bounded
+        double sg = 0.0, sa = 0.0;
+        for (int i = 0; i < m; ++i) {
+            sg += g[i];
+            sa += fabs(g[i]);
+        }
+        const double sg_hi = sg + (m + 1) * 0x1p-53 * sa;
+        const double B = fval + fixed;
+        const double Bc = h[4] + sg_hi + fixed;
+        const double scale = fabs(B) > 1.0 ? fabs(B) : 1.0;
+        std::lock_guard<std::mutex> lk(g_cert_mu);
+        ++g_cert.nodes;
+        if ((int)h[7] != 0 || (int)h[2] != IPM_OK) {
+            ++g_cert.failed;
+            return;
+        }
+        const double rel = (Bc - B) / scale;
+        g_cert.max_rel = rel > g_cert.max_rel ? rel : g_cert.max_rel;
+        g_cert.sum_rel += rel;
+        const double mis = fabs(h[0] - (fval - sg)) / scale;   // the rerun's phi against F - sum(gamma)
+        g_cert.max_mismatch = mis > g_cert.max_mismatch ? mis : g_cert.max_mismatch;
+        g_cert.max_shift = h[6] > g_cert.max_shift ? h[6] : g_cert.max_shift;
+    };
     std::vector<int> x(NB > 0 ? NB : 1);
     std::vector<double> col(n);
     auto store_fracsol = [&]() {
@@ -303,8 +356,14 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     heuristic();
 
     double bound = f + fixedvalue;
-    if (bound < Bab_LBGet() + 1.0) return bound;
-    if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) return bound;
+    if (bound < Bab_LBGet() + 1.0) {
+        certify(false, f, fixedvalue);
+        return bound;
+    }
+    if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) {
+        certify(false, f, fixedvalue);
+        return bound;
+    }
 
     pc.mark(EP_REBUILD);
     viol3 = tri_update_dev(E, H, PP_, H.dual_gamma, &tri_add, &tri_sub);
@@ -314,7 +373,10 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     // the reference's BLAS calls reject m = 0 (src/bounding.c:122-131,
     // src/bundle.c:63, 315) and its result is undefined.  The basic bound is
     // the node's bound, returned as the reference's early exits return it.
-    if (PP_->NIneq == 0) return bound;
+    if (PP_->NIneq == 0) {
+        certify(false, f, fixedvalue);
+        return bound;
+    }
     for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
     double t = 0.5 * (bound - Bab_LBGet()) / (PP_->NIneq * viol3 * viol3);
 
@@ -723,6 +785,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     bound = f + fixedvalue;
     if (rank == 0) diff = basic_bound - bound;
     pc.mark(EP_REBUILD);
+    certify(true, f, fixedvalue);
     return bound;
 }
 
@@ -760,6 +823,29 @@ BQB_API void bqb_engine_profile(double* out, int reset)
         const long long v = reset ? g_eprof_ns[i].exchange(0) : g_eprof_ns[i].load();
         if (out) out[i] = 1e-9 * (double)v;
     }
+}
+
+// FP64 certificates of the engines' node bounds on (1) / off (0): each node
+// costs one more IPM and a Cholesky factorisation.  bqb_certify_stats:
+// out[6] = {nodes certified, the largest and the mean excess of the
+// certified bound over the node's bound (relative to max(1, |bound|)),
+// nodes whose certificate failed, the largest diagonal shift a certificate
+// needed, the largest difference between the rerun IPM's value and the
+// bundle's F - sum(gamma) (relative)}; reset != 0 zeroes the statistics.
+// No reference counterpart.
+BQB_API void bqb_certify_enable(int on) { g_cert_on.store(on ? 1 : 0); }
+BQB_API void bqb_certify_stats(double* out, int reset)
+{
+    std::lock_guard<std::mutex> lk(g_cert_mu);
+    if (out) {
+        out[0] = (double)g_cert.nodes;
+        out[1] = g_cert.max_rel;
+        out[2] = g_cert.nodes > g_cert.failed ? g_cert.sum_rel / (double)(g_cert.nodes - g_cert.failed) : 0.0;
+        out[3] = (double)g_cert.failed;
+        out[4] = g_cert.max_shift;
+        out[5] = g_cert.max_mismatch;
+    }
+    if (reset) g_cert = CertStats{};
 }
 
 // Parent start on (1) or off (0, the reference's start at every node).
