@@ -255,6 +255,16 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
         upload_cuts(E, H, PP_);
         pc.mark(EP_UPLOAD);
     };
+    // A node that branches without running its bundle (the use_diff rule, or
+    // no violated triangle) has no final cuts of its own: its children get
+    // its parent's (original vertex numbers, so they stay valid for every
+    // descendant that keeps their vertices; the child's mapping drops the
+    // others), so parent-informed starts and recorded parent features reach
+    // past it.
+    auto pass_parent_cuts = [&]() {
+        if ((warm_active() || warm_recording() || g_parent_start.load() != 0) && E.parent)
+            E.final_cuts = std::make_shared<ParentCuts>(*E.parent);
+    };
     // the certificate of the bound B = fval + fixed value at the current
     // multipliers (none: the basic bound)
     auto certify = [&](bool with_cuts, double fval, double fixed) {
@@ -362,6 +372,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     }
     if (params.use_diff && rank != 0 && bound > Bab_LBGet() + diff + 1.0) {
         certify(false, f, fixedvalue);
+        pass_parent_cuts();
         return bound;
     }
 
@@ -375,6 +386,7 @@ double sdp_bound(Engine& E, BabNode* node, Problem* SP_, Problem* PP_, int rank)
     // the node's bound, returned as the reference's early exits return it.
     if (PP_->NIneq == 0) {
         certify(false, f, fixedvalue);
+        pass_parent_cuts();
         return bound;
     }
     for (int i = 0; i < PP_->NIneq; ++i) H.dual_gamma[i] = H.cuts[i].y;
