@@ -104,12 +104,13 @@ void BundleDev::ensure_m(int m_, cudaStream_t s)
 
 extern std::atomic<int> g_eprof_on;
 
-// lambda_eta counters of the engines (with the engines' phase profile on):
-// calls, rounds, sum of k, cycles in the QP, cycles, sum of m.
+// lambda_eta counters of the engines and the fused kernel (with the engines'
+// phase profile on): calls, rounds, sum of k, cycles in the QP, cycles, sum
+// of m.
 DevBuf<unsigned long long> g_le_prof;
 std::mutex g_le_prof_mu;
 
-static unsigned long long* le_prof_device()
+unsigned long long* le_prof_device()
 {
     if (!g_eprof_on.load()) return nullptr;
     std::lock_guard<std::mutex> lock(g_le_prof_mu);

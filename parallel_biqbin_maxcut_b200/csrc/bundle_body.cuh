@@ -57,12 +57,13 @@ __device__ __forceinline__ void qp_chol_step(double (&s)[KP], int p, bool& pd, d
 }
 
 // Forward substitution step J for u and w together (lane p holds u_p, w_p
-// and row p of the factor): u_J *= 1/L_JJ, then u_p -= L_pJ u_J below.
+// and row p of the factor; R: the factor's diagonal reciprocals in shared
+// memory): u_J *= 1/L_JJ, then u_p -= L_pJ u_J below.
 template <int KP, int J>
-__device__ __forceinline__ void qp_fwd_step(const double (&s)[KP], int p, double rdiag, double& u, double& w)
+__device__ __forceinline__ void qp_fwd_step(const double (&s)[KP], int p, const double* R, double& u, double& w)
 {
     if constexpr (J < KP) {
-        const double rj = __shfl_sync(0xffffffffu, rdiag, J);
+        const double rj = R[J];
         const double uj = __dmul_rn(__shfl_sync(0xffffffffu, u, J), rj);
         const double wj = __dmul_rn(__shfl_sync(0xffffffffu, w, J), rj);
         if (p == J) {
@@ -72,17 +73,17 @@ __device__ __forceinline__ void qp_fwd_step(const double (&s)[KP], int p, double
             u = __dsub_rn(u, __dmul_rn(s[J], uj));
             w = __dsub_rn(w, __dmul_rn(s[J], wj));
         }
-        qp_fwd_step<KP, J + 1>(s, p, rdiag, u, w);
+        qp_fwd_step<KP, J + 1>(s, p, R, u, w);
     }
 }
 
 // Backward substitution step J (from KP - 1 down): u_J *= 1/L_JJ, then
 // u_p -= L_Jp u_J above; Lr holds the factor by rows.
 template <int KP, int J>
-__device__ __forceinline__ void qp_bwd_step(const double* Lr, int p, double rdiag, double& u, double& w)
+__device__ __forceinline__ void qp_bwd_step(const double* Lr, int p, const double* R, double& u, double& w)
 {
     if constexpr (J >= 0) {
-        const double rj = __shfl_sync(0xffffffffu, rdiag, J);
+        const double rj = R[J];
         const double uj = __dmul_rn(__shfl_sync(0xffffffffu, u, J), rj);
         const double wj = __dmul_rn(__shfl_sync(0xffffffffu, w, J), rj);
         if (p == J) {
@@ -93,14 +94,14 @@ __device__ __forceinline__ void qp_bwd_step(const double* Lr, int p, double rdia
             u = __dsub_rn(u, __dmul_rn(l, uj));
             w = __dsub_rn(w, __dmul_rn(l, wj));
         }
-        qp_bwd_step<KP, J - 1>(Lr, p, rdiag, u, w);
+        qp_bwd_step<KP, J - 1>(Lr, p, R, u, w);
     }
 }
 
-// warp_qp for k <= KP (16 or 32): lane a < k keeps the QP's entry a of
+// warp_qp for k <= KP (8, 12 or 16): lane a < k keeps the QP's entry a of
 // lambda, z, Q lambda, c, u, w and row a of A = Q + Diag(z ./ lambda) in
 // registers; ws holds the factor's column broadcasts, then its rows (KP x KP
-// doubles).  The arithmetic is warp_qp's below, operation for operation
+// doubles), then its diagonal reciprocals (KP).  The arithmetic is warp_qp's below, operation for operation
 // (the same sums in the same order, the same warp reductions), so both
 // forms return the same bits; this one has no shared-memory loop per row.
 template <int KP>
@@ -140,7 +141,8 @@ __device__ __noinline__ bool warp_qp_reg(int k, const double* Q, const double* c
     double res_p = 1.0 - s2;
     double gap = (s4 + 0.5 * s3) - (y - 0.5 * s3);
     int cnt = 0;
-    double* L = ws;   // KP x KP
+    double* L = ws;             // KP x KP
+    double* R = ws + KP * KP;   // KP
     while (fabs(gap) > 1e-5) {
         ++cnt;
         // A = Q + Diag(z ./ lambda) (lower, padded with the identity), r = c - y + Qlam
@@ -165,10 +167,11 @@ __device__ __noinline__ bool warp_qp_reg(int k, const double* Q, const double* c
         if (lane < KP) {
 #pragma unroll
             for (int r = 0; r < KP; ++r) L[lane * KP + r] = r <= lane ? a[r] : 0.0;
+            R[lane] = rdiag;
         }
         __syncwarp();
-        qp_fwd_step<KP, 0>(a, lane, rdiag, u, w);
-        qp_bwd_step<KP, KP - 1>(L, lane, rdiag, u, w);
+        qp_fwd_step<KP, 0>(a, lane, R, u, w);
+        qp_bwd_step<KP, KP - 1>(L, lane, R, u, w);
         const double su = warp_sum(own ? 0.0 + u : 0.0), sw = warp_sum(own ? 0.0 + w : 0.0);
         const double dy = (res_p + sw) / su;
         double ap = -BQB_BUNDLE_BIG, ad = -BQB_BUNDLE_BIG;
@@ -223,6 +226,8 @@ __device__ __noinline__ bool warp_qp_reg(int k, const double* Q, const double* c
 // Bundles of up to 16 go to the register form above (same results).
 __device__ inline bool warp_qp(int k, const double* Q, const double* c, double* lam, double* ws)
 {
+    if (k <= 8) return warp_qp_reg<8>(k, Q, c, lam, ws);
+    if (k <= 12) return warp_qp_reg<12>(k, Q, c, lam, ws);
     if (k <= 16) return warp_qp_reg<16>(k, Q, c, lam, ws);
     const int lane = threadIdx.x & 31;
     double* A = ws;

@@ -36,6 +36,7 @@
 
 #include "engine.h"
 #include "globals.h"
+#include "internal.h"
 #include "ipm.cuh"
 #include "nodek.h"
 
@@ -121,6 +122,7 @@ int next_pow2(int v)
 void fill_cfg(FusedCfg& c, int N0, int count, int rank, unsigned long long seed, size_t smem_optin)
 {
     memset(&c, 0, sizeof c);
+    c.le_prof = le_prof_device();
     c.N0 = N0;
     c.count = count;
     c.rank = rank;

@@ -36,6 +36,10 @@ extern std::atomic<int> g_large_share;
 // L), shift used, status (csrc/certificate.cu).  ws: n x n scratch.
 void sdp_certificate(DevBuf<double>& ws, const double* dL, const double* dy, int n, double* dout, cudaStream_t s);
 
+// The lambda_eta counters' device address while the engines' phase profile
+// is on, else null (csrc/bundle.cu).
+unsigned long long* le_prof_device();
+
 // Raise the reference's fatal error for a non-zero IPM status word.
 void check_ipm_status_host(const double* out);
 

@@ -1171,12 +1171,6 @@ BQB_API int bqb_ipm_autotune(int n, int reps, int* best_grid, double* best_ms)
     out.ensure(4);
     const int T = (n + CB - 1) / CB;
     std::vector<int> cand = {T * T, (T * T + 1) / 2, (T * T + 3) / 4, (T * T + 7) / 8, R.num_sms};
-    int keep = -1;
-    {
-        std::lock_guard<std::mutex> lock(g_sched_mu);
-        auto it = g_sched.find(T);
-        if (it != g_sched.end()) keep = it->second;
-    }
     cudaEvent_t e0, e1;
     BQB_CUDA(cudaEventCreate(&e0));
     BQB_CUDA(cudaEventCreate(&e1));
@@ -1201,7 +1195,9 @@ BQB_API int bqb_ipm_autotune(int n, int reps, int* best_grid, double* best_ms)
     }
     BQB_CUDA(cudaEventDestroy(e0));
     BQB_CUDA(cudaEventDestroy(e1));
-    (void)keep;
+    // (DevBuf does not free: the tuning problem's buffers go here)
+    for (double* q : {dL.p, dX.p, ws.p, out.p})
+        if (q) BQB_CUDA(cudaFree(q));
     bqb_ipm_schedule_set(n, bg);   // the fastest candidate stays in the schedule
     if (best_grid) *best_grid = bg;
     if (best_ms) *best_ms = bms;

@@ -1113,7 +1113,7 @@ __device__ void nk_bundle_iterations(const FusedCfg& c, Nk& k, int bdl_iter)
     const size_t nn = (size_t)k.n * k.n;
     for (int it = 0; it < bdl_iter; ++it) {
         LeArgs a{k.G, k.ldg, k.slot, m, nullptr, k.Fv, k.gam, k.lam, k.eta, k.dgam, k.gtest, k.dstate, k.istate,
-                 k.qpws, -1};
+                 k.qpws, -1, c.le_prof};
         {
             NkTimer tm(c.prof, NKP_LAMBDA);
             nk_lambda_eta(a);

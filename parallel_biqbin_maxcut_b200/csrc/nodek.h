@@ -85,6 +85,7 @@ struct FusedCfg {
     unsigned long long* lb;   // incumbent, order-preserving bits of a double
     double* ipm_stats;
     unsigned long long* prof;   // NKP_COUNT phase times (ns, summed over CTAs)
+    unsigned long long* le_prof;   // (may be null) lambda_eta counters, as the engines' (bqb_lambda_eta_profile)
     // learned warm start (warm.h): BF16 weights (null: off) and the
     // {kept, rejected} proposal counters
     const void* warm_p;
