@@ -86,9 +86,10 @@ LEG_CALLS = {
     "engines": "bqb_solve_parallel (16 concurrent engines; above 128 vertices the fused kernel does not apply), "
                "GW rounding with 4096 hyperplanes per round projected on the tensor cores (TF32), root effort "
                "(the root runs every outer round of SDPbound unless pruned)",
-    "engines_parent_start": "the engines leg with parent start (each child starts from its parent's final "
-                            "triangle, pentagonal and heptagonal cuts and multipliers when that start's dual "
-                            "value is lower)",
+    "engines_parent_start": "16 engines and 4096-hyperplane rounding as the engines leg, with parent start "
+                            "(each child starts from its parent's final triangle, pentagonal and heptagonal cuts "
+                            "and multipliers when that start's dual value is lower) and without root effort (the "
+                            "root gives up as the reference's rule says; its children are cheap with parent start)",
     "engines_learned": "the engines leg with the shipped warm-start model (children start from the parent's "
                        "multipliers where the model keeps them)",
     "plain_dropin": "bqb_solve: serial best-first B&B, one node at a time through the drop-in SDPbound",
@@ -480,7 +481,7 @@ def run_gpu(args):
             tto_sched = _lib.autotune_ipm([343], reps=2)
             cases.append(("torus343", TORUS_NAME, instances.torus3d(7, 1),
                           [("engines", dict(threads=16, gw_hyperplanes=4096, root_effort=True), None),
-                           ("engines_parent_start", dict(threads=16, gw_hyperplanes=4096, root_effort=True,
+                           ("engines_parent_start", dict(threads=16, gw_hyperplanes=4096, root_effort=False,
                                                          parent_start=True), None),
                            ("engines_learned", dict(threads=16, gw_hyperplanes=4096, root_effort=True), p_w)]))
         tto = {}
@@ -830,9 +831,37 @@ def run_case(args):
     the side; 7 gives n = 343); `--case fused`: `--count` subproblems
     (k ~ U[0, --kmax] fixed) of a seeded G(n, 0.5) +-1 instance bounded by
     one fused-kernel launch, after the root on the engine path;
-    `--case torus-root`: the 7x7x7 torus's root node on one engine."""
+    `--case torus-root`: the 7x7x7 torus's root node on one engine;
+    `--case kgon`: the pentagonal (--kgon-k 5, 3 types) or heptagonal (7, 4
+    types) annealing chains on the IPM solution X of the torus root
+    (`--count` chains, `--repeats` launches); `--case cert`: the FP64
+    certificate of the torus root's IPM bound, `--repeats` times."""
     lib = _lib.load()
     assert lib.bqb_init(0) == 0, lib.bqb_last_error()
+    if args.case in ("kgon", "cert"):
+        L343 = instances.root_matrix(instances.torus3d(7, 1))
+        n = L343.shape[0]
+        Lc = _lib.colmajor(L343)
+        X = np.zeros(n * n)
+        y = np.zeros(n)
+        out = np.zeros(4)
+        assert lib.bqb_ipm_dual(_lib.dptr(Lc), n, _lib.dptr(X), _lib.dptr(y), _lib.dptr(out)) == 0
+        for rep in range(args.repeats):
+            t0 = time.perf_counter()
+            if args.case == "kgon":
+                k, types = (5, 3) if args.kgon_k == 5 else (7, 4)
+                cost = np.zeros(args.count)
+                perm = np.zeros(args.count * 7, np.int32)
+                rc = lib.bqb_kgon_sa(_lib.dptr(X), n, k, types, args.count, 0x5eed + rep, _lib.dptr(cost),
+                                     _lib.iptr(perm))
+                print(f"kgon k={k} chains={args.count} rc={rc} best={cost.min():.6f} "
+                      f"wall={1e3 * (time.perf_counter() - t0):.2f} ms", flush=True)
+            else:
+                c = np.zeros(4)
+                assert lib.bqb_sdp_certificate(_lib.dptr(Lc), _lib.dptr(y), n, _lib.dptr(c)) == 0
+                print(f"cert n={n} phi={out[0]:.6f} certified={c[0]:.6f} rel={(c[0] - out[0]) / abs(out[0]):.3e} "
+                      f"shift={c[2]} wall={1e3 * (time.perf_counter() - t0):.2f} ms", flush=True)
+        return
     if args.case == "torus-root":
         # the torus's root node on one engine (rank 0), batched GW rounding
         A = np.ascontiguousarray(instances.torus3d(7, 1))
@@ -956,7 +985,8 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-nodes-per-step", type=int, default=256,
                     help="subproblems per step of the reference arm (bounded CPU sample)")
-    ap.add_argument("--case", choices=["ipm", "ipm-torus", "fused", "torus-root"], default=None,
+    ap.add_argument("--kgon-k", type=int, default=5, choices=[5, 7], help="--case kgon: 5 or 7")
+    ap.add_argument("--case", choices=["ipm", "ipm-torus", "fused", "torus-root", "kgon", "cert"], default=None,
                     help="run one small profiling case instead of the benchmark")
     ap.add_argument("--n", type=int, default=100, help="--case: vertices (ipm-torus: the side)")
     ap.add_argument("--repeats", type=int, default=3, help="--case ipm/ipm-torus: calls")
