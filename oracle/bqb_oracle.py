@@ -170,6 +170,68 @@ class IpmResult:
     phi: float
     iters: int
     alphas: list
+    y: np.ndarray = None   # the dual vector of the last iterate (phi = its sum)
+
+
+def sdp_certificate(L: np.ndarray, y: np.ndarray):
+    """FP64 certificate of a basic SDP bound from any dual vector y: returns
+    (bound, lambda_lb, shift).  No reference counterpart (the reference's
+    bound is its IPM's e'y); this restates the library's certificate
+    (csrc/certificate.cu) for its tests.  For any y, max <L, X> over
+    diag(X) = e, X psd is at most e'y + n max(0, -lambda_min(Diag(y) - L));
+    a completed floating-point Cholesky factorisation of A = Diag(y) - L + tI
+    gives lambda_min(A) >= -g/(1-g) trace(A), g = (n+1)u/(1-(n+1)u) (Higham,
+    Accuracy and Stability of Numerical Algorithms, Theorem 10.3).  The shift
+    t is 0, else found by doubling from trace * 2^-40 and 40 bisections; the
+    errors of forming the diagonal and of summing y are added as there.
+    LAPACK's factorisation stands in for the kernel's (the bound holds for
+    any completed one)."""
+    L = np.asarray(L, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    n = len(y)
+    u = 2.0 ** -53
+
+    def gam(k):
+        return k * u / (1.0 - k * u)
+
+    z = y - np.diag(L)
+    sy, say, tr, mz = float(y.sum()), float(np.abs(y).sum()), float(np.abs(z).sum()), float(np.abs(z).max())
+    slack = 1.0 + 4.0 * n * u
+
+    def passes(t):
+        A = -L.copy()
+        A[np.diag_indices(n)] = z + t
+        try:
+            np.linalg.cholesky(A)
+            return True
+        except np.linalg.LinAlgError:
+            return False
+
+    t = 0.0
+    ok = passes(0.0)
+    if not ok:
+        lo, t = 0.0, max(tr, 1.0) * 2.0 ** -40
+        for _ in range(64):
+            ok = passes(t)
+            if ok:
+                break
+            lo, t = t, 2.0 * t
+        if ok:
+            for _ in range(40):
+                mid = 0.5 * (lo + t)
+                if not (lo < mid < t):
+                    break
+                if passes(mid):
+                    t = mid
+                else:
+                    lo = mid
+    if not ok:
+        return float("inf"), float("-inf"), t
+    g = gam(n + 1)
+    lam = -(g / (1.0 - g) * (tr + n * t) * slack + t + 2.0 * u * (mz + t)) * slack
+    corr = n * -lam if lam < 0 else 0.0
+    v = sy + gam(n) * say * slack + corr
+    return v + abs(v) * 2.0 ** -50, lam, t
 
 
 def ipm_mc_pk(L: np.ndarray, max_iter: int = 500) -> IpmResult:
@@ -231,7 +293,7 @@ def ipm_mc_pk(L: np.ndarray, max_iter: int = 500) -> IpmResult:
         psi = float(np.vdot(L, X))
         gap = abs(phi - psi)
         alphas.append((ap, ad))
-    return IpmResult(X=X, phi=phi, iters=it, alphas=alphas)
+    return IpmResult(X=X, phi=phi, iters=it, alphas=alphas, y=y.copy())
 
 
 def fct_eval(L: np.ndarray, cuts: Cuts, gamma: np.ndarray):

@@ -8,7 +8,8 @@ IPM's bound by less than 1e-9 relative, needs no shift, and its eigenvalue
 bound lies below numpy's lambda_min; with y lowered until Diag(y) - L is
 indefinite it still bounds the oracle's primal value <L, X>; and with the
 engines' certification on, every node of a B&B is certified within the
-goal's 1e-6 relative (in fact 1e-9)."""
+goal's 1e-6 relative (in fact 1e-9).  The certified bounds equal the
+oracle's restatement (oracle/bqb_oracle.py sdp_certificate) on the same y."""
 import ctypes as C
 
 import numpy as np
@@ -54,6 +55,9 @@ def test_certificate_of_the_ipm_dual(lib, kind, nv, seed):
     assert c[0] >= phi and (c[0] - phi) <= REL * abs(phi), (c[0], phi)
     lam = np.linalg.eigvalsh(np.diag(y) - L).min()
     assert c[1] <= lam + 1e-12 * np.abs(L).max() * n
+    # the oracle's certificate of the same y (LAPACK's factorisation)
+    bo, lo, to = O.sdp_certificate(L, y)
+    assert to == 0.0 and abs(c[0] - bo) <= 1e-12 * abs(bo), (c[0], bo)
     if n <= 129:   # the oracle's IPM: its phi agrees and its primal value is below the certificate
         r = O.ipm_mc_pk(L)
         assert abs(phi - r.phi) <= 1e-6 * abs(r.phi)
@@ -80,6 +84,8 @@ def test_certificate_of_an_infeasible_dual(lib):
     assert c[0] >= float(np.sum(L * r.X))
     exact = yl.sum() + n * -lam
     assert exact - n * scale <= c[0] <= exact + 1e-6 * abs(exact)
+    bo, _, to = O.sdp_certificate(L, yl)
+    assert to > 0.0 and abs(c[0] - bo) <= 1e-9 * abs(bo), (c[0], bo)
 
 
 @pytest.mark.gpu
